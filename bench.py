@@ -1,0 +1,436 @@
+#!/usr/bin/env python
+"""LtL stepping throughput on B200: GCUPS of every exact GPU variant.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one generation of the whole grid): a 16384 x 16384
+torus, R = 5, Bosco's rule (S33-57 / B34-45 with the centre counted, i.e. the
+reference's S32-56 / B34-45), start grid = the reference generator's grid for
+--seed 1 -d 0.5 (host-generated, uploaded once).  Each variant (plain CUDA-core
+SWAR stencil, bit-packed, tcgen05 tensor core when built) is first checked
+bit-exact against the reference's own step-100 grid (tests/golden/golden.json),
+then timed: K steps, each preceded by an untimed 256 MiB L2 flush, each bracketed
+by CUDA events on the solver's stream.  `value` is the fastest variant's
+whole-job GCUPS (cells * steps / max-over-ranks time; every rank runs its own
+replica grid, so scaling is weak).
+
+With --impl reference the reference's own CPU solver (built from its sources
+into oracle/_ref/, AMX16 when the host has AMX-INT8, else AVX2) is timed on the
+host cores for the same workload.
+"""
+import argparse
+import glob
+import hashlib
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 16384
+RADIUS = 5
+RULE = (32, 56, 34, 45)
+SEED = 1
+DENSITY = 0.5
+WORKLOAD = ("16384x16384 torus, R=5 Moore, Bosco S33-57/B34-45 (centre counted; reference S32-56/B34-45), "
+            "start grid = reference generator --seed 1 -d 0.5 --threads 1")
+BYTES_PER_UPDATE = {"plain": 2.0, "tensor": 2.0, "packed": 0.25}
+DTYPE = {"plain": "u8", "tensor": "u8 (tcgen05 kind::i8)", "packed": "b1 (32 cells per u32)"}
+REF_RULE_TAG = "R5_S32-56_B34-45"
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_table():
+    """Per-launch DRAM bytes from the committed ncu summary, keyed by variant."""
+    out = {}
+    p = os.path.join(ROOT, "profiles", "traffic_n16384_r5.txt")
+    if os.path.exists(p):
+        for line in open(p):
+            line = line.strip()
+            if not line or line.startswith("#"):
+                continue
+            kv = dict(x.split("=", 1) for x in line.split())
+            if "variant" in kv and "dram_bytes_per_launch" in kv:
+                out[kv["variant"]] = float(kv["dram_bytes_per_launch"])
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"ltl_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        self.fh = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def dist_setup(args):
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def golden_step100():
+    p = os.path.join(ROOT, "tests", "golden", "golden.json")
+    for c in json.load(open(p))["cases"]:
+        if c["name"] == "config2_bosco_r5_n16384_amx16":
+            for cp in c["checkpoints"]:
+                if cp["step"] == 100:
+                    return cp["sha256"]
+    return None
+
+
+def run_variant(C, torch, name, start, args, flush, sampler=None):
+    vcode = {"plain": C.VARIANT_PLAIN, "tensor": C.VARIANT_TENSOR, "packed": C.VARIANT_PACKED}[name]
+    stream = torch.cuda.Stream()
+    s = C.CUDASolver(N, RADIUS, RULE, variant=vcode, device=torch.cuda.current_device())
+    try:
+        s.set_stream(stream.cuda_stream)
+        depth = s.info.temporal_depth
+        # bit-exactness against the reference's own grid after 100 generations
+        s.setState(start)
+        s.doSteps(100 - 100 % depth)
+        rest = 100 % depth
+        if rest:
+            raise RuntimeError("temporal depth does not divide 100")
+        got = s.getCurrentState()
+        want = golden_step100()
+        bit_exact = want is not None and hashlib.sha256(got.tobytes()).hexdigest() == want
+        # warm-up from the start grid
+        s.setState(start)
+        s.doSteps(args.warmup * depth)
+        s.synchronize()
+        passes = max(1, args.steps // depth)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(passes)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(passes)]
+        s.set_timing(True)
+        barrier(args.world)
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        with torch.cuda.stream(stream):
+            for p in range(passes):
+                flush.zero_()
+                starts[p].record(stream)
+                s.doSteps(depth)
+                ends[p].record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        barrier(args.world)
+        ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+        kernel_ms, kernel_launches, all_launches = s.get_timing()
+        s.set_timing(False)
+        gens = passes * depth
+        return dict(ms_total=ms, generations=gens, kernel_ms=kernel_ms, kernel_launches=kernel_launches,
+                    all_launches=all_launches, depth=depth, bit_exact_step100=bool(bit_exact), clocks=clocks,
+                    operand_bits=s.info.operand_bits)
+    finally:
+        s.close()
+
+
+def e2e_run(C, torch, name, start, steps):
+    """Through the public API with host buffers: upload the start grid from pinned
+    memory, advance `steps` generations, download the grid -- timed together."""
+    vcode = {"plain": C.VARIANT_PLAIN, "tensor": C.VARIANT_TENSOR, "packed": C.VARIANT_PACKED}[name]
+    stream = torch.cuda.Stream()
+    pinned_in = torch.from_numpy(start).pin_memory()
+    pinned_out = torch.empty_like(pinned_in).pin_memory()
+    import ctypes
+    L = C.lib()
+    s = C.CUDASolver(N, RADIUS, RULE, variant=vcode, device=torch.cuda.current_device())
+    try:
+        s.set_stream(stream.cuda_stream)
+        depth = s.info.temporal_depth
+        steps = max(depth, steps - steps % depth)
+        times = []
+        for it in range(3):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record(stream)
+            C.ltl.check(L.ltl_upload(s._h, ctypes.c_void_p(pinned_in.data_ptr()), N))
+            s.doSteps(steps)
+            C.ltl.check(L.ltl_download(s._h, ctypes.c_void_p(pinned_out.data_ptr()), N))
+            b.record(stream)
+            stream.synchronize()
+            if it > 0:
+                times.append(a.elapsed_time(b))
+        ms = sum(times) / len(times)
+        return dict(ms=ms, steps=steps, gcups=N * N * steps / (ms * 1e-3) / 1e9, h2d=N * N, d2h=N * N)
+    finally:
+        s.close()
+
+
+# ---------------------------------------------------------------------------
+# Reference CPU solver (built from the reference sources into oracle/_ref/)
+# ---------------------------------------------------------------------------
+def cpu_flags():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("flags"):
+                return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def reference_binary():
+    flags = cpu_flags()
+    base = os.path.join(ROOT, "oracle", "_ref")
+    native = os.path.join(base, REF_RULE_TAG + "_native", "prog")
+    portable = os.path.join(base, REF_RULE_TAG + "_portable", "prog")
+    need_native = {"avx512f", "avx512bw", "avx512vl", "amx_int8", "amx_tile", "avx512_fp16", "avx512_vnni"}
+    if os.path.exists(native) and need_native <= flags:
+        return native, "native"
+    if os.path.exists(portable) and "avx2" in flags:
+        return portable, "portable"
+    return None, None
+
+
+def run_reference(steps, threads, solver):
+    exe, build = reference_binary()
+    if exe is None:
+        return None
+    t0 = time.time()
+    r = subprocess.run([exe, str(N), str(solver), str(steps), "-d", str(DENSITY), "--seed", str(SEED), "--threads",
+                        str(threads)], capture_output=True, text=True, cwd="/tmp", timeout=1800)
+    wall = time.time() - t0
+    if r.returncode != 0:
+        return None
+    ms = float(r.stdout.strip().splitlines()[0])
+    return dict(ms_per_step=ms, gcups=N * N / (ms * 1e-3) / 1e9, wall_s=wall, build=build, exe=exe)
+
+
+def reference_solver_choice():
+    flags = cpu_flags()
+    if {"amx_int8", "amx_tile"} <= flags:
+        return 2, "AMX16 (solver 2)"
+    return 3, "AVX2 (solver 3)"
+
+
+def cpu_baseline_sample(threads):
+    """~10-30 s of the reference's best CPU solver on this workload."""
+    solver, label = reference_solver_choice()
+    probe = run_reference(1, threads, solver)
+    if probe is None:
+        return None
+    steps = int(max(1, min(50, 20000.0 / max(probe["ms_per_step"], 1e-3))))
+    res = run_reference(steps, threads, solver)
+    if res is None:
+        return None
+    return {"value": round(res["gcups"], 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
+            "sample": f"reference {label}, {res['build']} build, {N}x{N} R=5 Bosco, {steps} steps after a "
+                      f"1-step probe, its own ms/step ({res['ms_per_step']:.1f} ms)"}
+
+
+def main_reference(args):
+    world, rank, _ = env_int("WORLD_SIZE", 1), env_int("RANK", 0), env_int("LOCAL_RANK", 0)
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    solver, label = reference_solver_choice()
+    exe, build = reference_binary()
+    if exe is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference binaries not built for this host "
+                          "(oracle/_ref missing or CPU lacks AVX2)"}))
+        return
+    # warm-up sample (page-in, caches), then the timed sample
+    run_reference(max(1, min(args.warmup, 2)), threads, solver)
+    probe = run_reference(1, threads, solver)
+    budget_ms = 150000.0
+    steps = int(max(1, min(args.steps, budget_ms / max(probe["ms_per_step"], 1e-3))))
+    res = run_reference(steps, threads, solver)
+    gcups = res["gcups"]
+    line = {
+        "impl": "reference", "metric": "GCUPS", "value": round(gcups, 4), "unit": "GCUPS", "n_gpus": args.gpus,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": round(res["ms_per_step"], 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic: reference generator start grid", "config": {"workload": WORKLOAD, "solver": label},
+        "cpu_baseline": {"value": round(gcups, 4), "unit": "GCUPS", "cores": threads, "kind": "reference",
+                         "sample": f"reference {label} ({build} build), {steps} steps of {N}x{N}, "
+                                   f"{threads} OpenMP threads, its own ms/step"},
+        "e2e": {"value": round(gcups, 4), "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variants", default="plain,packed,tensor")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        main_reference(args)
+        return
+
+    world, rank, local = dist_setup(args)
+    args.world = world
+    import torch
+    torch.cuda.set_device(local)
+    import cat_cpu_b200 as C
+
+    start = C.start_grid(N, SEED, DENSITY, 1)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    results = {}
+    sampler = ClockSampler(local)
+    for name in [v for v in args.variants.split(",") if v]:
+        try:
+            results[name] = run_variant(C, torch, name, start, args, flush, sampler if rank == 0 else None)
+        except C.LtlError as e:
+            if e.code == C.ltl.EUNSUPPORTED:
+                results[name] = {"unsupported": str(e)}
+                continue
+            raise
+    peak, peak_kind = measured_peaks()
+    traffic = traffic_table()
+    variants = {}
+    best = None
+    for name, r in results.items():
+        if "unsupported" in r:
+            variants[name] = r
+            continue
+        t_max = max_over_ranks(r["ms_total"], world)
+        gcups = world * N * N * r["generations"] / (t_max * 1e-3) / 1e9
+        kernel_ms_launch = r["kernel_ms"] / max(r["kernel_launches"], 1)
+        alg = N * N * BYTES_PER_UPDATE[name] * r["depth"]
+        achieved = alg / (kernel_ms_launch * 1e-3) / 1e9
+        variants[name] = {
+            "gcups": round(gcups, 3), "ms_per_step": round(t_max / r["generations"], 5),
+            "kernel_ms_per_launch": round(kernel_ms_launch, 5), "temporal_depth": r["depth"],
+            "bit_exact_step100": r["bit_exact_step100"], "dtype": DTYPE[name],
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic.get(name)},
+            "gpu_launches": r["all_launches"],
+        }
+        if r["bit_exact_step100"] and (best is None or gcups > variants[best]["gcups"]):
+            best = name
+    if best is None:
+        raise SystemExit("no variant was bit-exact against the reference grid")
+    head = variants[best]
+    line = {
+        "metric": "GCUPS (cell updates / s / 1e9), one generation of a 16384^2 LtL torus per step, bit-exact",
+        "value": head["gcups"], "unit": "GCUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": head["dtype"], "data": "synthetic: reference generator start grid (seed 1, d=0.5), one replica "
+                                        "per rank",
+        "config": {"workload": WORKLOAD, "variant": best, "n": N, "radius": RADIUS, "rule_centre_excluded": RULE,
+                   "l2": "flushed before every timed step (256 MiB device write, untimed)",
+                   "parallelism": f"replicas x{world}"},
+        "variants": variants,
+        "roofline": dict(head["roofline"], peak_kind=f"{peak_kind} hbm_gbs"),
+        "gpu_launches": head["gpu_launches"],
+    }
+    if "plain" in variants and "gcups" in variants.get("tensor", {}):
+        line["tensor_vs_plain"] = round(variants["tensor"]["gcups"] / variants["plain"]["gcups"], 3)
+    if rank == 0 and results[best].get("clocks"):
+        line["clocks"] = results[best]["clocks"]
+    # end to end through the public API with host buffers
+    e2 = e2e_run(C, torch, best, start, args.e2e_steps or args.steps)
+    e2_ms = max_over_ranks(e2["ms"], world)
+    line["e2e"] = {"value": round(world * N * N * e2["steps"] / (e2_ms * 1e-3) / 1e9, 3), "unit": "GCUPS",
+                   "h2d_bytes_per_step": int(e2["h2d"] / e2["steps"]), "d2h_bytes_per_step": int(e2["d2h"] /
+                                                                                                e2["steps"]),
+                   "note": f"upload start grid from pinned host memory + {e2['steps']} steps + download, "
+                           f"{best} variant"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline_sample(os.cpu_count() or 1)
+        if cb is not None:
+            line["cpu_baseline"] = cb
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,392 @@
+// k_packed.cu -- K3: bit-packed LtL step (one bit per cell) and the PACK codec.
+//
+// Same function as the reference's HostSolver<int> step (kezada94/CAT_cpu,
+// src/CellularAutomata/Solvers/HostSolver.tpp:58-91, torus halo :93-140), with
+// 32 cells per 32-bit word and the neighbour count kept bit-sliced:
+//   h(row) = horizontal (2R+1)-window count of one row, as PH bit planes, by a
+//            carry-save (Wallace) reduction of the 2R+1 shifted row words;
+//   B      = vertical sliding sum of h over 2R+1 rows, as PB bit planes
+//            (B -= h(r-R); B += h(r+R+1) while a thread walks down its band);
+//   next   = s ? [smin+1 <= B <= smax+1] : [bmin <= B <= bmax]   (B includes the centre)
+// evaluated with bit-sliced comparators.  Every operation acts on 32 cells.
+//
+// The PACK codec (ltl_pack_device / ltl_unpack_device) stores row i of a grid
+// as ceil(cols/64) uint64 words, cell (i, j) = bit j % 64 of word j / 64.
+#include <algorithm>
+
+#include "ltl_kernels.h"
+
+namespace ltl {
+
+__host__ __device__ constexpr int bits_for(int v) {
+    int b = 0;
+    while ((1 << b) <= v) ++b;
+    return b;
+}
+
+// Wallace reduction: out[0..P) = bit planes of the number of set inputs per lane.
+template <int M, int L, int P>
+__device__ __forceinline__ void wallace(const uint32_t* v, uint32_t* out) {
+    if constexpr (L < P) {
+        if constexpr (M == 0) {
+            out[L] = 0u;
+            wallace<0, L + 1, P>(v, out);
+        } else {
+            constexpr int NF = (M >= 3) ? (M - 1) / 2 : 0;
+            constexpr int REM = M - 2 * NF;
+            constexpr int NH = (REM == 2) ? 1 : 0;
+            constexpr int NC = NF + NH;
+            uint32_t carry[NC > 0 ? NC : 1];
+            uint32_t acc = v[0];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                uint32_t a = acc, b = v[1 + 2 * f], c = v[2 + 2 * f];
+                acc = a ^ b ^ c;
+                carry[f] = (a & b) | (a & c) | (b & c);
+            }
+            if constexpr (NH == 1) {
+                uint32_t b = v[M - 1];
+                carry[NF] = acc & b;
+                acc ^= b;
+            }
+            out[L] = acc;
+            wallace<NC, L + 1, P>(carry, out);
+        }
+    }
+}
+
+// B -= h (h <= B per lane), B has PB planes, h has PH planes.
+template <int PB, int PH>
+__device__ __forceinline__ void planes_sub(uint32_t (&B)[PB], const uint32_t (&h)[PH]) {
+    uint32_t br = 0u;
+#pragma unroll
+    for (int i = 0; i < PB; ++i) {
+        uint32_t b = B[i];
+        uint32_t x = (i < PH) ? h[i] : 0u;
+        B[i] = b ^ x ^ br;
+        br = (~b & (x | br)) | (x & br);
+    }
+}
+
+// B += h
+template <int PB, int PH>
+__device__ __forceinline__ void planes_add(uint32_t (&B)[PB], const uint32_t (&h)[PH]) {
+    uint32_t cy = 0u;
+#pragma unroll
+    for (int i = 0; i < PB; ++i) {
+        uint32_t b = B[i];
+        uint32_t x = (i < PH) ? h[i] : 0u;
+        B[i] = b ^ x ^ cy;
+        cy = (b & x) | (b & cy) | (x & cy);
+    }
+}
+
+// Lanes where lo <= B <= hi (lo, hi in [0, 2^PB); caller folds empty intervals).
+template <int PB>
+__device__ __forceinline__ uint32_t planes_in(const uint32_t (&B)[PB], int lo, int hi) {
+    uint32_t ge = 0xffffffffu, le = 0xffffffffu;  // carry-in of B + ~lo + 1 and hi + ~B + 1
+#pragma unroll
+    for (int i = 0; i < PB; ++i) {
+        uint32_t b = B[i];
+        uint32_t lm = 0u - (uint32_t)((lo >> i) & 1);
+        uint32_t hm = 0u - (uint32_t)((hi >> i) & 1);
+        ge = (lm & (b & ge)) | (~lm & (b | ge));
+        le = (hm & (~b | le)) | (~hm & (~b & le));
+    }
+    return ge & le;
+}
+
+struct PackedRule {
+    int lo0, hi0, lo1, hi1;  // birth (dead cell) and survival (live cell) intervals on B
+    uint32_t empty0, empty1; // ~0u when the interval is empty
+};
+
+static PackedRule make_packed_rule(const Rule& r) {
+    const int maxB = (2 * r.radius + 1) * (2 * r.radius + 1);
+    PackedRule p{};
+    auto fold = [&](int lo, int hi, int& olo, int& ohi, uint32_t& empty) {
+        lo = std::max(lo, 0);
+        hi = std::min(hi, maxB);
+        if (lo > hi) {
+            olo = 0;
+            ohi = 0;
+            empty = 0xffffffffu;
+        } else {
+            olo = lo;
+            ohi = hi;
+            empty = 0u;
+        }
+    };
+    fold(r.bmin, r.bmax, p.lo0, p.hi0, p.empty0);
+    fold(r.smin + 1, r.smax + 1, p.lo1, p.hi1, p.empty1);
+    return p;
+}
+
+// Horizontal window count of one frame row for word column fw (frame column).
+// All lanes of the warp must call it together (shuffles).
+template <int R, int PH>
+__device__ __forceinline__ void hcount(const uint32_t* __restrict__ row, int fw, bool active, int lane,
+                                       uint32_t (&h)[PH]) {
+    uint32_t own = active ? __ldg(row + fw) : 0u;
+    uint32_t left = __shfl_up_sync(0xffffffffu, own, 1);
+    uint32_t right = __shfl_down_sync(0xffffffffu, own, 1);
+    if (lane == 0 && active) left = __ldg(row + fw - 1);
+    if (lane == 31 && active) right = __ldg(row + fw + 1);
+    uint32_t x[2 * R + 1];
+#pragma unroll
+    for (int d = -R; d <= R; ++d) {
+        uint32_t v;
+        if (d == 0)
+            v = own;
+        else if (d > 0)
+            v = __funnelshift_rc(own, right, d);   // cells j + d: higher bits, then the right word
+        else
+            v = __funnelshift_lc(left, own, -d);   // cells j - |d|: lower bits, then the left word
+        x[d + R] = v;
+    }
+    wallace<2 * R + 1, 0, PH>(x, h);
+}
+
+constexpr int kPackedBand = 64;
+
+template <int R>
+__global__ void __launch_bounds__(128)
+k_packed_step(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int n, int nw, int HR, int HW,
+              size_t wp, int n_wstrips, int n_items, PackedRule pr) {
+    constexpr int PH = bits_for(2 * R + 1);
+    constexpr int PB = bits_for((2 * R + 1) * (2 * R + 1));
+    const int lane = threadIdx.x & 31;
+    const int warps_per_cta = blockDim.x >> 5;
+    const int gwarp = blockIdx.x * warps_per_cta + (threadIdx.x >> 5);
+    const int gwarps = gridDim.x * warps_per_cta;
+
+    for (int item = gwarp; item < n_items; item += gwarps) {
+        const int ws = item % n_wstrips;
+        const int band = item / n_wstrips;
+        const int r0 = band * kPackedBand;
+        const int r1 = min(r0 + kPackedBand, n);
+        const int w = ws * 32 + lane;     // inner word
+        const bool active = w <= nw;      // w == nw is the right halo word (neighbour of the last word)
+        const bool outputs = w < nw;
+        const int fw = HW + w;
+        auto rowp = [&](int r) { return cur + (size_t)(HR + r) * wp; };
+
+        uint32_t B[PB];
+#pragma unroll
+        for (int i = 0; i < PB; ++i) B[i] = 0u;
+#pragma unroll 1
+        for (int dy = -R; dy <= R; ++dy) {
+            uint32_t h[PH];
+            hcount<R, PH>(rowp(r0 + dy), fw, active, lane, h);
+            planes_add<PB, PH>(B, h);
+        }
+#pragma unroll 1
+        for (int r = r0; r < r1; ++r) {
+            if (outputs) {
+                uint32_t s = __ldg(rowp(r) + fw);
+                uint32_t in1 = planes_in<PB>(B, pr.lo1, pr.hi1) & ~pr.empty1;
+                uint32_t in0 = planes_in<PB>(B, pr.lo0, pr.hi0) & ~pr.empty0;
+                nxt[(size_t)(HR + r) * wp + fw] = (s & in1) | (~s & in0);
+            }
+            if (r + 1 < r1) {
+                uint32_t h[PH];
+                hcount<R, PH>(rowp(r - R), fw, active, lane, h);
+                planes_sub<PB, PH>(B, h);
+                hcount<R, PH>(rowp(r + R + 1), fw, active, lane, h);
+                planes_add<PB, PH>(B, h);
+            }
+        }
+    }
+}
+
+bool packed_supported(int n, int radius) { return radius >= 1 && radius <= 32 && n >= radius; }
+
+template <int R>
+static cudaError_t launch_packed_r(const PackedFrame& c, const PackedFrame& x, const PackedRule& pr,
+                                   cudaStream_t s) {
+    const int n_wstrips = (c.nw + 1 + 31) / 32;
+    const int bands = (c.n + kPackedBand - 1) / kPackedBand;
+    const int items = n_wstrips * bands;
+    const int wpc = 4;
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_packed_step<R>, wpc * 32, 0);
+    if (per_sm < 1) per_sm = 1;
+    int ctas = std::min((items + wpc - 1) / wpc, sms * per_sm);
+    k_packed_step<R><<<ctas, wpc * 32, 0, s>>>(c.words, x.words, c.n, c.nw, c.HR, c.HW, c.wpitch, n_wstrips,
+                                               items, pr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_packed_step(const PackedFrame& cur, const PackedFrame& nxt, const Rule& rule,
+                               cudaStream_t s) {
+    PackedRule pr = make_packed_rule(rule);
+    switch (rule.radius) {
+#define LTL_PR(r) \
+    case r: return launch_packed_r<r>(cur, nxt, pr, s);
+        LTL_PR(1) LTL_PR(2) LTL_PR(3) LTL_PR(4) LTL_PR(5) LTL_PR(6) LTL_PR(7) LTL_PR(8)
+        LTL_PR(9) LTL_PR(10) LTL_PR(11) LTL_PR(12) LTL_PR(13) LTL_PR(14) LTL_PR(15) LTL_PR(16)
+        LTL_PR(17) LTL_PR(18) LTL_PR(19) LTL_PR(20) LTL_PR(21) LTL_PR(22) LTL_PR(23) LTL_PR(24)
+        LTL_PR(25) LTL_PR(26) LTL_PR(27) LTL_PR(28) LTL_PR(29) LTL_PR(30) LTL_PR(31) LTL_PR(32)
+#undef LTL_PR
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Packed halo: column halo bits of inner rows (bit position p of the frame row
+// holds cell (p - 32*HW) mod n), then whole top/bottom rows copied from the
+// inner rows they wrap to.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t packed_bit(const uint32_t* row, int HW, int cell) {
+    int p = 32 * HW + cell;
+    return (row[p >> 5] >> (p & 31)) & 1u;
+}
+
+__global__ void k_packed_halo_cols(uint32_t* __restrict__ g, int n, int nw, int HR, int HW, size_t wp) {
+    // per inner row: words [0, HW) and [HW + nw - 1, HW + nw + HW)
+    const int per_row = 2 * HW + 1;
+    const long long total = (long long)n * per_row;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / per_row);
+        const int k = (int)(t % per_row);
+        const int fw = k < HW ? k : HW + nw - 1 + (k - HW);
+        uint32_t* row = g + (size_t)(HR + i) * wp;
+        uint32_t v = 0u;
+        if (fw == HW + nw - 1) {
+            // last inner word: keep its inner bits, rewrite the bits past n
+            const int inner_bits = n - 32 * (nw - 1);
+            v = inner_bits >= 32 ? row[fw] : (row[fw] & ((1u << inner_bits) - 1u));
+            for (int b = inner_bits; b < 32; ++b) {
+                int cell = 32 * (nw - 1) + b;
+                v |= packed_bit(row, HW, cell % n) << b;
+            }
+        } else {
+            for (int b = 0; b < 32; ++b) {
+                int cell = 32 * (fw - HW) + b;
+                int src = ((cell % n) + n) % n;
+                v |= packed_bit(row, HW, src) << b;
+            }
+        }
+        // the halo words only read inner bits (< n), never bits written here
+        row[fw] = v;
+    }
+}
+
+__global__ void k_packed_halo_rows(uint32_t* __restrict__ g, int n, int HR, size_t wp) {
+    const int band = blockIdx.y;  // 0 .. 2HR-1
+    const int r = band < HR ? band : n + band;
+    const int src = HR + (((r - HR) % n) + n) % n;
+    uint32_t* d = g + (size_t)r * wp;
+    const uint32_t* sp = g + (size_t)src * wp;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < (int)wp; w += gridDim.x * blockDim.x) d[w] = sp[w];
+}
+
+cudaError_t launch_packed_halo(const PackedFrame& f, cudaStream_t s) {
+    const long long total = (long long)f.n * (2 * f.HW + 1);
+    int blocks = (int)std::min<long long>((total + 127) / 128, 4096);
+    k_packed_halo_cols<<<blocks, 128, 0, s>>>(f.words, f.n, f.nw, f.HR, f.HW, f.wpitch);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    dim3 g2((unsigned)std::max<size_t>(1, std::min<size_t>((f.wpitch + 127) / 128, 64)), (unsigned)(2 * f.HR));
+    k_packed_halo_rows<<<g2, 128, 0, s>>>(f.words, f.n, f.HR, f.wpitch);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Byte frame <-> packed frame (inner cells only; halos are refilled after).
+// ---------------------------------------------------------------------------
+__global__ void k_pack_frame(const uint8_t* __restrict__ src, int n, int H, size_t pitch, uint32_t* __restrict__ dst,
+                             int nw, int HR, int HW, size_t wp) {
+    const long long total = (long long)n * nw;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / nw), w = (int)(t % nw);
+        const uint8_t* p = src + (size_t)(H + i) * pitch + H + 32 * w;
+        uint32_t v = 0u;
+        for (int b = 0; b < 32 && 32 * w + b < n; ++b) v |= (uint32_t)(p[b] & 1u) << b;
+        dst[(size_t)(HR + i) * wp + HW + w] = v;
+    }
+}
+
+__global__ void k_unpack_frame(const uint32_t* __restrict__ src, int n, int nw, int HR, int HW, size_t wp,
+                               uint8_t* __restrict__ dst, int H, size_t pitch) {
+    const long long total = (long long)n * nw;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / nw), w = (int)(t % nw);
+        const uint32_t v = src[(size_t)(HR + i) * wp + HW + w];
+        uint8_t* p = dst + (size_t)(H + i) * pitch + H + 32 * w;
+        for (int b = 0; b < 32 && 32 * w + b < n; ++b) p[b] = (uint8_t)((v >> b) & 1u);
+    }
+}
+
+cudaError_t launch_pack_frame(const Frame& src, const PackedFrame& dst, cudaStream_t s) {
+    long long total = (long long)src.n * dst.nw;
+    int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+    k_pack_frame<<<blocks, 256, 0, s>>>(src.base, src.n, src.H, src.pitch, dst.words, dst.nw, dst.HR, dst.HW,
+                                        dst.wpitch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_frame(const PackedFrame& src, const Frame& dst, cudaStream_t s) {
+    long long total = (long long)src.n * src.nw;
+    int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+    k_unpack_frame<<<blocks, 256, 0, s>>>(src.words, src.n, src.nw, src.HR, src.HW, src.wpitch, dst.base, dst.H,
+                                          dst.pitch);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_halo_fill(dst, s);
+}
+
+// ---------------------------------------------------------------------------
+// PACK codec on dense device buffers.
+// ---------------------------------------------------------------------------
+__global__ void k_pack64(const uint8_t* __restrict__ cells, size_t cp, int rows, int cols, uint64_t* __restrict__ words,
+                         size_t wp) {
+    const int nw = (cols + 63) / 64;
+    const long long total = (long long)rows * nw;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / nw), w = (int)(t % nw);
+        const uint8_t* p = cells + (size_t)i * cp + 64 * (size_t)w;
+        uint64_t v = 0ull;
+        for (int b = 0; b < 64 && 64 * w + b < cols; ++b) v |= (uint64_t)(p[b] ? 1u : 0u) << b;
+        words[(size_t)i * wp + w] = v;
+    }
+}
+
+__global__ void k_unpack64(const uint64_t* __restrict__ words, size_t wp, int rows, int cols, uint8_t* __restrict__ cells,
+                           size_t cp) {
+    const int nw = (cols + 63) / 64;
+    const long long total = (long long)rows * nw;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / nw), w = (int)(t % nw);
+        const uint64_t v = words[(size_t)i * wp + w];
+        uint8_t* p = cells + (size_t)i * cp + 64 * (size_t)w;
+        for (int b = 0; b < 64 && 64 * w + b < cols; ++b) p[b] = (uint8_t)((v >> b) & 1ull);
+    }
+}
+
+cudaError_t launch_pack(const uint8_t* cells, size_t cell_pitch, int rows, int cols, uint64_t* words,
+                        size_t word_pitch_words, cudaStream_t s) {
+    if (rows == 0 || cols == 0) return cudaSuccess;
+    long long total = (long long)rows * ((cols + 63) / 64);
+    int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+    k_pack64<<<blocks, 256, 0, s>>>(cells, cell_pitch, rows, cols, words, word_pitch_words);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(const uint64_t* words, size_t word_pitch_words, int rows, int cols, uint8_t* cells,
+                          size_t cell_pitch, cudaStream_t s) {
+    if (rows == 0 || cols == 0) return cudaSuccess;
+    long long total = (long long)rows * ((cols + 63) / 64);
+    int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+    k_unpack64<<<blocks, 256, 0, s>>>(words, word_pitch_words, rows, cols, cells, cell_pitch);
+    return cudaGetLastError();
+}
+
+}  // namespace ltl

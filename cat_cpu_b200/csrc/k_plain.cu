@@ -1,0 +1,461 @@
+// k_plain.cu -- CUDA-core kernels of libltl_b200:
+//   K5 torus halo fill, K1 plain LtL step (SWAR fast path for R <= 5 and a
+//   generic two-pass path for any R), K6 population / comparison, and the
+//   dense <-> frame copies used by upload/download.
+//
+// Semantics restated from the reference (kezada94/CAT_cpu):
+//   step  HostSolver<int>::CAStepAlgorithm, src/CellularAutomata/Solvers/HostSolver.tpp:58-73
+//   count HostSolver<int>::countAliveNeighbors (centre excluded), HostSolver.tpp:75-91
+//   rule  transitionFunction [a <= k <= b], HostSolver.tpp:47-51
+//   halo  fillHorizontal/VerticalBoundaryConditions (torus), HostSolver.tpp:93-140
+#include <algorithm>
+
+#include "ltl_kernels.h"
+
+namespace ltl {
+
+// ---------------------------------------------------------------------------
+// K5: halo fill.  Frame cell (r, c) <- inner ((r-H) mod n, (c-H) mod n).  All
+// sources are inner cells, so no ordering between halo bands is needed.
+// Top/bottom bands copy 16-byte chunks whose columns are inner (same column in
+// the source row); everything else goes byte by byte.
+// ---------------------------------------------------------------------------
+__global__ void k_halo_rows(uint8_t* __restrict__ g, int n, int H, size_t pitch) {
+    const int band = blockIdx.y;                       // 0 .. 2H-1
+    const int r = band < H ? band : n + band;          // frame row
+    const int src_r = H + wrap_mod(r - H, n);
+    const int W = n + 2 * H;
+    const int nchunks = (W + 15) / 16;
+    uint8_t* dst_row = g + (size_t)r * pitch;
+    const uint8_t* src_row = g + (size_t)src_r * pitch;
+    for (int ch = blockIdx.x * blockDim.x + threadIdx.x; ch < nchunks; ch += gridDim.x * blockDim.x) {
+        int c0 = ch * 16;
+        if (c0 >= H && c0 + 16 <= H + n) {
+            *(uint4*)(dst_row + c0) = *(const uint4*)(src_row + c0);
+        } else {
+            for (int c = c0; c < c0 + 16 && c < W; ++c) dst_row[c] = src_row[H + wrap_mod(c - H, n)];
+        }
+    }
+}
+
+__global__ void k_halo_cols(uint8_t* __restrict__ g, int n, int H, size_t pitch) {
+    // inner rows only; 2H halo bytes per row
+    const int per_row = 2 * H;
+    const long long total = (long long)n * per_row;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(t / per_row);
+        int k = (int)(t % per_row);
+        int c = k < H ? k : n + k;  // frame column
+        uint8_t* row = g + (size_t)(H + i) * pitch;
+        row[c] = row[H + wrap_mod(c - H, n)];
+    }
+}
+
+cudaError_t launch_halo_fill(const Frame& f, cudaStream_t s) {
+    const int W = f.n + 2 * f.H;
+    const int nchunks = (W + 15) / 16;
+    dim3 g1((unsigned)std::min((nchunks + 127) / 128, 64), (unsigned)(2 * f.H));
+    k_halo_rows<<<g1, 128, 0, s>>>(f.base, f.n, f.H, f.pitch);
+    long long total = (long long)f.n * 2 * f.H;
+    int blocks = (int)std::min<long long>((total + 255) / 256, 4096);
+    k_halo_cols<<<blocks, 256, 0, s>>>(f.base, f.n, f.H, f.pitch);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// K1 fast path (R <= 5): SWAR with 8-bit lanes.
+//
+// A warp owns a 512-column strip: lane L holds the 16-cell chunk at inner
+// columns [x, x+16), x = strip*480 - 16 + 16L, as four 32-bit words of byte
+// lanes.  It slides a vertical window of 2R+1 rows down its band: V = column
+// sums (<= 2R+1 per lane).  Row sums of V come from the lane's own words plus
+// the neighbouring lanes' edge words (warp shuffles), so lanes 1..30 produce
+// 16 output cells each (480 per warp).  Box counts B <= (2R+1)^2 <= 121 fit a
+// byte lane, and the interval rule is evaluated four cells at a time with the
+// borrow bit of each lane (rule_swar8).
+// ---------------------------------------------------------------------------
+constexpr int kStripOut = 480;  // output columns per warp
+constexpr int kQD = 4;          // prefetch depth (rows) of the entering-row queue
+
+__device__ __forceinline__ uint4 ld_row_chunk(const uint8_t* p) { return __ldg((const uint4*)p); }
+
+__device__ __forceinline__ void v_add(uint32_t (&v)[4], uint4 a) {
+    v[0] += a.x; v[1] += a.y; v[2] += a.z; v[3] += a.w;
+}
+__device__ __forceinline__ void v_slide(uint32_t (&v)[4], uint4 in, uint4 out) {
+    v[0] += in.x - out.x; v[1] += in.y - out.y; v[2] += in.z - out.z; v[3] += in.w - out.w;
+}
+
+// Row box sums for the lane's four output words.  w[0..7] = byte words at
+// offsets -8 .. +28 of the lane's chunk (two words of the left lane, the four
+// own words, two words of the right lane).  Output word m covers cells
+// 4m..4m+3; its sum runs over byte offsets 4m-R .. 4m+R, i.e. w-offsets
+// 4m-R+8 ... 4m+R+8.
+template <int R, int M>
+__device__ __forceinline__ uint32_t row_box_word(const uint32_t* w) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int d = -R; d <= R; ++d) {
+        // offsets are compile-time constants after unrolling
+        const int o = 4 * M + d + 8;
+        const int idx = o >> 2, sh = o & 3;
+        uint32_t x = (sh == 0) ? w[idx] : __byte_perm(w[idx], w[idx + 1], 0x3210 + 0x1111 * sh);
+        acc += x;
+    }
+    return acc;
+}
+
+template <int R>
+__global__ void __launch_bounds__(128)
+k_plain_swar8(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n, int H, size_t pitch,
+              int band_rows, int n_strips, int n_items, RuleSwar8 q) {
+    const int lane = threadIdx.x & 31;
+    const int warps_per_cta = blockDim.x >> 5;
+    const int gwarp = blockIdx.x * warps_per_cta + (threadIdx.x >> 5);
+    const int gwarps = gridDim.x * warps_per_cta;
+
+    for (int item = gwarp; item < n_items; item += gwarps) {
+        const int strip = item % n_strips;
+        const int band = item / n_strips;
+        const int r0 = band * band_rows;
+        const int r1 = min(r0 + band_rows, n);
+        const int x = strip * kStripOut - 16 + 16 * lane;      // inner column of this lane's chunk
+        const bool loads = x < n + 16;                          // chunks past that feed no output
+        const bool outputs = lane >= 1 && lane <= 30 && x < n;
+        const uint8_t* col = cur + (size_t)H + (loads ? x : 0);
+        auto rowp = [&](int r) { return col + (size_t)(H + r) * pitch; };
+        const int rmax = n - 1 + R;                             // last frame-inner row any window needs
+
+        uint32_t V[4] = {0u, 0u, 0u, 0u};
+        if (loads) {
+#pragma unroll 1
+            for (int dy = -R; dy <= R; ++dy) v_add(V, ld_row_chunk(rowp(r0 + dy)));
+        }
+        uint4 qrow[kQD];
+#pragma unroll
+        for (int t = 0; t < kQD; ++t) {
+            int rr = min(r0 + R + 1 + t, rmax);
+            qrow[t] = loads ? ld_row_chunk(rowp(rr)) : make_uint4(0, 0, 0, 0);
+        }
+
+        for (int r = r0; r < r1; r += kQD) {
+#pragma unroll
+            for (int t = 0; t < kQD; ++t) {
+                const int rr = r + t;
+                if (rr < r1) {
+                    uint32_t w[8];
+                    w[0] = __shfl_up_sync(0xffffffffu, V[2], 1);
+                    w[1] = __shfl_up_sync(0xffffffffu, V[3], 1);
+                    w[2] = V[0]; w[3] = V[1]; w[4] = V[2]; w[5] = V[3];
+                    w[6] = __shfl_down_sync(0xffffffffu, V[0], 1);
+                    w[7] = __shfl_down_sync(0xffffffffu, V[1], 1);
+                    if (outputs) {
+                        uint4 c = ld_row_chunk(rowp(rr));
+                        uint4 o;
+                        o.x = rule_swar8(row_box_word<R, 0>(w), c.x, q);
+                        o.y = rule_swar8(row_box_word<R, 1>(w), c.y, q);
+                        o.z = rule_swar8(row_box_word<R, 2>(w), c.z, q);
+                        o.w = rule_swar8(row_box_word<R, 3>(w), c.w, q);
+                        uint8_t* dst = nxt + (size_t)(H + rr) * pitch + H + x;
+                        if (x + 16 <= n) {
+                            *(uint4*)dst = o;
+                        } else {
+                            const uint8_t* ob = (const uint8_t*)&o;
+                            for (int j = 0; j < n - x; ++j) dst[j] = ob[j];
+                        }
+                    }
+                    if (loads) {
+                        uint4 out = ld_row_chunk(rowp(rr - R));
+                        v_slide(V, qrow[t], out);
+                        int nr = min(rr + R + 1 + kQD, rmax);
+                        qrow[t] = ld_row_chunk(rowp(nr));
+                    }
+                }
+            }
+        }
+    }
+}
+
+bool plain_swar8_supported(int radius) { return radius >= 1 && radius <= 5; }
+
+int plain_swar8_band_rows(int n, int device) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int strips = (n + kStripOut - 1) / kStripOut;
+    // ~8 work items per resident warp slot (16 warps/SM assumed) for balance,
+    // but never fewer than 32 rows per band (the window start-up costs 2R+1 rows).
+    long long target_items = (long long)sms * 16 * 8;
+    int bands = (int)std::max<long long>(1, target_items / std::max(strips, 1));
+    int rows = (n + bands - 1) / bands;
+    rows = std::max(32, std::min(rows, 512));
+    return rows;
+}
+
+template <int R>
+static cudaError_t launch_swar8_r(const Frame& cur, const Frame& nxt, const RuleSwar8& q, int band_rows,
+                                  cudaStream_t s) {
+    const int n = cur.n;
+    const int strips = (n + kStripOut - 1) / kStripOut;
+    const int bands = (n + band_rows - 1) / band_rows;
+    const int items = strips * bands;
+    const int warps_per_cta = 4;
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_plain_swar8<R>, warps_per_cta * 32, 0);
+    if (per_sm < 1) per_sm = 1;
+    int ctas = std::min((items + warps_per_cta - 1) / warps_per_cta, sms * per_sm);
+    k_plain_swar8<R><<<ctas, warps_per_cta * 32, 0, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch, band_rows,
+                                                         strips, items, q);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows,
+                               cudaStream_t s) {
+    RuleSwar8 q = make_rule_swar8(rule);
+    switch (rule.radius) {
+        case 1: return launch_swar8_r<1>(cur, nxt, q, band_rows, s);
+        case 2: return launch_swar8_r<2>(cur, nxt, q, band_rows, s);
+        case 3: return launch_swar8_r<3>(cur, nxt, q, band_rows, s);
+        case 4: return launch_swar8_r<4>(cur, nxt, q, band_rows, s);
+        case 5: return launch_swar8_r<5>(cur, nxt, q, band_rows, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K1 generic path (any R >= 1), two passes:
+//  (a) k_vsum: V[r][c] = sum_{dy=-R..R} X[r+dy][c] for every frame column c,
+//      as uint16 (two cells per 32-bit register, SWAR), one thread per 4
+//      columns sliding down a band of rows;
+//  (b) k_hsum_rule: per row, an exclusive prefix of V over the window
+//      [H+j0-R, H+j0+T+R) in shared memory, B = P[q+2R+1] - P[q], k = B - s,
+//      interval rule, one output byte per cell.
+// Work per cell is independent of R.
+// ---------------------------------------------------------------------------
+constexpr int kVBand = 128;
+
+__global__ void k_vsum(const uint8_t* __restrict__ X, uint16_t* __restrict__ V, int n, int H, size_t pitch,
+                       int R, int nwords) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r0 = blockIdx.y * kVBand;
+    if (w >= nwords || r0 >= n) return;
+    const int r1 = min(r0 + kVBand, n);
+    const uint8_t* col = X + 4 * (size_t)w;
+    auto ldw = [&](int r) { return __ldg((const uint32_t*)(col + (size_t)(H + r) * pitch)); };
+    uint32_t lo = 0, hi = 0;
+    for (int dy = -R; dy <= R; ++dy) {
+        uint32_t x = ldw(r0 + dy);
+        lo += __byte_perm(x, 0, 0x4140);
+        hi += __byte_perm(x, 0, 0x4342);
+    }
+    uint16_t* out = V + 4 * (size_t)w;
+    for (int r = r0; r < r1; ++r) {
+        *(uint2*)(out + (size_t)r * pitch) = make_uint2(lo, hi);
+        if (r + 1 < r1) {
+            uint32_t a = ldw(r + R + 1), b = ldw(r - R);
+            lo += __byte_perm(a, 0, 0x4140) - __byte_perm(b, 0, 0x4140);
+            hi += __byte_perm(a, 0, 0x4342) - __byte_perm(b, 0, 0x4342);
+        }
+    }
+}
+
+constexpr int kHT = 1024;      // output columns per CTA row segment
+constexpr int kHThreads = 256;
+constexpr int kHRows = 4;      // rows per CTA
+
+__global__ void __launch_bounds__(kHThreads)
+k_hsum_rule(const uint8_t* __restrict__ X, const uint16_t* __restrict__ V, uint8_t* __restrict__ Y, int n,
+            int H, size_t pitch, Rule rule) {
+    extern __shared__ int P[];  // L + 1 entries, L = kHT + 2R
+    __shared__ int warp_tot[kHThreads / 32];
+    const int R = rule.radius;
+    const int j0 = blockIdx.x * kHT;
+    const int L = kHT + 2 * R;
+    const int per = (L + kHThreads - 1) / kHThreads;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int s1 = H + j0 - R;  // frame column of P index 0
+
+    for (int rr = 0; rr < kHRows; ++rr) {
+        const int r = blockIdx.y * kHRows + rr;
+        if (r >= n) break;
+        const uint16_t* vrow = V + (size_t)r * pitch;
+        // thread-local sequential sums over [tid*per, tid*per+per)
+        int a0 = tid * per;
+        int local = 0;
+        for (int u = 0; u < per; ++u) {
+            int t = a0 + u;
+            if (t < L) {
+                int c = s1 + t;
+                local += (c < (int)pitch) ? vrow[c] : 0;
+            }
+        }
+        // block exclusive scan of `local`
+        int incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) warp_tot[wid] = incl;
+        __syncthreads();
+        int wpre = 0;
+        for (int k = 0; k < wid; ++k) wpre += warp_tot[k];
+        int run = wpre + incl - local;  // exclusive prefix at a0
+        for (int u = 0; u < per; ++u) {
+            int t = a0 + u;
+            if (t < L) {
+                P[t] = run;
+                int c = s1 + t;
+                run += (c < (int)pitch) ? vrow[c] : 0;
+            }
+        }
+        if (tid == kHThreads - 1) P[L] = run;  // last thread's running total is the grand total
+        __syncthreads();
+        // outputs: 4 cells per thread
+        for (int q0 = tid * 4; q0 < kHT; q0 += kHThreads * 4) {
+            int j = j0 + q0;
+            if (j >= n) break;
+            const uint8_t* xr = X + (size_t)(H + r) * pitch + H + j;
+            uint32_t sw = *(const uint32_t*)xr;
+            uint32_t ow = 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                int q = q0 + u;
+                int B = P[q + 2 * R + 1] - P[q];
+                int sv = (sw >> (8 * u)) & 0xff;
+                int nv = rule_scalar(B - sv, sv, rule.smin, rule.smax, rule.bmin, rule.bmax);
+                ow |= (uint32_t)nv << (8 * u);
+            }
+            uint8_t* yr = Y + (size_t)(H + r) * pitch + H + j;
+            if (j + 4 <= n) {
+                *(uint32_t*)yr = ow;
+            } else {
+                for (int u = 0; u < n - j; ++u) yr[u] = (uint8_t)((ow >> (8 * u)) & 0xff);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+size_t plain_generic_vbuf_bytes(int n, size_t pitch) { return (size_t)n * pitch * sizeof(uint16_t); }
+
+cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, uint16_t* vbuf,
+                                 cudaStream_t s) {
+    const int n = cur.n;
+    const int nwords = (int)(cur.pitch / 4);
+    dim3 gv((nwords + 127) / 128, (n + kVBand - 1) / kVBand);
+    k_vsum<<<gv, 128, 0, s>>>(cur.base, vbuf, n, cur.H, cur.pitch, rule.radius, nwords);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int L = kHT + 2 * rule.radius;
+    size_t smem = (size_t)(L + 1) * sizeof(int);
+    if (smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(k_hsum_rule, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 gh((n + kHT - 1) / kHT, (n + kHRows - 1) / kHRows);
+    k_hsum_rule<<<gh, kHThreads, smem, s>>>(cur.base, vbuf, nxt.base, n, cur.H, cur.pitch, rule);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// K6: population and comparison over inner cells.
+// ---------------------------------------------------------------------------
+__global__ void k_population(const uint8_t* __restrict__ g, int n, int H, size_t pitch,
+                             unsigned long long* out) {
+    unsigned long long acc = 0;
+    const long long total = (long long)n * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(t / n), j = (int)(t % n);
+        acc += g[(size_t)(H + i) * pitch + H + j];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+}
+
+__global__ void k_compare(const uint8_t* __restrict__ g, int n, int H, size_t pitch,
+                          const uint8_t* __restrict__ other, size_t opitch, unsigned long long* out) {
+    unsigned long long cnt = 0, first = ~0ull;
+    const long long total = (long long)n * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(t / n), j = (int)(t % n);
+        if (g[(size_t)(H + i) * pitch + H + j] != other[(size_t)i * opitch + j]) {
+            ++cnt;
+            if ((unsigned long long)t < first) first = (unsigned long long)t;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+        unsigned long long f2 = __shfl_down_sync(0xffffffffu, first, o);
+        first = f2 < first ? f2 : first;
+    }
+    if ((threadIdx.x & 31) == 0 && cnt) {
+        atomicAdd(out, cnt);
+        atomicMin(out + 1, first);
+    }
+}
+
+cudaError_t launch_population(const Frame& f, unsigned long long* scratch, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    long long total = (long long)f.n * f.n;
+    int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    k_population<<<blocks, 256, 0, s>>>(f.base, f.n, f.H, f.pitch, scratch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compare(const Frame& f, const uint8_t* other, size_t other_pitch,
+                           unsigned long long* scratch, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(scratch + 1, 0xff, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    long long total = (long long)f.n * f.n;
+    int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    k_compare<<<blocks, 256, 0, s>>>(f.base, f.n, f.H, f.pitch, other, other_pitch, scratch);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Dense n x n <-> frame inner copies (device to device).
+// ---------------------------------------------------------------------------
+__global__ void k_copy_in(uint8_t* __restrict__ g, int n, int H, size_t pitch, const uint8_t* __restrict__ src,
+                          size_t sp) {
+    const long long total = (long long)n * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(t / n), j = (int)(t % n);
+        g[(size_t)(H + i) * pitch + H + j] = src[(size_t)i * sp + j] ? 1 : 0;
+    }
+}
+
+__global__ void k_copy_out(const uint8_t* __restrict__ g, int n, int H, size_t pitch, uint8_t* __restrict__ dst,
+                           size_t dp) {
+    const long long total = (long long)n * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(t / n), j = (int)(t % n);
+        dst[(size_t)i * dp + j] = g[(size_t)(H + i) * pitch + H + j];
+    }
+}
+
+cudaError_t launch_copy_in(const Frame& f, const uint8_t* src, size_t src_pitch, cudaStream_t s) {
+    long long total = (long long)f.n * f.n;
+    int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+    k_copy_in<<<blocks, 256, 0, s>>>(f.base, f.n, f.H, f.pitch, src, src_pitch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_copy_out(const Frame& f, uint8_t* dst, size_t dst_pitch, cudaStream_t s) {
+    long long total = (long long)f.n * f.n;
+    int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+    k_copy_out<<<blocks, 256, 0, s>>>(f.base, f.n, f.H, f.pitch, dst, dst_pitch);
+    return cudaGetLastError();
+}
+
+}  // namespace ltl

@@ -1,0 +1,73 @@
+// ltl_kernels.h -- host-side launchers of the libltl_b200 kernels (internal).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ltl_internal.cuh"
+
+namespace ltl {
+
+// K5: refresh the torus halo of a frame (every halo cell <- its inner source).
+cudaError_t launch_halo_fill(const Frame& f, cudaStream_t s);
+
+// K1 fast path: SWAR 8-bit lanes, warp-shuffle row sums; R <= 5.
+bool plain_swar8_supported(int radius);
+cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows,
+                               cudaStream_t s);
+int plain_swar8_band_rows(int n, int device);
+
+// K1 generic path (any R): vertical sliding sums into `vbuf` (uint16, n rows x
+// pitch entries), then a prefix-sum horizontal pass with the rule fused.
+cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, uint16_t* vbuf,
+                                 cudaStream_t s);
+size_t plain_generic_vbuf_bytes(int n, size_t pitch);
+
+// K6: population and comparison over the inner n x n cells.  `scratch` holds
+// two uint64 (count, first index) in device memory.
+cudaError_t launch_population(const Frame& f, unsigned long long* scratch, cudaStream_t s);
+cudaError_t launch_compare(const Frame& f, const uint8_t* other, size_t other_pitch,
+                           unsigned long long* scratch, cudaStream_t s);
+
+// Copies between a dense n x n grid (pitch bytes per row) and a frame's inner cells.
+cudaError_t launch_copy_in(const Frame& f, const uint8_t* src, size_t src_pitch, cudaStream_t s);
+cudaError_t launch_copy_out(const Frame& f, uint8_t* dst, size_t dst_pitch, cudaStream_t s);
+
+// K3: bit-packed variant.  Packed frame: 32-bit words, cell (i, j) is bit j % 32
+// of word j / 32 (LSB first; two consecutive words are one little-endian uint64
+// of the PACK codec).  Inner row i is frame row HR + i, inner word w is frame
+// column HW + w; halo bits hold torus copies, like the byte frame.
+struct PackedFrame {
+    uint32_t* words;
+    int n;          // cells per side
+    int nw;         // inner words per row = ceil(n / 32)
+    int HR;         // halo rows (>= R + 1)
+    int HW;         // halo words on each side (1: radius <= 32)
+    size_t wpitch;  // words per frame row
+};
+bool packed_supported(int n, int radius);
+cudaError_t launch_packed_step(const PackedFrame& cur, const PackedFrame& nxt, const Rule& rule,
+                               cudaStream_t s);
+cudaError_t launch_packed_halo(const PackedFrame& f, cudaStream_t s);
+cudaError_t launch_pack_frame(const Frame& src, const PackedFrame& dst, cudaStream_t s);
+cudaError_t launch_unpack_frame(const PackedFrame& src, const Frame& dst, cudaStream_t s);
+cudaError_t launch_pack(const uint8_t* cells, size_t cell_pitch, int rows, int cols, uint64_t* words,
+                        size_t word_pitch_words, cudaStream_t s);
+cudaError_t launch_unpack(const uint64_t* words, size_t word_pitch_words, int rows, int cols, uint8_t* cells,
+                          size_t cell_pitch, cudaStream_t s);
+
+// K2: tcgen05 banded-product step.
+struct TensorPlan;
+bool tensor_supported(int n, int radius, char* why, size_t why_len);
+TensorPlan* tensor_plan_create(const Frame& a, const Frame& b, const Rule& rule, int device, char* why,
+                               size_t why_len);
+void tensor_plan_destroy(TensorPlan* p);
+int tensor_plan_depth(const TensorPlan* p);
+int tensor_plan_operand_bits(const TensorPlan* p);
+int tensor_plan_halo_needed(int radius);
+// Advance one pass (tensor_plan_depth generations) from frame `src_is_a ? a : b`.
+cudaError_t launch_tensor_pass(TensorPlan* p, bool src_is_a, cudaStream_t s);
+unsigned int* tensor_plan_error_flag(TensorPlan* p);
+
+}  // namespace ltl

@@ -1,0 +1,211 @@
+"""GPU parity: every variant of libltl_b200, called through its C ABI, against
+the reference's golden vectors and the CPU restatement oracle.  Bit-exact.
+
+Marked `gpu`: needs a CUDA device and the built cat_cpu_b200/libltl_b200.so.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.goldutil import sha, describe_mismatch
+
+pytestmark = pytest.mark.gpu
+
+C = None
+
+
+def setup_module(module):
+    global C
+    import cat_cpu_b200 as _C
+    C = _C
+    O.set_threads(os.cpu_count() or 8)
+
+
+VARIANTS = ["plain", "packed"]
+VCODE = {"plain": 0, "tensor": 1, "packed": 2}
+
+
+def supported(variant, n, r):
+    if variant == "packed":
+        return r <= 32 and n >= r
+    if variant == "tensor":
+        return r <= 127 and n >= r
+    return n >= r
+
+
+def make(variant, n, r, rule):
+    return C.CUDASolver(n, r, rule, variant=VCODE[variant])
+
+
+def run_golden_case(variant, c, max_step=None):
+    n, r, rule = c["n"], c["radius"], tuple(c["rule"])
+    g0 = C.start_grid(n, c["seed"], c["density"], c["gen_threads"])
+    assert sha(g0) == c["checkpoints"][0]["sha256"]
+    s = make(variant, n, r, rule)
+    try:
+        s.setState(g0)
+        done = 0
+        for cp in c["checkpoints"][1:]:
+            if max_step is not None and cp["step"] > max_step:
+                break
+            s.doSteps(cp["step"] - done)
+            done = cp["step"]
+            got = s.getCurrentState()
+            if sha(got) != cp["sha256"]:
+                want = O.run(g0, r, rule, done) if n * n <= 4096 * 4096 else None
+                msg = describe_mismatch(got, want) if want is not None else "sha differs"
+                pytest.fail(f"{variant} {c['name']} step {done}: {msg}")
+            assert s.population() == cp["population"]
+    finally:
+        s.close()
+
+
+SMALL_CASES = None
+
+
+def small_case_names(golden):
+    return sorted(k for k, c in golden.items() if c["n"] <= 1100)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_golden_small(golden, variant):
+    ran = 0
+    for name in small_case_names(golden):
+        c = golden[name]
+        if not supported(variant, c["n"], c["radius"]):
+            continue
+        run_golden_case(variant, c)
+        ran += 1
+    assert ran >= 20
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_golden_config2_16384(golden, variant):
+    """16384^2, seed 1, R=5 Bosco: steps 1, 10, 100, 1000 against the reference."""
+    run_golden_case(variant, golden["config2_bosco_r5_n16384_amx16"])
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_random_vs_oracle_every_step(variant):
+    rng = np.random.default_rng(11 + VCODE[variant])
+    for trial in range(24):
+        r = int(rng.choice([1, 2, 3, 4, 5, 6, 7, 8, 11, 16, 17, 24, 32, 40, 64]))
+        if not supported(variant, 10 ** 6, r):
+            continue
+        n = int(rng.integers(max(r, 1), max(r + 2, 4 * r + 70)))
+        N = (2 * r + 1) ** 2
+        d = float(rng.uniform(0.2, 0.6))
+        lo = int(rng.integers(0, N // 2))
+        rule = (lo, lo + int(rng.integers(0, N // 2)), int(rng.integers(0, N // 2)), int(rng.integers(N // 3, N)))
+        g = (rng.random((n, n)) < d).astype(np.uint8)
+        s = make(variant, n, r, rule)
+        try:
+            s.setState(g)
+            for step in range(4):
+                g = O.step(g, r, rule)
+                s.doStep()
+                got = s.getCurrentState()
+                assert np.array_equal(got, g), f"{variant} n={n} r={r} rule={rule} step {step + 1}: " + \
+                    describe_mismatch(got, g)
+        finally:
+            s.close()
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_counts_near_thresholds_r5(variant):
+    """Every count value 0..120 sits on a threshold at least once: sweep rules over
+    a dense random grid so that an off-by-one anywhere in the count flips cells."""
+    n, r = 509, 5
+    g = (np.random.default_rng(3).random((n, n)) < 0.5).astype(np.uint8)
+    for t in range(0, 121, 7):
+        rule = (t, t + 3, t + 1, t + 2)
+        s = make(variant, n, r, rule)
+        try:
+            s.setState(g)
+            s.doStep()
+            want = O.step(g, r, rule)
+            got = s.getCurrentState()
+            assert np.array_equal(got, want), f"{variant} rule {rule}: " + describe_mismatch(got, want)
+        finally:
+            s.close()
+
+
+def test_population_and_compare_device():
+    import torch
+    n = 777
+    g = C.start_grid(n, 5, 0.4, 1)
+    s = make("plain", n, 5, O.BOSCO_R5)
+    try:
+        s.setState(g)
+        assert s.population() == int(g.sum())
+        dev = torch.from_numpy(g).cuda()
+        mm, first = s.compare_device(dev.data_ptr(), n)
+        assert (mm, first) == (0, -1)
+        g2 = g.copy()
+        g2[3, 4] ^= 1
+        g2[100, 200] ^= 1
+        dev2 = torch.from_numpy(g2).cuda()
+        torch.cuda.synchronize()
+        mm, first = s.compare_device(dev2.data_ptr(), n)
+        assert mm == 2 and first == 3 * n + 4
+        out = torch.zeros((n, n), dtype=torch.uint8, device="cuda")
+        s.download_device(out.data_ptr(), n)
+        s.synchronize()
+        assert np.array_equal(out.cpu().numpy(), g)
+    finally:
+        s.close()
+
+
+def test_upload_device_and_streams():
+    import torch
+    n = 300
+    g = C.start_grid(n, 9, 0.5, 1)
+    dev = torch.from_numpy(g).cuda()
+    st = torch.cuda.Stream()
+    for variant in VARIANTS:
+        s = make(variant, n, 5, O.BOSCO_R5)
+        try:
+            s.set_stream(st.cuda_stream)
+            s.upload_device(dev.data_ptr(), n)
+            s.doSteps(20)
+            s.synchronize()
+            assert np.array_equal(s.getCurrentState(), O.run(g, 5, O.BOSCO_R5, 20)), variant
+        finally:
+            s.close()
+
+
+def test_pack_codec_roundtrip():
+    import torch
+    import ctypes
+    L = C.lib()
+    rng = np.random.default_rng(2)
+    for rows, cols in [(1, 1), (3, 63), (5, 64), (7, 65), (64, 1000), (129, 4096)]:
+        cells = (rng.random((rows, cols)) < 0.5).astype(np.uint8)
+        d_cells = torch.from_numpy(cells).cuda()
+        nw = (cols + 63) // 64
+        d_words = torch.zeros((rows, nw), dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        C.ltl.check(L.ltl_pack_device(ctypes.c_void_p(d_cells.data_ptr()), cols, rows, cols,
+                                      ctypes.c_void_p(d_words.data_ptr()), nw * 8, None))
+        torch.cuda.synchronize()
+        words = d_words.cpu().numpy().view(np.uint64)
+        want = np.zeros((rows, nw), dtype=np.uint64)
+        for j in range(cols):
+            want[:, j // 64] |= cells[:, j].astype(np.uint64) << np.uint64(j % 64)
+        assert np.array_equal(words, want), (rows, cols)
+        back = torch.zeros((rows, cols), dtype=torch.uint8, device="cuda")
+        C.ltl.check(L.ltl_unpack_device(ctypes.c_void_p(d_words.data_ptr()), nw * 8, rows, cols,
+                                        ctypes.c_void_p(back.data_ptr()), cols, None))
+        torch.cuda.synchronize()
+        assert np.array_equal(back.cpu().numpy(), cells)
+
+
+def test_errors_on_device():
+    with pytest.raises(C.LtlError) as e:
+        C.CUDASolver(64, 40, (1, 2, 3, 4), variant=VCODE["packed"])
+    assert e.value.code == C.ltl.EUNSUPPORTED
+    with pytest.raises(C.LtlError) as e:
+        C.CUDASolver(64, 5, O.BOSCO_R5, device=99)
+    assert e.value.code == C.ltl.ECUDA
