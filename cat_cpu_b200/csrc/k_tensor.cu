@@ -1,15 +1,513 @@
-// k_tensor.cu -- K2 placeholder (replaced by the tcgen05 implementation).
+// k_tensor.cu -- K2: the LtL step as two banded 0/1 matrix products on the
+// 5th-generation tensor cores (tcgen05, kind::i8, accumulators in TMEM).
+//
+// This is the reference's AMX formulation (kezada94/CAT_cpu,
+// src/CellularAutomata/Solvers/AMXSolver16.cpp:63-138 band tiles, :254-309 row
+// sums X*B, :322-384 column sums + rule) re-designed for sm_100a:
+//   - one CTA owns a tile of Tr x Tc output cells.  TMA brings the halo'd input
+//     tile X (128 rows x 256 bytes, two 128-byte swizzle atoms) into shared memory;
+//   - product 1:  H = X * B_h   (row sums; M = 128 tile rows, N = 32-column
+//     chunks, K = a 64-column window; u8 x u8 -> s32 in TMEM).  B_h is the 0/1
+//     band |k - PADC - n| <= R, built once per CTA in shared memory;
+//   - H (<= 2R+1) is read back with tcgen05.ld, re-quantised to u8 and stored
+//     as the MN-major B operand of
+//   - product 2:  C = B_v * H   (column sums; M = 128, N = Tc, K = 128) with the
+//     band B_v[m][k] = [m <= k <= m + 2R], so the reference's transposed
+//     scatter between the two products (AMXSolver.cpp:321-325) disappears;
+//   - epilogue: C is the box count including the centre, the birth/survival
+//     interval rule (HostSolver.tpp:47-73, k = C - centre) is applied four
+//     cells per register, and the uint8 result goes straight to global memory.
+// Exactness: inputs are 0/1, H <= 2R+1 <= 255 fits u8, C <= (2R+1)^2 in s32.
+//
+// Every wait on an mbarrier is bounded (globaltimer); on timeout the kernel
+// sets a bit in an error word that the host reads (ltl_synchronize), finishes
+// waiting for its own TMA copy (also bounded), frees its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
 #include <cstdio>
+#include <cstring>
+
 #include "ltl_kernels.h"
+
 namespace ltl {
-struct TensorPlan { unsigned int* err; };
-bool tensor_supported(int, int, char* why, size_t n) { snprintf(why, n, "not built yet"); return false; }
-TensorPlan* tensor_plan_create(const Frame&, const Frame&, const Rule&, int, char* why, size_t n) {
-    snprintf(why, n, "not built yet"); return nullptr; }
-void tensor_plan_destroy(TensorPlan*) {}
-int tensor_plan_depth(const TensorPlan*) { return 1; }
-int tensor_plan_operand_bits(const TensorPlan*) { return 0; }
-int tensor_plan_halo_needed(int r) { return halo_for(r, 1); }
-cudaError_t launch_tensor_pass(TensorPlan*, bool, cudaStream_t) { return cudaErrorNotSupported; }
-unsigned int* tensor_plan_error_flag(TensorPlan* p) { return p ? p->err : nullptr; }
+
+// ---------------------------------------------------------------------------
+// PTX helpers (sm_100a)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait for `phase` of `bar`: false after `limit_ns` of wall time.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint64_t limit_ns) {
+    if (mbar_try(bar, phase)) return true;
+    const uint64_t t0 = globaltimer();
+    while (true) {
+        if (mbar_try(bar, phase)) return true;
+        if (globaltimer() - t0 > limit_ns) return false;
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
+            "r"(smem_u32(dst)),
+        "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// 32 consecutive TMEM columns of this thread's lane (32-bit each).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Shared-memory matrix descriptors (tcgen05 "version 1" format).
+// K-major, 128-byte swizzle: 8-row atoms of 1024 B (SBO), LBO unused.
+__device__ __forceinline__ uint64_t desc_k_sw128(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) |
+           ((uint64_t)1u << 46) | ((uint64_t)2u << 61);
+}
+// No swizzle ("interleave"): 8 x 16-byte core matrices stored as 128 contiguous
+// bytes; `lbo` / `sbo` are the byte strides between core matrices along the
+// leading / strided dimension.
+__device__ __forceinline__ uint64_t desc_noswz(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1u << 46);
+}
+
+// Instruction descriptor: kind::i8, u8 x u8 -> s32, M = 128.
+__host__ __device__ constexpr uint32_t idesc_u8(int N, bool b_mn_major) {
+    return (2u << 4)                       // D format s32
+           | (0u << 7) | (0u << 10)        // A, B unsigned 8-bit
+           | (0u << 15)                    // A K-major
+           | ((b_mn_major ? 1u : 0u) << 16)
+           | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+// ---------------------------------------------------------------------------
+// Tile geometry
+// ---------------------------------------------------------------------------
+constexpr int kAtomBytes = 128 * 128;  // one 128-row x 128-byte swizzle atom
+constexpr int kAtoms = 2;              // X tile = 128 rows x 256 columns
+constexpr int kXCols = 128 * kAtoms;
+constexpr int kN1 = 32;                // product-1 column chunk
+constexpr int kThreads = 128;
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any legitimate wait
+
+struct TensorParams {
+    uint8_t* out;      // destination frame base
+    int n, H;
+    long long pitch;
+    int R, PADC;       // radius, column halo of the tile (multiple of 16, >= R)
+    int Tr, Tc;        // output rows / columns per tile
+    int K1c;           // product-1 K window (multiple of 32)
+    int tiles_x, tiles_y;
+    RuleSwar8 q;       // rule on the box count (used when (2R+1)^2 <= 127)
+    int slo, shi, blo, bhi;  // rule on the box count, scalar form
+    unsigned int* err;
+};
+
+struct SmemLayout {
+    int x_off, hs_off, bh_off, bv_off, bar_off, tmem_off, total;
+};
+
+__host__ __device__ inline SmemLayout smem_layout(int Tc, int K1c) {
+    SmemLayout L{};
+    int o = 0;
+    L.x_off = o;
+    o += kAtoms * kAtomBytes;               // 32 KB, 1024-aligned
+    L.hs_off = o;
+    o += 128 * Tc;                          // H as u8, MN-major
+    L.bh_off = o;
+    o += kN1 * K1c;                         // B_h
+    L.bv_off = o;
+    o += 128 * 128;                         // B_v
+    L.bar_off = o;
+    o += 2 * 8;
+    L.tmem_off = o;
+    o += 16;
+    L.total = o;
+    return L;
+}
+
+__device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    uint32_t lo = __byte_perm(a, b, 0x0040);
+    uint32_t hi = __byte_perm(c, d, 0x0040);
+    return __byte_perm(lo, hi, 0x5410);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const SmemLayout L = smem_layout(p.Tc, p.K1c);
+    uint8_t* xs = smem + L.x_off;
+    uint8_t* hs = smem + L.hs_off;
+    uint8_t* bh = smem + L.bh_off;
+    uint8_t* bv = smem + L.bv_off;
+    uint64_t* bars = (uint64_t*)(smem + L.bar_off);  // [0] TMA, [1] MMA
+    uint32_t* tmem_slot = (uint32_t*)(smem + L.tmem_off);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tile = blockIdx.x;
+    const int ty = tile / p.tiles_x, tx = tile % p.tiles_x;
+    const int r0 = ty * p.Tr, c0 = tx * p.Tc;
+    const int R = p.R, PADC = p.PADC, Tc = p.Tc, K1c = p.K1c;
+    constexpr uint32_t kTmemCols = 256;
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+        mbar_expect_tx(&bars[0], kAtoms * kAtomBytes);
+        const int y = p.H + r0 - R;
+        const int x = p.H + c0 - PADC;
+#pragma unroll
+        for (int a = 0; a < kAtoms; ++a) tma_load_2d(xs + a * kAtomBytes, &xmap, &bars[0], x + 128 * a, y);
+    }
+    // Band matrices (no-swizzle K-major layouts: [k / 16][row][16 bytes]).
+    // B_h[n][k] = [|k - PADC - n| <= R], n < 32, k < K1c
+    for (int idx = tid; idx < kN1 * K1c; idx += kThreads) {
+        const int k = idx / kN1, n = idx % kN1;
+        const int d = k - PADC - n;
+        bh[((k >> 4) * kN1 + n) * 16 + (k & 15)] = (d >= -R && d <= R) ? 1 : 0;
+    }
+    // B_v[m][k] = [m <= k <= m + 2R], m, k < 128
+    for (int idx = tid; idx < 128 * 128; idx += kThreads) {
+        const int k = idx / 128, m = idx % 128;
+        bv[((k >> 4) * 128 + m) * 16 + (k & 15)] = (k >= m && k <= m + 2 * R) ? 1 : 0;
+    }
+    fence_proxy_async();
+    __syncthreads();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+
+    // ---- product 1: H = X * B_h --------------------------------------------
+    if (tid == 0) {
+        ok = mbar_wait(&bars[0], 0, kWaitLimitNs);
+        if (ok) {
+            tc_fence_after();
+            const uint32_t xa = smem_u32(xs), ba = smem_u32(bh);
+            const uint32_t id1 = idesc_u8(kN1, false);
+            for (int n0 = 0; n0 < Tc; n0 += kN1) {
+                for (int s = 0; s < K1c / 32; ++s) {
+                    const int col = n0 + 32 * s;  // X column of this K step
+                    const uint32_t a_addr = xa + (col >> 7) * kAtomBytes + (col & 127);
+                    const uint64_t ad = desc_k_sw128(a_addr);
+                    const uint64_t bd = desc_noswz(ba + s * 2 * kN1 * 16, kN1 * 16, 128);
+                    mma_i8(tmem + n0, ad, bd, id1, s > 0 ? 1u : 0u);
+                }
+            }
+            mma_commit(&bars[1]);
+        } else {
+            atomicOr(p.err, 1u);
+        }
+    }
+    __syncthreads();
+    // (if thread 0 gave up on the TMA wait it issued nothing and this wait times out too)
+    ok = mbar_wait(&bars[1], 0, kWaitLimitNs);
+    if (!ok) atomicOr(p.err, 2u);
+    if (__syncthreads_and(ok)) {
+        tc_fence_after();
+        // ---- re-quantise H to u8 (MN-major B operand of product 2) ---------
+        const int k = warp * 32 + lane;  // H row = TMEM lane
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int cb = 0; cb < Tc; cb += 32) {
+            uint32_t v[32];
+            tmem_ld32(trow + cb, v);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint4 w;
+                w.x = pack4(v[16 * h + 0], v[16 * h + 1], v[16 * h + 2], v[16 * h + 3]);
+                w.y = pack4(v[16 * h + 4], v[16 * h + 5], v[16 * h + 6], v[16 * h + 7]);
+                w.z = pack4(v[16 * h + 8], v[16 * h + 9], v[16 * h + 10], v[16 * h + 11]);
+                w.w = pack4(v[16 * h + 12], v[16 * h + 13], v[16 * h + 14], v[16 * h + 15]);
+                const int chunk = (cb >> 4) + h;
+                *(uint4*)(hs + (chunk * 128 + k) * 16) = w;
+            }
+        }
+        fence_proxy_async();
+        tc_fence_before();
+        __syncthreads();
+        // ---- product 2: C = B_v * H  (into the same TMEM columns) ------------
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t va = smem_u32(bv), ha = smem_u32(hs);
+            const uint32_t id2 = idesc_u8(Tc, true);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const uint64_t ad = desc_noswz(va + s * 2 * 128 * 16, 128 * 16, 128);
+                const uint64_t bd = desc_noswz(ha + s * 32 * 16, 128, 128 * 16);
+                mma_i8(tmem, ad, bd, id2, s > 0 ? 1u : 0u);
+            }
+            mma_commit(&bars[1]);
+        }
+        __syncwarp();
+        ok = mbar_wait(&bars[1], 1, kWaitLimitNs);
+        if (!ok) atomicOr(p.err, 4u);
+        if (ok) {
+            tc_fence_after();
+            // ---- epilogue: rule, store -------------------------------------
+            const int m = warp * 32 + lane;      // output row within the tile
+            const int gi = r0 + m;               // grid row
+            const bool row_ok = (m < p.Tr) && (gi < p.n);
+            const int xr = m + R;                // X tile row of the centre cell
+            const uint8_t* xrow = xs + xr * 128;
+            uint8_t* orow = p.out + (size_t)(p.H + gi) * (size_t)p.pitch + p.H + c0;
+            const bool small = (2 * R + 1) * (2 * R + 1) <= 127;
+            for (int cb = 0; cb < Tc; cb += 32) {
+                uint32_t v[32];
+                tmem_ld32(trow + cb, v);
+                if (!row_ok) continue;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int xc = PADC + cb + 16 * h;  // X column of these 16 cells
+                    const int atom = xc >> 7, ch = (xc & 127) >> 4;
+                    const uint4 s4 = *(const uint4*)(xrow + atom * kAtomBytes + ((ch ^ (xr & 7)) << 4));
+                    const uint32_t sw[4] = {s4.x, s4.y, s4.z, s4.w};
+                    uint32_t o[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const uint32_t* b = &v[16 * h + 4 * q];
+                        if (small) {
+                            o[q] = rule_swar8(pack4(b[0], b[1], b[2], b[3]), sw[q], p.q);
+                        } else {
+                            uint32_t r = 0;
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                const int B = (int)b[e];
+                                const int sv = (sw[q] >> (8 * e)) & 1;
+                                const int lo = sv ? p.slo : p.blo, hi = sv ? p.shi : p.bhi;
+                                r |= (uint32_t)((B >= lo) & (B <= hi)) << (8 * e);
+                            }
+                            o[q] = r;
+                        }
+                    }
+                    const int gj = c0 + cb + 16 * h;
+                    if (gj + 16 <= p.n) {
+                        *(uint4*)(orow + cb + 16 * h) = make_uint4(o[0], o[1], o[2], o[3]);
+                    } else if (gj < p.n) {
+                        for (int e = 0; e < p.n - gj; ++e)
+                            orow[cb + 16 * h + e] = (uint8_t)((o[e >> 2] >> (8 * (e & 3))) & 0xff);
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        // never leave with the TMA copy still in flight into this CTA's shared memory
+        if (lane == 0 && !mbar_wait(&bars[0], 0, kWaitLimitNs)) atomicOr(p.err, 8u);
+        __syncwarp();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+struct TensorPlan {
+    CUtensorMap map[2];  // source frame a / b
+    TensorParams prm[2]; // destination frame b / a
+    int smem_bytes;
+    int grid;
+    unsigned int* err;
+};
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+static int pad_for(int R) { return (int)round_up((size_t)R, 16); }
+
+int tensor_plan_halo_needed(int radius) { return std::max(16, pad_for(radius)); }
+
+bool tensor_supported(int n, int radius, char* why, size_t why_len) {
+    if (radius < 1 || radius > 32) {
+        snprintf(why, why_len, "tensor variant supports 1 <= R <= 32 (got %d)", radius);
+        return false;
+    }
+    if (n < radius) {
+        snprintf(why, why_len, "n < R");
+        return false;
+    }
+    return true;
+}
+
+TensorPlan* tensor_plan_create(const Frame& a, const Frame& b, const Rule& rule, int device, char* why,
+                               size_t why_len) {
+    if (!tensor_supported(a.n, rule.radius, why, why_len)) return nullptr;
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+    if (major != 10) {
+        snprintf(why, why_len, "tcgen05 needs an sm_100 device (compute capability %d.x)", major);
+        return nullptr;
+    }
+    auto encode = encode_fn();
+    if (!encode) {
+        snprintf(why, why_len, "cuTensorMapEncodeTiled not available");
+        return nullptr;
+    }
+    TensorPlan* P = new TensorPlan();
+    const int R = rule.radius;
+    const int PADC = pad_for(R);
+    const int Tc = ((kXCols - 2 * PADC) / kN1) * kN1;  // 224 for R <= 16, 192 for R <= 32
+    const int Tr = 128 - 2 * R;
+    const int K1c = (int)round_up((size_t)(kN1 + PADC + R), 32);
+    if (Tc < kN1 || Tr < 1 || K1c > kN1 + 2 * PADC) {
+        snprintf(why, why_len, "no tile shape for R=%d", R);
+        delete P;
+        return nullptr;
+    }
+    const Frame* src[2] = {&a, &b};
+    const Frame* dst[2] = {&b, &a};
+    for (int i = 0; i < 2; ++i) {
+        const Frame& f = *src[i];
+        cuuint64_t gdim[2] = {(cuuint64_t)f.pitch, (cuuint64_t)(f.n + 2 * f.H)};
+        cuuint64_t gstride[1] = {(cuuint64_t)f.pitch};
+        cuuint32_t box[2] = {128, 128};
+        cuuint32_t estride[2] = {1, 1};
+        CUresult cr = encode(&P->map[i], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)f.base, gdim, gstride, box, estride,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (cr != CUDA_SUCCESS) {
+            snprintf(why, why_len, "cuTensorMapEncodeTiled failed (%d)", (int)cr);
+            delete P;
+            return nullptr;
+        }
+        TensorParams& q = P->prm[i];
+        q.out = dst[i]->base;
+        q.n = f.n;
+        q.H = f.H;
+        q.pitch = (long long)f.pitch;
+        q.R = R;
+        q.PADC = PADC;
+        q.Tr = Tr;
+        q.Tc = Tc;
+        q.K1c = K1c;
+        q.tiles_x = (f.n + Tc - 1) / Tc;
+        q.tiles_y = (f.n + Tr - 1) / Tr;
+        q.q = make_rule_swar8(rule);
+        q.slo = rule.smin + 1;
+        q.shi = rule.smax + 1;
+        q.blo = rule.bmin;
+        q.bhi = rule.bmax;
+    }
+    if (cudaMalloc(&P->err, sizeof(unsigned int)) != cudaSuccess) {
+        snprintf(why, why_len, "error-flag allocation failed");
+        delete P;
+        return nullptr;
+    }
+    cudaMemset(P->err, 0, sizeof(unsigned int));
+    for (auto& q : P->prm) q.err = P->err;
+    P->smem_bytes = smem_layout(Tc, K1c).total + 1024;
+    P->grid = P->prm[0].tiles_x * P->prm[0].tiles_y;
+    if (cudaFuncSetAttribute(k_tensor_step, cudaFuncAttributeMaxDynamicSharedMemorySize, P->smem_bytes) !=
+        cudaSuccess) {
+        snprintf(why, why_len, "cannot reserve %d bytes of shared memory", P->smem_bytes);
+        cudaFree(P->err);
+        delete P;
+        return nullptr;
+    }
+    return P;
+}
+
+void tensor_plan_destroy(TensorPlan* p) {
+    if (!p) return;
+    if (p->err) cudaFree(p->err);
+    delete p;
+}
+
+int tensor_plan_depth(const TensorPlan*) { return 1; }
+int tensor_plan_operand_bits(const TensorPlan*) { return 8; }
+unsigned int* tensor_plan_error_flag(TensorPlan* p) { return p ? p->err : nullptr; }
+
+cudaError_t launch_tensor_pass(TensorPlan* p, bool src_is_a, cudaStream_t s) {
+    const int i = src_is_a ? 0 : 1;
+    k_tensor_step<<<p->grid, kThreads, p->smem_bytes, s>>>(p->map[i], p->prm[i]);
+    return cudaGetLastError();
+}
+
+}  // namespace ltl

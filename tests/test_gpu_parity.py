@@ -23,7 +23,7 @@ def setup_module(module):
     O.set_threads(os.cpu_count() or 8)
 
 
-VARIANTS = ["plain", "packed"]
+VARIANTS = ["plain", "packed", "tensor"]
 VCODE = {"plain": 0, "tensor": 1, "packed": 2}
 
 
@@ -31,7 +31,7 @@ def supported(variant, n, r):
     if variant == "packed":
         return r <= 32 and n >= r
     if variant == "tensor":
-        return r <= 127 and n >= r
+        return r <= 32 and n >= r
     return n >= r
 
 
