@@ -18,6 +18,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libltl_b200.so")
+PROG = os.path.join(PKG, "ltl_prog")
+HOST = os.path.join(PKG, "host")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -67,12 +69,25 @@ def build(force=False, jobs=None, verbose=False, ptxas_verbose=False):
     if errors:
         raise RuntimeError("\n".join(errors))
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", "g++", "-o", LIB] + objs + ["-lcudart", "-lpthread"]
+        # static CUDA runtime: the library does not depend on which libcudart.so.12
+        # the host process (e.g. torch) loaded first
+        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", "g++", "-cudart", "static", "-o", LIB] + objs + \
+            ["-lpthread", "-ldl", "-lrt"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed\n{r.stdout}\n{r.stderr}")
+    src = os.path.join(HOST, "ltl_prog.cpp")
+    deps = [src, os.path.join(HOST, "ltl_solver.hpp"), os.path.join(ROOT, "include", "ltl.h"), LIB]
+    if force or not os.path.exists(PROG) or os.path.getmtime(PROG) < max(os.path.getmtime(d) for d in deps):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", HOST, src, "-o", PROG,
+               "-L", PKG, "-lltl_b200", "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"ltl_prog build failed\n{r.stdout}\n{r.stderr}")
     return LIB
 
 

@@ -81,44 +81,46 @@ __device__ __forceinline__ void planes_add(uint32_t (&B)[PB], const uint32_t (&h
     }
 }
 
-// Lanes where lo <= B <= hi (lo, hi in [0, 2^PB); caller folds empty intervals).
+// Lanes where lo <= B <= hi, given the thresholds as per-plane masks (all-ones
+// where the threshold's bit is set); lo, hi < 2^PB.  Two carry chains:
+//   ge = carry out of B + ~lo + 1,  le = carry out of hi + ~B + 1.
 template <int PB>
-__device__ __forceinline__ uint32_t planes_in(const uint32_t (&B)[PB], int lo, int hi) {
-    uint32_t ge = 0xffffffffu, le = 0xffffffffu;  // carry-in of B + ~lo + 1 and hi + ~B + 1
+__device__ __forceinline__ uint32_t planes_in(const uint32_t (&B)[PB], const uint32_t* lm, const uint32_t* hm) {
+    uint32_t ge = 0xffffffffu, le = 0xffffffffu;
 #pragma unroll
     for (int i = 0; i < PB; ++i) {
-        uint32_t b = B[i];
-        uint32_t lm = 0u - (uint32_t)((lo >> i) & 1);
-        uint32_t hm = 0u - (uint32_t)((hi >> i) & 1);
-        ge = (lm & (b & ge)) | (~lm & (b | ge));
-        le = (hm & (~b | le)) | (~hm & (~b & le));
+        const uint32_t b = B[i];
+        ge = (lm[i] & (b & ge)) | (~lm[i] & (b | ge));
+        le = (hm[i] & (~b | le)) | (~hm[i] & (~b & le));
     }
     return ge & le;
 }
 
+constexpr int kMaxPlanes = 16;
+
+// Birth (dead cell, index 0) and survival (live cell, index 1) intervals on the
+// box count B, as per-plane bit masks (kernel parameters, so the comparator
+// reads them from the constant bank).  `keep` is ~0u, or 0 for an empty interval.
 struct PackedRule {
-    int lo0, hi0, lo1, hi1;  // birth (dead cell) and survival (live cell) intervals on B
-    uint32_t empty0, empty1; // ~0u when the interval is empty
+    uint32_t lo[2][kMaxPlanes];
+    uint32_t hi[2][kMaxPlanes];
+    uint32_t keep[2];
 };
 
 static PackedRule make_packed_rule(const Rule& r) {
     const int maxB = (2 * r.radius + 1) * (2 * r.radius + 1);
     PackedRule p{};
-    auto fold = [&](int lo, int hi, int& olo, int& ohi, uint32_t& empty) {
-        lo = std::max(lo, 0);
-        hi = std::min(hi, maxB);
-        if (lo > hi) {
-            olo = 0;
-            ohi = 0;
-            empty = 0xffffffffu;
-        } else {
-            olo = lo;
-            ohi = hi;
-            empty = 0u;
+    const int los[2] = {r.bmin, r.smin + 1};
+    const int his[2] = {r.bmax, r.smax + 1};
+    for (int k = 0; k < 2; ++k) {
+        int lo = std::max(los[k], 0), hi = std::min(his[k], maxB);
+        p.keep[k] = lo > hi ? 0u : 0xffffffffu;
+        if (lo > hi) lo = hi = 0;
+        for (int i = 0; i < kMaxPlanes; ++i) {
+            p.lo[k][i] = ((lo >> i) & 1) ? 0xffffffffu : 0u;
+            p.hi[k][i] = ((hi >> i) & 1) ? 0xffffffffu : 0u;
         }
-    };
-    fold(r.bmin, r.bmax, p.lo0, p.hi0, p.empty0);
-    fold(r.smin + 1, r.smax + 1, p.lo1, p.hi1, p.empty1);
+    }
     return p;
 }
 
@@ -147,29 +149,54 @@ __device__ __forceinline__ void hcount(const uint32_t* __restrict__ row, int fw,
     wallace<2 * R + 1, 0, PH>(x, h);
 }
 
-constexpr int kPackedBand = 64;
+constexpr int kPackedWarps = 4;
+
+// Rows per work item: enough items for ~32 resident warps per SM, but at least
+// 32 rows so that the (2R+1)-row start-up of each band stays a small fraction.
+static int packed_band_rows(int n, int n_wstrips, int sms) {
+    long long want_items = (long long)sms * 32;
+    long long bands = std::max<long long>(1, want_items / std::max(n_wstrips, 1));
+    int rows = (int)((n + bands - 1) / bands);
+    rows = std::max(32, std::min(rows, 256));
+    return (rows + 15) / 16 * 16;
+}
+
+// Shared-memory ring of the last 2R+2 row counts h (PH planes per lane), so each
+// row's horizontal count is computed once on entry and read back on exit.
+template <int R>
+struct PackedRing {
+    static constexpr int PH = bits_for(2 * R + 1);
+    static constexpr int ROWS = 2 * R + 2;
+    static constexpr int BYTES = ROWS * PH * 32 * 4 * kPackedWarps;
+    static constexpr bool fits = BYTES <= 96 * 1024;
+};
 
 template <int R>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kPackedWarps * 32)
 k_packed_step(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int n, int nw, int HR, int HW,
-              size_t wp, int n_wstrips, int n_items, PackedRule pr) {
+              size_t wp, int n_wstrips, int n_items, int band_rows, const __grid_constant__ PackedRule pr) {
     constexpr int PH = bits_for(2 * R + 1);
     constexpr int PB = bits_for((2 * R + 1) * (2 * R + 1));
+    constexpr bool kRing = PackedRing<R>::fits;
+    constexpr int RING = 2 * R + 2;
+    extern __shared__ uint32_t ring_all[];
     const int lane = threadIdx.x & 31;
-    const int warps_per_cta = blockDim.x >> 5;
-    const int gwarp = blockIdx.x * warps_per_cta + (threadIdx.x >> 5);
-    const int gwarps = gridDim.x * warps_per_cta;
+    const int wid = threadIdx.x >> 5;
+    uint32_t* ring = ring_all + (size_t)wid * RING * PH * 32;
+    const int gwarp = blockIdx.x * kPackedWarps + wid;
+    const int gwarps = gridDim.x * kPackedWarps;
 
     for (int item = gwarp; item < n_items; item += gwarps) {
         const int ws = item % n_wstrips;
         const int band = item / n_wstrips;
-        const int r0 = band * kPackedBand;
-        const int r1 = min(r0 + kPackedBand, n);
+        const int r0 = band * band_rows;
+        const int r1 = min(r0 + band_rows, n);
         const int w = ws * 32 + lane;     // inner word
         const bool active = w <= nw;      // w == nw is the right halo word (neighbour of the last word)
         const bool outputs = w < nw;
         const int fw = HW + w;
         auto rowp = [&](int r) { return cur + (size_t)(HR + r) * wp; };
+        auto slot = [&](int r) { return ring + (((r % RING) + RING) % RING) * PH * 32 + lane; };
 
         uint32_t B[PB];
 #pragma unroll
@@ -179,23 +206,40 @@ k_packed_step(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int 
             uint32_t h[PH];
             hcount<R, PH>(rowp(r0 + dy), fw, active, lane, h);
             planes_add<PB, PH>(B, h);
+            if constexpr (kRing) {
+                uint32_t* sl = slot(r0 + dy);
+#pragma unroll
+                for (int i = 0; i < PH; ++i) sl[32 * i] = h[i];
+            }
         }
 #pragma unroll 1
         for (int r = r0; r < r1; ++r) {
             if (outputs) {
-                uint32_t s = __ldg(rowp(r) + fw);
-                uint32_t in1 = planes_in<PB>(B, pr.lo1, pr.hi1) & ~pr.empty1;
-                uint32_t in0 = planes_in<PB>(B, pr.lo0, pr.hi0) & ~pr.empty0;
+                const uint32_t s = __ldg(rowp(r) + fw);
+                const uint32_t in1 = planes_in<PB>(B, pr.lo[1], pr.hi[1]) & pr.keep[1];
+                const uint32_t in0 = planes_in<PB>(B, pr.lo[0], pr.hi[0]) & pr.keep[0];
                 nxt[(size_t)(HR + r) * wp + fw] = (s & in1) | (~s & in0);
             }
             if (r + 1 < r1) {
                 uint32_t h[PH];
-                hcount<R, PH>(rowp(r - R), fw, active, lane, h);
+                if constexpr (kRing) {
+                    const uint32_t* sl = slot(r - R);
+#pragma unroll
+                    for (int i = 0; i < PH; ++i) h[i] = sl[32 * i];
+                } else {
+                    hcount<R, PH>(rowp(r - R), fw, active, lane, h);
+                }
                 planes_sub<PB, PH>(B, h);
                 hcount<R, PH>(rowp(r + R + 1), fw, active, lane, h);
                 planes_add<PB, PH>(B, h);
+                if constexpr (kRing) {
+                    uint32_t* sl = slot(r + R + 1);
+#pragma unroll
+                    for (int i = 0; i < PH; ++i) sl[32 * i] = h[i];
+                }
             }
         }
+        __syncwarp();
     }
 }
 
@@ -204,18 +248,23 @@ bool packed_supported(int n, int radius) { return radius >= 1 && radius <= 32 &&
 template <int R>
 static cudaError_t launch_packed_r(const PackedFrame& c, const PackedFrame& x, const PackedRule& pr,
                                    cudaStream_t s) {
-    const int n_wstrips = (c.nw + 1 + 31) / 32;
-    const int bands = (c.n + kPackedBand - 1) / kPackedBand;
-    const int items = n_wstrips * bands;
-    const int wpc = 4;
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_packed_step<R>, wpc * 32, 0);
+    const int n_wstrips = (c.nw + 1 + 31) / 32;
+    const int band_rows = packed_band_rows(c.n, n_wstrips, sms);
+    const int bands = (c.n + band_rows - 1) / band_rows;
+    const int items = n_wstrips * bands;
+    const int smem = PackedRing<R>::fits ? PackedRing<R>::BYTES : 0;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_packed_step<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_packed_step<R>, kPackedWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
-    int ctas = std::min((items + wpc - 1) / wpc, sms * per_sm);
-    k_packed_step<R><<<ctas, wpc * 32, 0, s>>>(c.words, x.words, c.n, c.nw, c.HR, c.HW, c.wpitch, n_wstrips,
-                                               items, pr);
+    int ctas = std::min((items + kPackedWarps - 1) / kPackedWarps, sms * per_sm);
+    k_packed_step<R><<<ctas, kPackedWarps * 32, smem, s>>>(c.words, x.words, c.n, c.nw, c.HR, c.HW, c.wpitch,
+                                                           n_wstrips, items, band_rows, pr);
     return cudaGetLastError();
 }
 

@@ -89,21 +89,59 @@ __device__ __forceinline__ void v_slide(uint32_t (&v)[4], uint4 in, uint4 out) {
 
 // Row box sums for the lane's four output words.  w[0..7] = byte words at
 // offsets -8 .. +28 of the lane's chunk (two words of the left lane, the four
-// own words, two words of the right lane).  Output word m covers cells
-// 4m..4m+3; its sum runs over byte offsets 4m-R .. 4m+R, i.e. w-offsets
-// 4m-R+8 ... 4m+R+8.
-template <int R, int M>
-__device__ __forceinline__ uint32_t row_box_word(const uint32_t* w) {
-    uint32_t acc = 0;
+// own words, two words of the right lane); byte offset o of the chunk is byte
+// o + 8 of w.  The (2R+1)-wide window is split into power-of-two segments
+// (e.g. 11 = 8 + 2 + 1), and the segment sums P_k (k consecutive bytes, SWAR)
+// are built by doubling: P_2k(y) = P_k(y) + P_k(y + k).
+template <int K>
+__device__ __forceinline__ void double_seg(const uint32_t (&a)[8], uint32_t (&b)[8]) {
 #pragma unroll
-    for (int d = -R; d <= R; ++d) {
-        // offsets are compile-time constants after unrolling
-        const int o = 4 * M + d + 8;
-        const int idx = o >> 2, sh = o & 3;
-        uint32_t x = (sh == 0) ? w[idx] : __byte_perm(w[idx], w[idx + 1], 0x3210 + 0x1111 * sh);
-        acc += x;
+    for (int j = 0; j < 8; ++j) {
+        if constexpr (K < 4) {
+            b[j] = (j + 1 < 8) ? a[j] + __funnelshift_r(a[j], a[j + 1], 8 * K) : 0u;
+        } else {
+            b[j] = (j + K / 4 < 8) ? a[j] + a[j + K / 4] : 0u;
+        }
     }
-    return acc;
+}
+
+template <int O>
+__device__ __forceinline__ uint32_t bytes_at(const uint32_t (&w)[8]) {
+    constexpr int idx = O >> 2, sh = O & 3;
+    if constexpr (sh == 0) {
+        return w[idx];
+    } else {
+        return __funnelshift_r(w[idx], w[idx + 1], 8 * sh);
+    }
+}
+
+template <int L, int O>
+__device__ __forceinline__ uint32_t window_sum(const uint32_t (&p1)[8], const uint32_t (&p2)[8],
+                                               const uint32_t (&p4)[8], const uint32_t (&p8)[8]) {
+    // sum of L consecutive bytes starting at w-offset O (L <= 15)
+    if constexpr (L == 0) {
+        return 0u;
+    } else if constexpr (L >= 8) {
+        return bytes_at<O>(p8) + window_sum<L - 8, O + 8>(p1, p2, p4, p8);
+    } else if constexpr (L >= 4) {
+        return bytes_at<O>(p4) + window_sum<L - 4, O + 4>(p1, p2, p4, p8);
+    } else if constexpr (L >= 2) {
+        return bytes_at<O>(p2) + window_sum<L - 2, O + 2>(p1, p2, p4, p8);
+    } else {
+        return bytes_at<O>(p1);
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void row_boxes(const uint32_t (&w)[8], uint32_t (&box)[4]) {
+    uint32_t p2[8], p4[8], p8[8];
+    double_seg<1>(w, p2);
+    double_seg<2>(p2, p4);
+    double_seg<4>(p4, p8);
+    box[0] = window_sum<2 * R + 1, 0 * 4 - R + 8>(w, p2, p4, p8);
+    box[1] = window_sum<2 * R + 1, 1 * 4 - R + 8>(w, p2, p4, p8);
+    box[2] = window_sum<2 * R + 1, 2 * 4 - R + 8>(w, p2, p4, p8);
+    box[3] = window_sum<2 * R + 1, 3 * 4 - R + 8>(w, p2, p4, p8);
 }
 
 template <int R>
@@ -152,11 +190,13 @@ k_plain_swar8(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n,
                     w[7] = __shfl_down_sync(0xffffffffu, V[1], 1);
                     if (outputs) {
                         uint4 c = ld_row_chunk(rowp(rr));
+                        uint32_t box[4];
+                        row_boxes<R>(w, box);
                         uint4 o;
-                        o.x = rule_swar8(row_box_word<R, 0>(w), c.x, q);
-                        o.y = rule_swar8(row_box_word<R, 1>(w), c.y, q);
-                        o.z = rule_swar8(row_box_word<R, 2>(w), c.z, q);
-                        o.w = rule_swar8(row_box_word<R, 3>(w), c.w, q);
+                        o.x = rule_swar8(box[0], c.x, q);
+                        o.y = rule_swar8(box[1], c.y, q);
+                        o.z = rule_swar8(box[2], c.z, q);
+                        o.w = rule_swar8(box[3], c.w, q);
                         uint8_t* dst = nxt + (size_t)(H + rr) * pitch + H + x;
                         if (x + 16 <= n) {
                             *(uint4*)dst = o;
@@ -183,12 +223,12 @@ int plain_swar8_band_rows(int n, int device) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const int strips = (n + kStripOut - 1) / kStripOut;
-    // ~8 work items per resident warp slot (16 warps/SM assumed) for balance,
-    // but never fewer than 32 rows per band (the window start-up costs 2R+1 rows).
-    long long target_items = (long long)sms * 16 * 8;
+    // Enough items for ~32 resident warps per SM, but bands of at least 96 rows:
+    // every band re-reads 2R+1 rows to start its vertical window.
+    long long target_items = (long long)sms * 32;
     int bands = (int)std::max<long long>(1, target_items / std::max(strips, 1));
     int rows = (n + bands - 1) / bands;
-    rows = std::max(32, std::min(rows, 512));
+    rows = std::max(96, std::min(rows, 512));
     return rows;
 }
 

@@ -152,13 +152,26 @@ __host__ __device__ constexpr uint32_t idesc_u8(int N, bool b_mn_major) {
 }
 
 // ---------------------------------------------------------------------------
-// Tile geometry
+// Tile geometry and the persistent, warp-specialised kernel
+//
+// One CTA per SM walks a strided list of tiles.  Warp roles:
+//   warp 0  TMA producer: X tiles into a 3-stage ring (x_full / x_empty);
+//   warp 1  MMA issuer:   product 1 of tile t into TMEM stage t % 2, then
+//                          product 2 of tile t-1 once its H is back in smem;
+//   warps 2-5 epilogue:  re-quantise H(t+1), then rule + store C(t).
+// TMEM: two accumulator stages of 256 columns (H and then C of one tile share
+// a stage).  All mbarrier waits are bounded.
 // ---------------------------------------------------------------------------
 constexpr int kAtomBytes = 128 * 128;  // one 128-row x 128-byte swizzle atom
 constexpr int kAtoms = 2;              // X tile = 128 rows x 256 columns
+constexpr int kXBytes = kAtoms * kAtomBytes;
 constexpr int kXCols = 128 * kAtoms;
+constexpr int kXStages = 3;
+constexpr int kAccStages = 2;
+constexpr int kAccCols = 256;          // TMEM columns per accumulator stage
 constexpr int kN1 = 32;                // product-1 column chunk
-constexpr int kThreads = 128;
+constexpr int kThreads = 192;          // 6 warps
+constexpr int kEpiWarps = 4;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any legitimate wait
 
 struct TensorParams {
@@ -178,19 +191,22 @@ struct SmemLayout {
     int x_off, hs_off, bh_off, bv_off, bar_off, tmem_off, total;
 };
 
+enum Bar { X_FULL = 0, X_EMPTY = 3, H_FULL = 6, HS_FULL = 8, C_FULL = 10, ACC_EMPTY = 12, NBARS = 14 };
+
 __host__ __device__ inline SmemLayout smem_layout(int Tc, int K1c) {
     SmemLayout L{};
     int o = 0;
     L.x_off = o;
-    o += kAtoms * kAtomBytes;               // 32 KB, 1024-aligned
+    o += kXStages * kXBytes;                // 96 KB, 1024-aligned stages
     L.hs_off = o;
-    o += 128 * Tc;                          // H as u8, MN-major
+    o += kAccStages * 128 * Tc;             // H as u8, MN-major, one buffer per accumulator stage
     L.bh_off = o;
     o += kN1 * K1c;                         // B_h
     L.bv_off = o;
     o += 128 * 128;                         // B_v
+    o = (o + 7) & ~7;
     L.bar_off = o;
-    o += 2 * 8;
+    o += NBARS * 8;
     L.tmem_off = o;
     o += 16;
     L.total = o;
@@ -203,6 +219,10 @@ __device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, ui
     return __byte_perm(lo, hi, 0x5410);
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
 k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -212,32 +232,28 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
     uint8_t* hs = smem + L.hs_off;
     uint8_t* bh = smem + L.bh_off;
     uint8_t* bv = smem + L.bv_off;
-    uint64_t* bars = (uint64_t*)(smem + L.bar_off);  // [0] TMA, [1] MMA
+    uint64_t* bars = (uint64_t*)(smem + L.bar_off);
     uint32_t* tmem_slot = (uint32_t*)(smem + L.tmem_off);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tile = blockIdx.x;
-    const int ty = tile / p.tiles_x, tx = tile % p.tiles_x;
-    const int r0 = ty * p.Tr, c0 = tx * p.Tc;
     const int R = p.R, PADC = p.PADC, Tc = p.Tc, K1c = p.K1c;
-    constexpr uint32_t kTmemCols = 256;
+    const int ntiles = p.tiles_x * p.tiles_y;
+    constexpr uint32_t kTmemCols = kAccStages * kAccCols;
 
     if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        for (int i = 0; i < kXStages; ++i) {
+            mbar_init(&bars[X_FULL + i], 1);
+            mbar_init(&bars[X_EMPTY + i], kEpiWarps);
+        }
+        for (int i = 0; i < kAccStages; ++i) {
+            mbar_init(&bars[H_FULL + i], 1);
+            mbar_init(&bars[HS_FULL + i], kEpiWarps);
+            mbar_init(&bars[C_FULL + i], 1);
+            mbar_init(&bars[ACC_EMPTY + i], kEpiWarps);
+        }
         fence_mbar_init();
     }
     if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (tid == 0) {
-        mbar_expect_tx(&bars[0], kAtoms * kAtomBytes);
-        const int y = p.H + r0 - R;
-        const int x = p.H + c0 - PADC;
-#pragma unroll
-        for (int a = 0; a < kAtoms; ++a) tma_load_2d(xs + a * kAtomBytes, &xmap, &bars[0], x + 128 * a, y);
-    }
     // Band matrices (no-swizzle K-major layouts: [k / 16][row][16 bytes]).
     // B_h[n][k] = [|k - PADC - n| <= R], n < 32, k < K1c
     for (int idx = tid; idx < kN1 * K1c; idx += kThreads) {
@@ -245,89 +261,159 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
         const int d = k - PADC - n;
         bh[((k >> 4) * kN1 + n) * 16 + (k & 15)] = (d >= -R && d <= R) ? 1 : 0;
     }
-    // B_v[m][k] = [m <= k <= m + 2R], m, k < 128
-    for (int idx = tid; idx < 128 * 128; idx += kThreads) {
-        const int k = idx / 128, m = idx % 128;
-        bv[((k >> 4) * 128 + m) * 16 + (k & 15)] = (k >= m && k <= m + 2 * R) ? 1 : 0;
+    // B_v[m][k] = [m <= k <= m + 2R], m, k < 128 (16 bytes per store)
+    for (int idx = tid; idx < 8 * 128; idx += kThreads) {
+        const int kc = idx / 128, m = idx % 128;
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint32_t v = 0;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int k = kc * 16 + 4 * q + e;
+                v |= (uint32_t)(k >= m && k <= m + 2 * R) << (8 * e);
+            }
+            w[q] = v;
+        }
+        *(uint4*)(bv + (kc * 128 + m) * 16) = make_uint4(w[0], w[1], w[2], w[3]);
     }
     fence_proxy_async();
+    tc_fence_before();
     __syncthreads();
+    tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    bool ok = true;
 
-    // ---- product 1: H = X * B_h --------------------------------------------
-    if (tid == 0) {
-        ok = mbar_wait(&bars[0], 0, kWaitLimitNs);
-        if (ok) {
-            tc_fence_after();
-            const uint32_t xa = smem_u32(xs), ba = smem_u32(bh);
+    if (warp == 0) {
+        // ------------------------- TMA producer -----------------------------
+        if (lane == 0) {
+            int it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
+                const int st = it % kXStages;
+                const uint32_t ph = (uint32_t)(it / kXStages) & 1u;
+                if (it >= kXStages) ok = mbar_wait(&bars[X_EMPTY + st], ph ^ 1u, kWaitLimitNs);
+                if (!ok) {
+                    atomicOr(p.err, 1u);
+                    break;
+                }
+                const int ty = t / p.tiles_x, tx = t % p.tiles_x;
+                const int y = p.H + ty * p.Tr - R;
+                const int x = p.H + tx * Tc - PADC;
+                uint8_t* dst = xs + st * kXBytes;
+                mbar_expect_tx(&bars[X_FULL + st], kXBytes);
+#pragma unroll
+                for (int a = 0; a < kAtoms; ++a) tma_load_2d(dst + a * kAtomBytes, &xmap, &bars[X_FULL + st], x + 128 * a, y);
+            }
+            // never leave with a copy in flight into this CTA's shared memory
+            const int issued = it;
+            for (int j = (issued > kXStages ? issued - kXStages : 0); j < issued; ++j) {
+                if (!mbar_wait(&bars[X_FULL + j % kXStages], (uint32_t)(j / kXStages) & 1u, kWaitLimitNs))
+                    atomicOr(p.err, 16u);
+            }
+        }
+    } else if (warp == 1) {
+        // --------------------------- MMA issuer -----------------------------
+        if (lane == 0) {
+            const uint32_t ba = smem_u32(bh), va = smem_u32(bv), ha0 = smem_u32(hs);
             const uint32_t id1 = idesc_u8(kN1, false);
-            for (int n0 = 0; n0 < Tc; n0 += kN1) {
-                for (int s = 0; s < K1c / 32; ++s) {
-                    const int col = n0 + 32 * s;  // X column of this K step
-                    const uint32_t a_addr = xa + (col >> 7) * kAtomBytes + (col & 127);
-                    const uint64_t ad = desc_k_sw128(a_addr);
-                    const uint64_t bd = desc_noswz(ba + s * 2 * kN1 * 16, kN1 * 16, 128);
-                    mma_i8(tmem + n0, ad, bd, id1, s > 0 ? 1u : 0u);
+            const uint32_t id2 = idesc_u8(Tc, true);
+            bool ok = true;
+            int it = 0;
+            auto product2 = [&](int j) -> bool {
+                const int as = j % kAccStages;
+                const uint32_t ph = (uint32_t)(j / kAccStages) & 1u;
+                if (!mbar_wait(&bars[HS_FULL + as], ph, kWaitLimitNs)) {
+                    atomicOr(p.err, 2u);
+                    return false;
+                }
+                tc_fence_after();
+                const uint32_t ha = ha0 + as * 128 * Tc;
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const uint64_t ad = desc_noswz(va + s * 2 * 128 * 16, 128 * 16, 128);
+                    const uint64_t bd = desc_noswz(ha + s * 32 * 16, 128, 128 * 16);
+                    mma_i8(tmem + as * kAccCols, ad, bd, id2, s > 0 ? 1u : 0u);
+                }
+                mma_commit(&bars[C_FULL + as]);
+                return true;
+            };
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
+                const int st = it % kXStages, as = it % kAccStages;
+                // product 1 of tile `it`: needs its X tile and a drained TMEM stage
+                ok = mbar_wait(&bars[X_FULL + st], (uint32_t)(it / kXStages) & 1u, kWaitLimitNs);
+                if (ok && it >= kAccStages)
+                    ok = mbar_wait(&bars[ACC_EMPTY + as], ((uint32_t)(it / kAccStages) & 1u) ^ 1u, kWaitLimitNs);
+                if (!ok) {
+                    atomicOr(p.err, 4u);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t xa = smem_u32(xs + st * kXBytes);
+                for (int n0 = 0; n0 < Tc; n0 += kN1) {
+                    for (int s = 0; s < K1c / 32; ++s) {
+                        const int col = n0 + 32 * s;  // X column of this K step
+                        const uint32_t a_addr = xa + (col >> 7) * kAtomBytes + (col & 127);
+                        const uint64_t ad = desc_k_sw128(a_addr);
+                        const uint64_t bd = desc_noswz(ba + s * 2 * kN1 * 16, kN1 * 16, 128);
+                        mma_i8(tmem + as * kAccCols + n0, ad, bd, id1, s > 0 ? 1u : 0u);
+                    }
+                }
+                mma_commit(&bars[H_FULL + as]);
+                // product 2 of the previous tile (its H was re-quantised meanwhile)
+                if (it >= 1 && !product2(it - 1)) {
+                    ok = false;
+                    break;
                 }
             }
-            mma_commit(&bars[1]);
-        } else {
-            atomicOr(p.err, 1u);
+            if (ok && it >= 1) product2(it - 1);
         }
-    }
-    __syncthreads();
-    // (if thread 0 gave up on the TMA wait it issued nothing and this wait times out too)
-    ok = mbar_wait(&bars[1], 0, kWaitLimitNs);
-    if (!ok) atomicOr(p.err, 2u);
-    if (__syncthreads_and(ok)) {
-        tc_fence_after();
-        // ---- re-quantise H to u8 (MN-major B operand of product 2) ---------
-        const int k = warp * 32 + lane;  // H row = TMEM lane
-        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-        for (int cb = 0; cb < Tc; cb += 32) {
-            uint32_t v[32];
-            tmem_ld32(trow + cb, v);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                uint4 w;
-                w.x = pack4(v[16 * h + 0], v[16 * h + 1], v[16 * h + 2], v[16 * h + 3]);
-                w.y = pack4(v[16 * h + 4], v[16 * h + 5], v[16 * h + 6], v[16 * h + 7]);
-                w.z = pack4(v[16 * h + 8], v[16 * h + 9], v[16 * h + 10], v[16 * h + 11]);
-                w.w = pack4(v[16 * h + 12], v[16 * h + 13], v[16 * h + 14], v[16 * h + 15]);
-                const int chunk = (cb >> 4) + h;
-                *(uint4*)(hs + (chunk * 128 + k) * 16) = w;
-            }
-        }
-        fence_proxy_async();
-        tc_fence_before();
-        __syncthreads();
-        // ---- product 2: C = B_v * H  (into the same TMEM columns) ------------
-        if (tid == 0) {
+    } else {
+        // ---------------------------- epilogue ------------------------------
+        const int q = warp & 3;                 // TMEM lane quarter of this warp
+        const int row = q * 32 + lane;          // H row / output row within the tile
+        const uint32_t lane_off = (uint32_t)(q * 32) << 16;
+        const bool small = (2 * R + 1) * (2 * R + 1) <= 127;
+        int ntile_mine = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) ++ntile_mine;
+        bool ok = true;
+        auto requant = [&](int j) -> bool {
+            const int as = j % kAccStages;
+            if (!mbar_wait(&bars[H_FULL + as], (uint32_t)(j / kAccStages) & 1u, kWaitLimitNs)) return false;
             tc_fence_after();
-            const uint32_t va = smem_u32(bv), ha = smem_u32(hs);
-            const uint32_t id2 = idesc_u8(Tc, true);
+            uint8_t* hsb = hs + as * 128 * Tc;
+            const uint32_t trow = tmem + as * kAccCols + lane_off;
+            for (int cb = 0; cb < Tc; cb += 32) {
+                uint32_t v[32];
+                tmem_ld32(trow + cb, v);
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const uint64_t ad = desc_noswz(va + s * 2 * 128 * 16, 128 * 16, 128);
-                const uint64_t bd = desc_noswz(ha + s * 32 * 16, 128, 128 * 16);
-                mma_i8(tmem, ad, bd, id2, s > 0 ? 1u : 0u);
+                for (int h = 0; h < 2; ++h) {
+                    uint4 w;
+                    w.x = pack4(v[16 * h + 0], v[16 * h + 1], v[16 * h + 2], v[16 * h + 3]);
+                    w.y = pack4(v[16 * h + 4], v[16 * h + 5], v[16 * h + 6], v[16 * h + 7]);
+                    w.z = pack4(v[16 * h + 8], v[16 * h + 9], v[16 * h + 10], v[16 * h + 11]);
+                    w.w = pack4(v[16 * h + 12], v[16 * h + 13], v[16 * h + 14], v[16 * h + 15]);
+                    const int chunk = (cb >> 4) + h;
+                    *(uint4*)(hsb + (chunk * 128 + row) * 16) = w;
+                }
             }
-            mma_commit(&bars[1]);
-        }
-        __syncwarp();
-        ok = mbar_wait(&bars[1], 1, kWaitLimitNs);
-        if (!ok) atomicOr(p.err, 4u);
-        if (ok) {
+            fence_proxy_async();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bars[HS_FULL + as]);
+            return true;
+        };
+        auto rule_store = [&](int j, int t) -> bool {
+            const int as = j % kAccStages, st = j % kXStages;
+            if (!mbar_wait(&bars[C_FULL + as], (uint32_t)(j / kAccStages) & 1u, kWaitLimitNs)) return false;
             tc_fence_after();
-            // ---- epilogue: rule, store -------------------------------------
-            const int m = warp * 32 + lane;      // output row within the tile
-            const int gi = r0 + m;               // grid row
-            const bool row_ok = (m < p.Tr) && (gi < p.n);
-            const int xr = m + R;                // X tile row of the centre cell
-            const uint8_t* xrow = xs + xr * 128;
+            const int ty = t / p.tiles_x, tx = t % p.tiles_x;
+            const int r0 = ty * p.Tr, c0 = tx * Tc;
+            const int gi = r0 + row;
+            const bool row_ok = (row < p.Tr) && (gi < p.n);
+            const int xr = row + R;
+            const uint8_t* xrow = xs + st * kXBytes + (xr & 127) * 128;
             uint8_t* orow = p.out + (size_t)(p.H + gi) * (size_t)p.pitch + p.H + c0;
-            const bool small = (2 * R + 1) * (2 * R + 1) <= 127;
+            const uint32_t trow = tmem + as * kAccCols + lane_off;
             for (int cb = 0; cb < Tc; cb += 32) {
                 uint32_t v[32];
                 tmem_ld32(trow + cb, v);
@@ -340,20 +426,20 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
                     const uint32_t sw[4] = {s4.x, s4.y, s4.z, s4.w};
                     uint32_t o[4];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const uint32_t* b = &v[16 * h + 4 * q];
+                    for (int qq = 0; qq < 4; ++qq) {
+                        const uint32_t* b = &v[16 * h + 4 * qq];
                         if (small) {
-                            o[q] = rule_swar8(pack4(b[0], b[1], b[2], b[3]), sw[q], p.q);
+                            o[qq] = rule_swar8(pack4(b[0], b[1], b[2], b[3]), sw[qq], p.q);
                         } else {
                             uint32_t r = 0;
 #pragma unroll
                             for (int e = 0; e < 4; ++e) {
                                 const int B = (int)b[e];
-                                const int sv = (sw[q] >> (8 * e)) & 1;
+                                const int sv = (sw[qq] >> (8 * e)) & 1;
                                 const int lo = sv ? p.slo : p.blo, hi = sv ? p.shi : p.bhi;
                                 r |= (uint32_t)((B >= lo) & (B <= hi)) << (8 * e);
                             }
-                            o[q] = r;
+                            o[qq] = r;
                         }
                     }
                     const int gj = c0 + cb + 16 * h;
@@ -365,13 +451,26 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
                     }
                 }
             }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&bars[ACC_EMPTY + as]);
+                mbar_arrive(&bars[X_EMPTY + st]);
+            }
+            return true;
+        };
+        // requant(0); for j: requant(j+1); rule(j)
+        if (ntile_mine > 0) ok = requant(0);
+        int t = blockIdx.x;
+        for (int j = 0; j < ntile_mine && ok; ++j, t += gridDim.x) {
+            if (j + 1 < ntile_mine) ok = requant(j + 1);
+            if (ok) ok = rule_store(j, t);
         }
+        if (!ok) atomicOr(p.err, 8u);
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
-        // never leave with the TMA copy still in flight into this CTA's shared memory
-        if (lane == 0 && !mbar_wait(&bars[0], 0, kWaitLimitNs)) atomicOr(p.err, 8u);
         __syncwarp();
         tmem_dealloc(tmem, kTmemCols);
     }
@@ -483,7 +582,9 @@ TensorPlan* tensor_plan_create(const Frame& a, const Frame& b, const Rule& rule,
     cudaMemset(P->err, 0, sizeof(unsigned int));
     for (auto& q : P->prm) q.err = P->err;
     P->smem_bytes = smem_layout(Tc, K1c).total + 1024;
-    P->grid = P->prm[0].tiles_x * P->prm[0].tiles_y;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    P->grid = std::min(P->prm[0].tiles_x * P->prm[0].tiles_y, sms);
     if (cudaFuncSetAttribute(k_tensor_step, cudaFuncAttributeMaxDynamicSharedMemorySize, P->smem_bytes) !=
         cudaSuccess) {
         snprintf(why, why_len, "cannot reserve %d bytes of shared memory", P->smem_bytes);
