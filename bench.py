@@ -244,6 +244,36 @@ def e2e_run(C, torch, name, start, steps):
         s.close()
 
 
+def batched_run(C, torch, steps, warmup_steps):
+    """The batched workload (4096 grids, sides log-uniform in [64, 2048], R in 1..8,
+    scaled interval rule, 256 steps per ltl_batch_step call)."""
+    import concurrent.futures as cf
+    import numpy as np
+    from cat_cpu_b200.workloads import batch_config
+    cfg = batch_config()
+    with cf.ThreadPoolExecutor(os.cpu_count() or 8) as ex:
+        grids = list(ex.map(lambda c: C.generate_state(c[0], c[4], c[3], 1), cfg))
+    flat = np.concatenate([g.ravel() for g in grids])
+    stream = torch.cuda.Stream()
+    b = C.Batch([(n, r, rule) for (n, r, rule, d, s) in cfg])
+    try:
+        b.set_stream(stream.cuda_stream)
+        b.upload_all(flat)
+        cells, dev_bytes, resident = b.info()
+        b.step(warmup_steps)
+        b.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        b.step(steps)
+        e.record(stream)
+        stream.synchronize()
+        ms = a.elapsed_time(e)
+        return dict(ms=ms, cells=cells, grids=len(cfg), steps=steps, resident_grids=resident)
+    finally:
+        b.close()
+
+
 # ---------------------------------------------------------------------------
 # Reference CPU solver (built from the reference sources into oracle/_ref/)
 # ---------------------------------------------------------------------------
@@ -413,6 +443,20 @@ def main():
         line["tensor_vs_plain"] = round(variants["tensor"]["gcups"] / variants["plain"]["gcups"], 3)
     if rank == 0 and results[best].get("clocks"):
         line["clocks"] = results[best]["clocks"]
+    # batched workload (grids*steps/s), one replica per rank
+    br = batched_run(C, torch, 256, 256)
+    b_ms = max_over_ranks(br["ms"], world)
+    b_gcups = world * br["cells"] * br["steps"] / (b_ms * 1e-3) / 1e9
+    line["batched"] = {
+        "workload": "4096 grids, sides log-uniform [64,2048], R uniform 1..8, scaled interval rule, density "
+                    "U[0.2,0.6] (mt19937_64 seed 4), 256 steps per ltl_batch_step call, bit-packed",
+        "grid_steps_per_s": round(world * br["grids"] * br["steps"] / (b_ms * 1e-3), 1),
+        "gcups": round(b_gcups, 2), "ms": round(b_ms, 3), "cells": br["cells"],
+        "shared_memory_resident_grids": br["resident_grids"],
+        "roofline": {"bound": "hbm", "bytes_per_update": 0.25, "achieved": round(b_gcups * 0.25, 1),
+                     "peak": peak, "unit": "GB/s", "frac": round(b_gcups * 0.25 / peak, 4),
+                     "frac_u8_equivalent": round(b_gcups * 2.0 / peak, 4)},
+    }
     # end to end through the public API with host buffers
     e2 = e2e_run(C, torch, best, start, args.e2e_steps or args.steps)
     e2_ms = max_over_ranks(e2["ms"], world)

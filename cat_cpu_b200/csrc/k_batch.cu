@@ -1,15 +1,724 @@
-// k_batch.cu -- placeholder for the batched persistent path.
+// k_batch.cu -- K4: many independent tori of uneven size, radius and rule,
+// advanced together (ltl_batch_* in include/ltl.h).
+//
+// Semantics per grid are the reference's HostSolver<int> step (kezada94/CAT_cpu,
+// src/CellularAutomata/Solvers/HostSolver.tpp:58-140); the reference runs one
+// grid per process (CPUBenchmark.cpp:63-85).  Design:
+//   - every grid is stored bit-packed (packed_core.cuh) in one device arena,
+//     two arenas ping-pong;
+//   - grids are grouped into rule classes (radius + rule); each class gets its
+//     own kernel instantiation, with the rule's bit masks in the constant bank;
+//   - "resident" grids (small enough that two packed copies fit in one SM's
+//     shared memory) are advanced all requested steps in ONE launch: a CTA loads
+//     the grid once, keeps the torus halo in shared memory and writes the grid
+//     back after the last step (temporal blocking of the whole run);
+//   - larger grids are advanced one generation per launch by a persistent
+//     kernel that walks a (grid, row band, word strip) work list, followed by a
+//     batched halo refresh; the whole step loop is captured in a CUDA graph, and
+//     the resident launches run concurrently on a forked stream.
+#include <algorithm>
+#include <map>
+#include <new>
+#include <vector>
+
 #include "../../include/ltl.h"
-#include "ltl_kernels.h"
-struct ltl_batch { int dummy; };
-extern "C" int ltl_batch_create(ltl_batch** out, int, const ltl_grid_desc*, int, int) {
-    if (out) *out = nullptr; ltl_set_error("batched path not built yet"); return LTL_EUNSUPPORTED; }
-extern "C" int ltl_batch_destroy(ltl_batch*) { return LTL_OK; }
-extern "C" int ltl_batch_set_stream(ltl_batch*, void*) { return LTL_EUNSUPPORTED; }
-extern "C" int ltl_batch_upload(ltl_batch*, int, const uint8_t*, size_t) { return LTL_EUNSUPPORTED; }
-extern "C" int ltl_batch_download(ltl_batch*, int, uint8_t*, size_t) { return LTL_EUNSUPPORTED; }
-extern "C" int ltl_batch_upload_all(ltl_batch*, const uint8_t*) { return LTL_EUNSUPPORTED; }
-extern "C" int ltl_batch_download_all(ltl_batch*, uint8_t*) { return LTL_EUNSUPPORTED; }
-extern "C" int ltl_batch_step(ltl_batch*, int) { return LTL_EUNSUPPORTED; }
-extern "C" int ltl_batch_synchronize(ltl_batch*) { return LTL_EUNSUPPORTED; }
-extern "C" int ltl_batch_info(const ltl_batch*, long long*, long long*, int*) { return LTL_EUNSUPPORTED; }
+#include "packed_core.cuh"
+
+namespace ltl {
+
+struct BatchGrid {
+    long long off;       // word offset of the grid's packed frame in an arena
+    long long cell_off;  // byte offset of the grid in the dense staging buffer
+    int n, nw, HR, wp;   // cells per side, inner words per row, halo rows, words per frame row
+    int R;
+};
+
+constexpr int kBatchWarps = 4;
+constexpr int kResThreads = 1024;
+constexpr int kResSmemLimit = 220 * 1024;
+
+// ---------------------------------------------------------------------------
+// Per-step kernel for the streamed grids of one rule class.
+// ---------------------------------------------------------------------------
+template <int R>
+__global__ void __launch_bounds__(kBatchWarps * 32)
+k_batch_step(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, const BatchGrid* __restrict__ grids,
+             const int4* __restrict__ items, int n_items, const __grid_constant__ PackedRule pr) {
+    constexpr int PH = bits_for(2 * R + 1);
+    constexpr int PB = bits_for((2 * R + 1) * (2 * R + 1));
+    const int lane = threadIdx.x & 31;
+    const int gwarp = blockIdx.x * kBatchWarps + (threadIdx.x >> 5);
+    const int gwarps = gridDim.x * kBatchWarps;
+    for (int it = gwarp; it < n_items; it += gwarps) {
+        const int4 item = items[it];  // grid, r0, r1, word strip
+        const BatchGrid g = grids[item.x];
+        const uint32_t* base = cur + g.off;
+        uint32_t* obase = nxt + g.off;
+        const int r0 = item.y, r1 = item.z;
+        const int w = item.w * 32 + lane;
+        const bool active = w <= g.nw;
+        const bool outputs = w < g.nw;
+        const int fw = 1 + w;
+        auto rowp = [&](int r) { return base + (size_t)(g.HR + r) * g.wp; };
+        uint32_t B[PB];
+#pragma unroll
+        for (int i = 0; i < PB; ++i) B[i] = 0u;
+#pragma unroll 1
+        for (int dy = -R; dy <= R; ++dy) {
+            uint32_t h[PH];
+            hcount<R, PH>(rowp(r0 + dy), fw, active, lane, h);
+            planes_add<PB, PH>(B, h);
+        }
+#pragma unroll 1
+        for (int r = r0; r < r1; ++r) {
+            if (outputs) {
+                const uint32_t s = __ldg(rowp(r) + fw);
+                const uint32_t in1 = planes_in<PB>(B, pr.lo[1], pr.hi[1]) & pr.keep[1];
+                const uint32_t in0 = planes_in<PB>(B, pr.lo[0], pr.hi[0]) & pr.keep[0];
+                obase[(size_t)(g.HR + r) * g.wp + fw] = (s & in1) | (~s & in0);
+            }
+            if (r + 1 < r1) {
+                uint32_t h[PH];
+                hcount<R, PH>(rowp(r - R), fw, active, lane, h);
+                planes_sub<PB, PH>(B, h);
+                hcount<R, PH>(rowp(r + R + 1), fw, active, lane, h);
+                planes_add<PB, PH>(B, h);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Halo refresh of packed frames (same rules as k_packed.cu's halo kernels):
+// bit position p of an inner row holds cell (p - 32) mod n, then the top and
+// bottom halo rows are copies of the inner rows they wrap to.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t frame_bit(const uint32_t* row, int cell) {
+    const int p = 32 + cell;
+    return (row[p >> 5] >> (p & 31)) & 1u;
+}
+
+__device__ __forceinline__ uint32_t halo_word(const uint32_t* row, int fw, int n, int nw) {
+    // frame word fw (0 = left halo, nw = last inner, nw + 1 = right halo)
+    if (fw == nw) {
+        const int inner_bits = n - 32 * (nw - 1);
+        uint32_t v = inner_bits >= 32 ? row[fw] : (row[fw] & ((1u << inner_bits) - 1u));
+        for (int b = inner_bits; b < 32; ++b) v |= frame_bit(row, (32 * (nw - 1) + b) % n) << b;
+        return v;
+    }
+    uint32_t v = 0u;
+    for (int b = 0; b < 32; ++b) {
+        const int cell = 32 * (fw - 1) + b;
+        v |= frame_bit(row, ((cell % n) + n) % n) << b;
+    }
+    return v;
+}
+
+__global__ void k_batch_halo_cols(uint32_t* __restrict__ arena, const BatchGrid* __restrict__ grids,
+                                  const int* __restrict__ list) {
+    const BatchGrid g = grids[list[blockIdx.y]];
+    uint32_t* f = arena + g.off;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < g.n * 3; t += gridDim.x * blockDim.x) {
+        const int i = t / 3, k = t % 3;
+        const int fw = k == 0 ? 0 : g.nw + (k - 1);
+        uint32_t* row = f + (size_t)(g.HR + i) * g.wp;
+        row[fw] = halo_word(row, fw, g.n, g.nw);
+    }
+}
+
+__global__ void k_batch_halo_rows(uint32_t* __restrict__ arena, const BatchGrid* __restrict__ grids,
+                                  const int* __restrict__ list) {
+    const BatchGrid g = grids[list[blockIdx.y]];
+    uint32_t* f = arena + g.off;
+    const int total = 2 * g.HR * g.wp;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int band = t / g.wp, w = t % g.wp;
+        const int r = band < g.HR ? band : g.n + band;
+        const int src = g.HR + (((r - g.HR) % g.n) + g.n) % g.n;
+        f[(size_t)r * g.wp + w] = f[(size_t)src * g.wp + w];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Resident kernel: whole grids in shared memory for `steps` generations.
+// ---------------------------------------------------------------------------
+__device__ void smem_halo(uint32_t* buf, int n, int nw, int HR, int wp) {
+    for (int t = threadIdx.x; t < n * 3; t += blockDim.x) {
+        const int i = t / 3, k = t % 3;
+        const int fw = k == 0 ? 0 : nw + (k - 1);
+        uint32_t* row = buf + (size_t)(HR + i) * wp;
+        row[fw] = halo_word(row, fw, n, nw);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 2 * HR * wp; t += blockDim.x) {
+        const int band = t / wp, w = t % wp;
+        const int r = band < HR ? band : n + band;
+        const int src = HR + (((r - HR) % n) + n) % n;
+        buf[(size_t)r * wp + w] = buf[(size_t)src * wp + w];
+    }
+    __syncthreads();
+}
+
+template <int R>
+__global__ void __launch_bounds__(kResThreads, 1)
+k_batch_resident(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, const BatchGrid* __restrict__ grids,
+                 const int* __restrict__ list, int n_list, int steps, const __grid_constant__ PackedRule pr) {
+    constexpr int PH = bits_for(2 * R + 1);
+    constexpr int PB = bits_for((2 * R + 1) * (2 * R + 1));
+    extern __shared__ uint32_t sm[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int li = blockIdx.x; li < n_list; li += gridDim.x) {
+        const BatchGrid g = grids[list[li]];
+        const int rows = g.n + 2 * g.HR;
+        uint32_t* bufA = sm;
+        uint32_t* bufB = sm + (size_t)rows * g.wp;
+        // inner words in, halos built in shared memory
+        for (int t = threadIdx.x; t < g.n * g.nw; t += blockDim.x) {
+            const int i = t / g.nw, w = t % g.nw;
+            bufA[(size_t)(g.HR + i) * g.wp + 1 + w] = src[g.off + (size_t)(g.HR + i) * g.wp + 1 + w];
+        }
+        __syncthreads();
+        smem_halo(bufA, g.n, g.nw, g.HR, g.wp);
+        // work split: every warp owns a band of rows of one 32-word strip
+        const int strips = (g.nw + 1 + 31) / 32;
+        const int warps = blockDim.x >> 5;
+        const int bands = max(1, warps / strips);
+        const int band_rows = (g.n + bands - 1) / bands;
+        for (int s = 0; s < steps; ++s) {
+            for (int it = wid; it < strips * bands; it += warps) {
+                const int ws = it % strips, band = it / strips;
+                const int r0 = band * band_rows, r1 = min(r0 + band_rows, g.n);
+                if (r0 >= r1) continue;  // warp-uniform
+                const int w = ws * 32 + lane;
+                const bool active = w <= g.nw, outputs = w < g.nw;
+                const int fw = 1 + w;
+                auto rowp = [&](int r) { return bufA + (size_t)(g.HR + r) * g.wp; };
+                uint32_t B[PB];
+#pragma unroll
+                for (int i = 0; i < PB; ++i) B[i] = 0u;
+#pragma unroll 1
+                for (int dy = -R; dy <= R; ++dy) {
+                    uint32_t h[PH];
+                    hcount<R, PH>(rowp(r0 + dy), fw, active, lane, h);
+                    planes_add<PB, PH>(B, h);
+                }
+#pragma unroll 1
+                for (int r = r0; r < r1; ++r) {
+                    if (outputs) {
+                        const uint32_t sv = rowp(r)[fw];
+                        const uint32_t in1 = planes_in<PB>(B, pr.lo[1], pr.hi[1]) & pr.keep[1];
+                        const uint32_t in0 = planes_in<PB>(B, pr.lo[0], pr.hi[0]) & pr.keep[0];
+                        bufB[(size_t)(g.HR + r) * g.wp + fw] = (sv & in1) | (~sv & in0);
+                    }
+                    if (r + 1 < r1) {
+                        uint32_t h[PH];
+                        hcount<R, PH>(rowp(r - R), fw, active, lane, h);
+                        planes_sub<PB, PH>(B, h);
+                        hcount<R, PH>(rowp(r + R + 1), fw, active, lane, h);
+                        planes_add<PB, PH>(B, h);
+                    }
+                }
+            }
+            __syncthreads();
+            smem_halo(bufB, g.n, g.nw, g.HR, g.wp);
+            uint32_t* t = bufA;
+            bufA = bufB;
+            bufB = t;
+        }
+        for (int t = threadIdx.x; t < g.n * g.nw; t += blockDim.x) {
+            const int i = t / g.nw, w = t % g.nw;
+            dst[g.off + (size_t)(g.HR + i) * g.wp + 1 + w] = bufA[(size_t)(g.HR + i) * g.wp + 1 + w];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Dense staging <-> arena (all grids of a list, or one grid)
+// ---------------------------------------------------------------------------
+__global__ void k_batch_pack(const uint8_t* __restrict__ cells, uint32_t* __restrict__ arena,
+                             const BatchGrid* __restrict__ grids, int first) {
+    const BatchGrid g = grids[first + blockIdx.y];
+    const uint8_t* c = cells + g.cell_off;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < g.n * g.nw; t += gridDim.x * blockDim.x) {
+        const int i = t / g.nw, w = t % g.nw;
+        uint32_t v = 0u;
+        for (int b = 0; b < 32 && 32 * w + b < g.n; ++b) v |= (uint32_t)(c[(size_t)i * g.n + 32 * w + b] ? 1u : 0u) << b;
+        arena[g.off + (size_t)(g.HR + i) * g.wp + 1 + w] = v;
+    }
+}
+
+__global__ void k_batch_unpack(const uint32_t* __restrict__ arena, uint8_t* __restrict__ cells,
+                               const BatchGrid* __restrict__ grids, int first) {
+    const BatchGrid g = grids[first + blockIdx.y];
+    uint8_t* c = cells + g.cell_off;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < g.n * g.nw; t += gridDim.x * blockDim.x) {
+        const int i = t / g.nw, w = t % g.nw;
+        const uint32_t v = arena[g.off + (size_t)(g.HR + i) * g.wp + 1 + w];
+        for (int b = 0; b < 32 && 32 * w + b < g.n; ++b) c[(size_t)i * g.n + 32 * w + b] = (uint8_t)((v >> b) & 1u);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Launch helpers per radius (R <= 32 in the packed representation)
+// ---------------------------------------------------------------------------
+template <int R>
+static size_t res_smem_bytes(int n) {
+    const int nw = (n + 31) / 32;
+    const int wp = (nw + 3 + 3) / 4 * 4;
+    return 2ull * (size_t)(n + 2 * (R + 1)) * wp * 4;
+}
+
+template <int R>
+static cudaError_t launch_batch_step_r(const uint32_t* cur, uint32_t* nxt, const BatchGrid* grids, const int4* items,
+                                       int n_items, const PackedRule& pr, int sms, cudaStream_t s) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<R>, kBatchWarps * 32, 0);
+    if (per_sm < 1) per_sm = 1;
+    const int ctas = std::max(1, std::min((n_items + kBatchWarps - 1) / kBatchWarps, sms * per_sm));
+    k_batch_step<R><<<ctas, kBatchWarps * 32, 0, s>>>(cur, nxt, grids, items, n_items, pr);
+    return cudaGetLastError();
+}
+
+template <int R>
+static cudaError_t launch_batch_resident_r(const uint32_t* src, uint32_t* dst, const BatchGrid* grids, const int* list,
+                                           int n_list, int steps, const PackedRule& pr, size_t smem, int sms,
+                                           cudaStream_t s) {
+    const int ctas = std::max(1, std::min(n_list, sms));
+    k_batch_resident<R><<<ctas, kResThreads, smem, s>>>(src, dst, grids, list, n_list, steps, pr);
+    return cudaGetLastError();
+}
+
+#define LTL_BATCH_RADII(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
+
+static cudaError_t batch_step_dispatch(int R, const uint32_t* cur, uint32_t* nxt, const BatchGrid* grids,
+                                       const int4* items, int n_items, const PackedRule& pr, int sms, cudaStream_t s) {
+    switch (R) {
+#define LTL_C(r) \
+    case r: return launch_batch_step_r<r>(cur, nxt, grids, items, n_items, pr, sms, s);
+        LTL_BATCH_RADII(LTL_C)
+#undef LTL_C
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+static cudaError_t batch_resident_dispatch(int R, const uint32_t* src, uint32_t* dst, const BatchGrid* grids,
+                                           const int* list, int n_list, int steps, const PackedRule& pr, size_t smem,
+                                           int sms, cudaStream_t s) {
+    switch (R) {
+#define LTL_C(r) \
+    case r: return launch_batch_resident_r<r>(src, dst, grids, list, n_list, steps, pr, smem, sms, s);
+        LTL_BATCH_RADII(LTL_C)
+#undef LTL_C
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int R>
+static cudaError_t prepare_resident_r(size_t smem) {
+    return cudaFuncSetAttribute(k_batch_resident<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+static cudaError_t batch_prepare_dispatch(int R, size_t smem) {
+    switch (R) {
+#define LTL_C(r) \
+    case r: return prepare_resident_r<r>(smem);
+        LTL_BATCH_RADII(LTL_C)
+#undef LTL_C
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+static size_t res_smem_dispatch(int R, int n) {
+    switch (R) {
+#define LTL_C(r) \
+    case r: return res_smem_bytes<r>(n);
+        LTL_BATCH_RADII(LTL_C)
+#undef LTL_C
+        default: return (size_t)-1;
+    }
+}
+
+}  // namespace ltl
+
+using namespace ltl;
+
+struct BatchClass {
+    Rule rule;
+    PackedRule pr;
+    std::vector<int> resident;   // grid ids kept in shared memory
+    std::vector<int> streamed;   // grid ids streamed per step
+    int* d_resident = nullptr;
+    int4* d_items = nullptr;
+    int n_items = 0;
+    size_t res_smem = 0;
+};
+
+struct ltl_batch {
+    int device = 0;
+    int sms = 148;
+    std::vector<BatchGrid> grids;
+    std::vector<ltl_grid_desc> descs;
+    std::vector<BatchClass> classes;
+    BatchGrid* d_grids = nullptr;
+    int* d_streamed_all = nullptr;
+    int n_streamed_all = 0;
+    uint32_t* arena[2] = {nullptr, nullptr};
+    size_t arena_words = 0;
+    uint8_t* staging = nullptr;
+    long long total_cells = 0;
+    bool cur_is_a = true;
+    cudaStream_t own = nullptr, stream = nullptr, aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    // graph cache: (steps, parity) -> exec
+    std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
+};
+
+static void batch_release(ltl_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    for (auto& c : b->classes) {
+        if (c.d_resident) cudaFree(c.d_resident);
+        if (c.d_items) cudaFree(c.d_items);
+    }
+    if (b->d_grids) cudaFree(b->d_grids);
+    if (b->d_streamed_all) cudaFree(b->d_streamed_all);
+    for (auto& a : b->arena)
+        if (a) cudaFree(a);
+    if (b->staging) cudaFree(b->staging);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->join) cudaEventDestroy(b->join);
+    if (b->aux) cudaStreamDestroy(b->aux);
+    if (b->own) cudaStreamDestroy(b->own);
+    delete b;
+}
+
+#define BATCH_CUDA(call)                                                                           \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            ltl_set_error("%s failed: %s", #call, cudaGetErrorString(e_));                         \
+            return e_ == cudaErrorMemoryAllocation ? LTL_ENOMEM : LTL_ECUDA;                       \
+        }                                                                                          \
+    } while (0)
+
+static int batch_build(ltl_batch* b, int flags) {
+    const int count = (int)b->descs.size();
+    // rule classes
+    std::map<std::vector<int>, int> cls_of;
+    size_t words = 0;
+    long long cells = 0;
+    b->grids.resize(count);
+    std::vector<int> cls_id(count);
+    for (int i = 0; i < count; ++i) {
+        const ltl_grid_desc& d = b->descs[i];
+        std::vector<int> key = {d.radius, d.smin, d.smax, d.bmin, d.bmax};
+        auto it = cls_of.find(key);
+        if (it == cls_of.end()) {
+            BatchClass c;
+            c.rule = Rule{d.radius, d.smin, d.smax, d.bmin, d.bmax};
+            c.pr = make_packed_rule(c.rule);
+            it = cls_of.emplace(key, (int)b->classes.size()).first;
+            b->classes.push_back(c);
+        }
+        cls_id[i] = it->second;
+        BatchGrid g{};
+        g.n = d.n;
+        g.nw = (d.n + 31) / 32;
+        g.HR = d.radius + 1;
+        g.wp = (g.nw + 3 + 3) / 4 * 4;
+        g.R = d.radius;
+        g.off = (long long)words;
+        g.cell_off = cells;
+        words += (size_t)(g.n + 2 * g.HR) * g.wp;
+        words = (words + 31) / 32 * 32;
+        cells += (long long)g.n * g.n;
+        b->grids[i] = g;
+    }
+    b->arena_words = words + 64;
+    b->total_cells = cells;
+    const bool no_resident = (flags & 1) != 0;
+    std::vector<int> streamed_all;
+    for (int i = 0; i < count; ++i) {
+        BatchClass& c = b->classes[cls_id[i]];
+        const size_t need = res_smem_dispatch(b->grids[i].R, b->grids[i].n);
+        if (!no_resident && need <= (size_t)kResSmemLimit) {
+            c.resident.push_back(i);
+            c.res_smem = std::max(c.res_smem, need);
+        } else {
+            c.streamed.push_back(i);
+            streamed_all.push_back(i);
+        }
+    }
+    BATCH_CUDA(cudaMalloc(&b->d_grids, sizeof(BatchGrid) * count));
+    BATCH_CUDA(cudaMemcpy(b->d_grids, b->grids.data(), sizeof(BatchGrid) * count, cudaMemcpyHostToDevice));
+    b->n_streamed_all = (int)streamed_all.size();
+    if (!streamed_all.empty()) {
+        BATCH_CUDA(cudaMalloc(&b->d_streamed_all, sizeof(int) * streamed_all.size()));
+        BATCH_CUDA(cudaMemcpy(b->d_streamed_all, streamed_all.data(), sizeof(int) * streamed_all.size(),
+                              cudaMemcpyHostToDevice));
+    }
+    for (auto& c : b->classes) {
+        if (!c.resident.empty()) {
+            BATCH_CUDA(batch_prepare_dispatch(c.rule.radius, c.res_smem));
+            BATCH_CUDA(cudaMalloc(&c.d_resident, sizeof(int) * c.resident.size()));
+            BATCH_CUDA(cudaMemcpy(c.d_resident, c.resident.data(), sizeof(int) * c.resident.size(),
+                                  cudaMemcpyHostToDevice));
+        }
+        std::vector<int4> items;
+        for (int gi : c.streamed) {
+            const BatchGrid& g = b->grids[gi];
+            const int strips = (g.nw + 1 + 31) / 32;
+            const int band_rows = 64;
+            for (int r0 = 0; r0 < g.n; r0 += band_rows)
+                for (int ws = 0; ws < strips; ++ws) items.push_back(make_int4(gi, r0, std::min(g.n, r0 + band_rows), ws));
+        }
+        c.n_items = (int)items.size();
+        if (!items.empty()) {
+            BATCH_CUDA(cudaMalloc(&c.d_items, sizeof(int4) * items.size()));
+            BATCH_CUDA(cudaMemcpy(c.d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
+        }
+    }
+    for (auto& a : b->arena) {
+        BATCH_CUDA(cudaMalloc(&a, b->arena_words * sizeof(uint32_t)));
+        BATCH_CUDA(cudaMemset(a, 0, b->arena_words * sizeof(uint32_t)));
+    }
+    BATCH_CUDA(cudaMalloc(&b->staging, (size_t)std::max<long long>(cells, 1)));
+    return LTL_OK;
+}
+
+extern "C" int ltl_batch_create(ltl_batch** out, int device, const ltl_grid_desc* descs, int count, int flags) {
+    if (!out || !descs || count < 1) {
+        ltl_set_error("ltl_batch_create: bad arguments");
+        return LTL_EINVAL;
+    }
+    *out = nullptr;
+    for (int i = 0; i < count; ++i) {
+        const ltl_grid_desc& d = descs[i];
+        if (d.n < 1 || d.radius < 1 || d.n < d.radius) {
+            ltl_set_error("ltl_batch_create: grid %d: need n >= radius >= 1 (n=%d, radius=%d)", i, d.n, d.radius);
+            return LTL_EINVAL;
+        }
+        if (d.radius > 16) {
+            ltl_set_error("ltl_batch_create: grid %d: batched grids support radius <= 16 (got %d)", i, d.radius);
+            return LTL_EUNSUPPORTED;
+        }
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        ltl_set_error("ltl_batch_create: CUDA device %d not available", device);
+        return LTL_ECUDA;
+    }
+    ltl_batch* b = new (std::nothrow) ltl_batch();
+    if (!b) return LTL_ENOMEM;
+    b->device = device;
+    b->descs.assign(descs, descs + count);
+    cudaSetDevice(device);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess) {
+        ltl_set_error("ltl_batch_create: stream/event creation failed");
+        batch_release(b);
+        return LTL_ECUDA;
+    }
+    b->stream = b->own;
+    int rc = batch_build(b, flags);
+    if (rc != LTL_OK) {
+        batch_release(b);
+        return rc;
+    }
+    *out = b;
+    return LTL_OK;
+}
+
+extern "C" int ltl_batch_destroy(ltl_batch* b) {
+    if (!b) return LTL_OK;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    batch_release(b);
+    return LTL_OK;
+}
+
+extern "C" int ltl_batch_set_stream(ltl_batch* b, void* stream) {
+    if (!b) {
+        ltl_set_error("null batch");
+        return LTL_EINVAL;
+    }
+    cudaStream_t s = stream ? (cudaStream_t)stream : b->own;
+    if (s != b->stream) {
+        for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+        b->graphs.clear();
+    }
+    b->stream = s;
+    return LTL_OK;
+}
+
+static uint32_t* cur_arena(ltl_batch* b) { return b->arena[b->cur_is_a ? 0 : 1]; }
+static uint32_t* nxt_arena(ltl_batch* b) { return b->arena[b->cur_is_a ? 1 : 0]; }
+
+static cudaError_t refresh_streamed_halo(ltl_batch* b, uint32_t* arena, cudaStream_t s) {
+    if (b->n_streamed_all == 0) return cudaSuccess;
+    dim3 g1(8, (unsigned)b->n_streamed_all);
+    k_batch_halo_cols<<<g1, 128, 0, s>>>(arena, b->d_grids, b->d_streamed_all);
+    k_batch_halo_rows<<<g1, 128, 0, s>>>(arena, b->d_grids, b->d_streamed_all);
+    return cudaGetLastError();
+}
+
+extern "C" int ltl_batch_upload_all(ltl_batch* b, const uint8_t* cells) {
+    if (!b || !cells) {
+        ltl_set_error("ltl_batch_upload_all: bad arguments");
+        return LTL_EINVAL;
+    }
+    BATCH_CUDA(cudaSetDevice(b->device));
+    BATCH_CUDA(cudaMemcpyAsync(b->staging, cells, (size_t)b->total_cells, cudaMemcpyHostToDevice, b->stream));
+    const int count = (int)b->grids.size();
+    for (int first = 0; first < count; first += 65535) {
+        dim3 g(16, (unsigned)std::min(65535, count - first));
+        k_batch_pack<<<g, 256, 0, b->stream>>>(b->staging, cur_arena(b), b->d_grids, first);
+    }
+    BATCH_CUDA(cudaGetLastError());
+    BATCH_CUDA(refresh_streamed_halo(b, cur_arena(b), b->stream));
+    BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    return LTL_OK;
+}
+
+extern "C" int ltl_batch_download_all(ltl_batch* b, uint8_t* cells) {
+    if (!b || !cells) {
+        ltl_set_error("ltl_batch_download_all: bad arguments");
+        return LTL_EINVAL;
+    }
+    BATCH_CUDA(cudaSetDevice(b->device));
+    const int count = (int)b->grids.size();
+    for (int first = 0; first < count; first += 65535) {
+        dim3 g(16, (unsigned)std::min(65535, count - first));
+        k_batch_unpack<<<g, 256, 0, b->stream>>>(cur_arena(b), b->staging, b->d_grids, first);
+    }
+    BATCH_CUDA(cudaGetLastError());
+    BATCH_CUDA(cudaMemcpyAsync(cells, b->staging, (size_t)b->total_cells, cudaMemcpyDeviceToHost, b->stream));
+    BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    return LTL_OK;
+}
+
+extern "C" int ltl_batch_upload(ltl_batch* b, int grid, const uint8_t* inner, size_t pitch) {
+    if (!b || !inner || grid < 0 || grid >= (int)b->grids.size() || pitch < (size_t)b->grids[grid].n) {
+        ltl_set_error("ltl_batch_upload: bad arguments");
+        return LTL_EINVAL;
+    }
+    BATCH_CUDA(cudaSetDevice(b->device));
+    const BatchGrid& g = b->grids[grid];
+    BATCH_CUDA(cudaMemcpy2DAsync(b->staging + g.cell_off, g.n, inner, pitch, g.n, g.n, cudaMemcpyHostToDevice,
+                                 b->stream));
+    k_batch_pack<<<dim3(16, 1), 256, 0, b->stream>>>(b->staging, cur_arena(b), b->d_grids, grid);
+    BATCH_CUDA(cudaGetLastError());
+    BATCH_CUDA(refresh_streamed_halo(b, cur_arena(b), b->stream));
+    BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    return LTL_OK;
+}
+
+extern "C" int ltl_batch_download(ltl_batch* b, int grid, uint8_t* inner, size_t pitch) {
+    if (!b || !inner || grid < 0 || grid >= (int)b->grids.size() || pitch < (size_t)b->grids[grid].n) {
+        ltl_set_error("ltl_batch_download: bad arguments");
+        return LTL_EINVAL;
+    }
+    BATCH_CUDA(cudaSetDevice(b->device));
+    const BatchGrid& g = b->grids[grid];
+    k_batch_unpack<<<dim3(16, 1), 256, 0, b->stream>>>(cur_arena(b), b->staging, b->d_grids, grid);
+    BATCH_CUDA(cudaGetLastError());
+    BATCH_CUDA(cudaMemcpy2DAsync(inner, pitch, b->staging + g.cell_off, g.n, g.n, g.n, cudaMemcpyDeviceToHost,
+                                 b->stream));
+    BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    return LTL_OK;
+}
+
+// Enqueue `steps` generations of every grid (stream-ordered on b->stream).
+static cudaError_t enqueue_steps(ltl_batch* b, int steps) {
+    cudaError_t e = cudaSuccess;
+    uint32_t* a0 = cur_arena(b);
+    uint32_t* a1 = nxt_arena(b);
+    bool any_res = false;
+    for (auto& c : b->classes) any_res |= !c.resident.empty();
+    if (any_res) {
+        e = cudaEventRecord(b->fork, b->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->aux, b->fork, 0);
+        uint32_t* dst = (steps % 2) ? a1 : a0;
+        for (auto& c : b->classes) {
+            if (c.resident.empty() || e != cudaSuccess) continue;
+            e = batch_resident_dispatch(c.rule.radius, a0, dst, b->d_grids, c.d_resident, (int)c.resident.size(),
+                                        steps, c.pr, c.res_smem, b->sms, b->aux);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(b->join, b->aux);
+    }
+    for (int s = 0; s < steps && e == cudaSuccess; ++s) {
+        const uint32_t* src = (s % 2) ? a1 : a0;
+        uint32_t* dst = (s % 2) ? a0 : a1;
+        for (auto& c : b->classes) {
+            if (c.n_items == 0 || e != cudaSuccess) continue;
+            e = batch_step_dispatch(c.rule.radius, src, dst, b->d_grids, c.d_items, c.n_items, c.pr, b->sms,
+                                    b->stream);
+        }
+        if (e == cudaSuccess) e = refresh_streamed_halo(b, dst, b->stream);
+    }
+    if (any_res && e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join, 0);
+    return e;
+}
+
+extern "C" int ltl_batch_step(ltl_batch* b, int steps) {
+    if (!b || steps < 0) {
+        ltl_set_error("ltl_batch_step: bad arguments");
+        return LTL_EINVAL;
+    }
+    if (steps == 0) return LTL_OK;
+    BATCH_CUDA(cudaSetDevice(b->device));
+    const std::pair<int, int> key(steps, b->cur_is_a ? 0 : 1);
+    auto it = b->graphs.find(key);
+    if (it == b->graphs.end()) {
+        cudaGraph_t g = nullptr;
+        BATCH_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = enqueue_steps(b, steps);
+        cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            ltl_set_error("ltl_batch_step: graph capture failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+            return LTL_ECUDA;
+        }
+        cudaGraphExec_t ex = nullptr;
+        cudaError_t e3 = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) {
+            ltl_set_error("ltl_batch_step: graph instantiate failed: %s", cudaGetErrorString(e3));
+            return LTL_ECUDA;
+        }
+        it = b->graphs.emplace(key, ex).first;
+    }
+    BATCH_CUDA(cudaGraphLaunch(it->second, b->stream));
+    if (steps % 2) b->cur_is_a = !b->cur_is_a;
+    return LTL_OK;
+}
+
+extern "C" int ltl_batch_synchronize(ltl_batch* b) {
+    if (!b) {
+        ltl_set_error("null batch");
+        return LTL_EINVAL;
+    }
+    BATCH_CUDA(cudaSetDevice(b->device));
+    BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    return LTL_OK;
+}
+
+extern "C" int ltl_batch_info(const ltl_batch* b, long long* cells, long long* device_bytes, int* temporal_depth) {
+    if (!b) {
+        ltl_set_error("null batch");
+        return LTL_EINVAL;
+    }
+    if (cells) *cells = b->total_cells;
+    if (device_bytes) *device_bytes = (long long)(2 * b->arena_words * 4 + b->total_cells);
+    if (temporal_depth) {
+        int res = 0;
+        for (auto& c : b->classes) res += (int)c.resident.size();
+        *temporal_depth = res;  // number of grids advanced in shared memory for a whole ltl_batch_step
+    }
+    return LTL_OK;
+}

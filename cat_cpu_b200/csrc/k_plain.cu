@@ -76,9 +76,6 @@ cudaError_t launch_halo_fill(const Frame& f, cudaStream_t s) {
 // borrow bit of each lane (rule_swar8).
 // ---------------------------------------------------------------------------
 constexpr int kStripOut = 480;  // output columns per warp
-constexpr int kQD = 4;          // prefetch depth (rows) of the entering-row queue
-
-__device__ __forceinline__ uint4 ld_row_chunk(const uint8_t* p) { return __ldg((const uint4*)p); }
 
 __device__ __forceinline__ void v_add(uint32_t (&v)[4], uint4 a) {
     v[0] += a.x; v[1] += a.y; v[2] += a.z; v[3] += a.w;
@@ -144,14 +141,35 @@ __device__ __forceinline__ void row_boxes(const uint32_t (&w)[8], uint32_t (&box
     box[3] = window_sum<2 * R + 1, 3 * 4 - R + 8>(w, p2, p4, p8);
 }
 
+// Each warp streams its strip's rows through a private shared-memory ring with
+// cp.async (16 bytes per lane per row, one commit group per row, kAhead rows in
+// flight): every row is read from global memory once per band, and the centre
+// and leaving rows come back from shared memory.  A lane only ever reads the
+// ring bytes it copied itself, so no intra-warp synchronisation is needed.
+constexpr int kRingRows = 32;  // power of two >= 2R + 2 + kAhead
+constexpr int kAhead = 8;
+constexpr int kPlainWarps = 4;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 template <int R>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kPlainWarps * 32)
 k_plain_swar8(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n, int H, size_t pitch,
               int band_rows, int n_strips, int n_items, RuleSwar8 q) {
+    static_assert(2 * R + 2 + kAhead <= kRingRows, "ring too small");
+    extern __shared__ uint4 ring_all[];
     const int lane = threadIdx.x & 31;
-    const int warps_per_cta = blockDim.x >> 5;
-    const int gwarp = blockIdx.x * warps_per_cta + (threadIdx.x >> 5);
-    const int gwarps = gridDim.x * warps_per_cta;
+    const int wid = threadIdx.x >> 5;
+    uint4* ring = ring_all + (size_t)wid * kRingRows * 32 + lane;
+    const int gwarp = blockIdx.x * kPlainWarps + wid;
+    const int gwarps = gridDim.x * kPlainWarps;
 
     for (int item = gwarp; item < n_items; item += gwarps) {
         const int strip = item % n_strips;
@@ -162,58 +180,51 @@ k_plain_swar8(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n,
         const bool loads = x < n + 16;                          // chunks past that feed no output
         const bool outputs = lane >= 1 && lane <= 30 && x < n;
         const uint8_t* col = cur + (size_t)H + (loads ? x : 0);
-        auto rowp = [&](int r) { return col + (size_t)(H + r) * pitch; };
-        const int rmax = n - 1 + R;                             // last frame-inner row any window needs
-
+        const int rlast = min(r1 - 1 + R, n - 1 + R);           // last row any window of the band needs
+        auto slot = [&](int r) { return ring + (r & (kRingRows - 1)) * 32; };
+        auto issue = [&](int r) {
+            if (loads && r <= rlast) cp_async16(slot(r), col + (size_t)(H + r) * pitch);
+            cp_async_commit();
+        };
+        // rows r0-R .. r0+R start the window; kAhead more go in flight behind them
+        for (int r = r0 - R; r <= r0 + R + kAhead; ++r) issue(r);
+        cp_async_wait<kAhead>();
         uint32_t V[4] = {0u, 0u, 0u, 0u};
-        if (loads) {
 #pragma unroll 1
-            for (int dy = -R; dy <= R; ++dy) v_add(V, ld_row_chunk(rowp(r0 + dy)));
-        }
-        uint4 qrow[kQD];
-#pragma unroll
-        for (int t = 0; t < kQD; ++t) {
-            int rr = min(r0 + R + 1 + t, rmax);
-            qrow[t] = loads ? ld_row_chunk(rowp(rr)) : make_uint4(0, 0, 0, 0);
-        }
+        for (int dy = -R; dy <= R; ++dy) v_add(V, *slot(r0 + dy));
 
-        for (int r = r0; r < r1; r += kQD) {
-#pragma unroll
-            for (int t = 0; t < kQD; ++t) {
-                const int rr = r + t;
-                if (rr < r1) {
-                    uint32_t w[8];
-                    w[0] = __shfl_up_sync(0xffffffffu, V[2], 1);
-                    w[1] = __shfl_up_sync(0xffffffffu, V[3], 1);
-                    w[2] = V[0]; w[3] = V[1]; w[4] = V[2]; w[5] = V[3];
-                    w[6] = __shfl_down_sync(0xffffffffu, V[0], 1);
-                    w[7] = __shfl_down_sync(0xffffffffu, V[1], 1);
-                    if (outputs) {
-                        uint4 c = ld_row_chunk(rowp(rr));
-                        uint32_t box[4];
-                        row_boxes<R>(w, box);
-                        uint4 o;
-                        o.x = rule_swar8(box[0], c.x, q);
-                        o.y = rule_swar8(box[1], c.y, q);
-                        o.z = rule_swar8(box[2], c.z, q);
-                        o.w = rule_swar8(box[3], c.w, q);
-                        uint8_t* dst = nxt + (size_t)(H + rr) * pitch + H + x;
-                        if (x + 16 <= n) {
-                            *(uint4*)dst = o;
-                        } else {
-                            const uint8_t* ob = (const uint8_t*)&o;
-                            for (int j = 0; j < n - x; ++j) dst[j] = ob[j];
-                        }
-                    }
-                    if (loads) {
-                        uint4 out = ld_row_chunk(rowp(rr - R));
-                        v_slide(V, qrow[t], out);
-                        int nr = min(rr + R + 1 + kQD, rmax);
-                        qrow[t] = ld_row_chunk(rowp(nr));
-                    }
+#pragma unroll 1
+        for (int rr = r0; rr < r1; ++rr) {
+            uint32_t w[8];
+            w[0] = __shfl_up_sync(0xffffffffu, V[2], 1);
+            w[1] = __shfl_up_sync(0xffffffffu, V[3], 1);
+            w[2] = V[0]; w[3] = V[1]; w[4] = V[2]; w[5] = V[3];
+            w[6] = __shfl_down_sync(0xffffffffu, V[0], 1);
+            w[7] = __shfl_down_sync(0xffffffffu, V[1], 1);
+            if (outputs) {
+                const uint4 c = *slot(rr);
+                uint32_t box[4];
+                row_boxes<R>(w, box);
+                uint4 o;
+                o.x = rule_swar8(box[0], c.x, q);
+                o.y = rule_swar8(box[1], c.y, q);
+                o.z = rule_swar8(box[2], c.z, q);
+                o.w = rule_swar8(box[3], c.w, q);
+                uint8_t* dst = nxt + (size_t)(H + rr) * pitch + H + x;
+                if (x + 16 <= n) {
+                    *(uint4*)dst = o;
+                } else {
+                    const uint32_t ow[4] = {o.x, o.y, o.z, o.w};
+                    for (int j = 0; j < n - x; ++j) dst[j] = (uint8_t)(ow[j >> 2] >> (8 * (j & 3)));
                 }
             }
+            if (rr + 1 < r1) {
+                issue(rr + R + 1 + kAhead);
+                cp_async_wait<kAhead>();          // row rr + R + 1 has landed
+                v_slide(V, *slot(rr + R + 1), *slot(rr - R));
+            }
         }
+        cp_async_wait<0>();
     }
 }
 
@@ -239,16 +250,33 @@ static cudaError_t launch_swar8_r(const Frame& cur, const Frame& nxt, const Rule
     const int strips = (n + kStripOut - 1) / kStripOut;
     const int bands = (n + band_rows - 1) / band_rows;
     const int items = strips * bands;
-    const int warps_per_cta = 4;
+    const int smem = kPlainWarps * kRingRows * 32 * (int)sizeof(uint4);
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_plain_swar8<R>, warps_per_cta * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_plain_swar8<R>, kPlainWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
-    int ctas = std::min((items + warps_per_cta - 1) / warps_per_cta, sms * per_sm);
-    k_plain_swar8<R><<<ctas, warps_per_cta * 32, 0, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch, band_rows,
+    int ctas = std::min((items + kPlainWarps - 1) / kPlainWarps, sms * per_sm);
+    k_plain_swar8<R><<<ctas, kPlainWarps * 32, smem, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch, band_rows,
                                                          strips, items, q);
     return cudaGetLastError();
+}
+
+template <int R>
+static cudaError_t prepare_swar8_r() {
+    const int smem = kPlainWarps * kRingRows * 32 * (int)sizeof(uint4);
+    return cudaFuncSetAttribute(k_plain_swar8<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+cudaError_t plain_prepare(int radius) {
+    switch (radius) {
+        case 1: return prepare_swar8_r<1>();
+        case 2: return prepare_swar8_r<2>();
+        case 3: return prepare_swar8_r<3>();
+        case 4: return prepare_swar8_r<4>();
+        case 5: return prepare_swar8_r<5>();
+        default: return cudaSuccess;
+    }
 }
 
 cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows,

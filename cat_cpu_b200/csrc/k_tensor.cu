@@ -158,7 +158,10 @@ __host__ __device__ constexpr uint32_t idesc_u8(int N, bool b_mn_major) {
 //   warp 0  TMA producer: X tiles into a 3-stage ring (x_full / x_empty);
 //   warp 1  MMA issuer:   product 1 of tile t into TMEM stage t % 2, then
 //                          product 2 of tile t-1 once its H is back in smem;
-//   warps 2-5 epilogue:  re-quantise H(t+1), then rule + store C(t).
+//   warps 2.. epilogue:  kEpiGroups groups of 4 warps (one warp per TMEM lane
+//                          quarter); group g handles the 32-column blocks
+//                          g, g + kEpiGroups, ... of every tile: re-quantise
+//                          H(t+1), then rule + store C(t).
 // TMEM: two accumulator stages of 256 columns (H and then C of one tile share
 // a stage).  All mbarrier waits are bounded.
 // ---------------------------------------------------------------------------
@@ -170,8 +173,9 @@ constexpr int kXStages = 3;
 constexpr int kAccStages = 2;
 constexpr int kAccCols = 256;          // TMEM columns per accumulator stage
 constexpr int kN1 = 32;                // product-1 column chunk
-constexpr int kThreads = 192;          // 6 warps
-constexpr int kEpiWarps = 4;
+constexpr int kEpiGroups = 4;          // epilogue warp groups (column blocks round-robin)
+constexpr int kEpiWarps = 4 * kEpiGroups;
+constexpr int kThreads = 64 + 32 * kEpiWarps;  // producer + MMA + epilogue warps
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any legitimate wait
 
 struct TensorParams {
@@ -370,6 +374,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
     } else {
         // ---------------------------- epilogue ------------------------------
         const int q = warp & 3;                 // TMEM lane quarter of this warp
+        const int grp = (warp - 2) >> 2;        // column group
         const int row = q * 32 + lane;          // H row / output row within the tile
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
         const bool small = (2 * R + 1) * (2 * R + 1) <= 127;
@@ -382,7 +387,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             tc_fence_after();
             uint8_t* hsb = hs + as * 128 * Tc;
             const uint32_t trow = tmem + as * kAccCols + lane_off;
-            for (int cb = 0; cb < Tc; cb += 32) {
+            for (int cb = 32 * grp; cb < Tc; cb += 32 * kEpiGroups) {
                 uint32_t v[32];
                 tmem_ld32(trow + cb, v);
 #pragma unroll
@@ -414,7 +419,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             const uint8_t* xrow = xs + st * kXBytes + (xr & 127) * 128;
             uint8_t* orow = p.out + (size_t)(p.H + gi) * (size_t)p.pitch + p.H + c0;
             const uint32_t trow = tmem + as * kAccCols + lane_off;
-            for (int cb = 0; cb < Tc; cb += 32) {
+            for (int cb = 32 * grp; cb < Tc; cb += 32 * kEpiGroups) {
                 uint32_t v[32];
                 tmem_ld32(trow + cb, v);
                 if (!row_ok) continue;

@@ -201,6 +201,13 @@ extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin
         }
     }
     if (variant == LTL_VARIANT_PLAIN) c->band_rows = plain_swar8_band_rows(n, device);
+    if (variant == LTL_VARIANT_PLAIN) e = plain_prepare(radius);
+    if (variant == LTL_VARIANT_PACKED) e = packed_prepare(radius);
+    if (e != cudaSuccess) {
+        ltl_set_error("ltl_create: kernel setup failed: %s", cudaGetErrorString(e));
+        release(c);
+        return LTL_ECUDA;
+    }
     if (variant == LTL_VARIANT_PACKED) {
         PackedFrame p{};
         p.n = n;

@@ -14,6 +14,10 @@ cudaError_t launch_halo_fill(const Frame& f, cudaStream_t s);
 
 // K1 fast path: SWAR 8-bit lanes, warp-shuffle row sums; R <= 5.
 bool plain_swar8_supported(int radius);
+// One-time function attributes (dynamic shared memory) so that launches can be
+// captured in CUDA graphs without configuration calls.
+cudaError_t plain_prepare(int radius);
+cudaError_t packed_prepare(int radius);
 cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows,
                                cudaStream_t s);
 int plain_swar8_band_rows(int n, int device);
