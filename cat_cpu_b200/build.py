@@ -69,9 +69,8 @@ def build(force=False, jobs=None, verbose=False, ptxas_verbose=False):
     if errors:
         raise RuntimeError("\n".join(errors))
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        # static CUDA runtime: the library does not depend on which libcudart.so.12
-        # the host process (e.g. torch) loaded first
-        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", "g++", "-cudart", "static", "-o", LIB] + objs + \
+        # shared CUDA runtime: one runtime instance per process, shared with torch
+        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", "g++", "-cudart", "shared", "-o", LIB] + objs + \
             ["-lpthread", "-ldl", "-lrt"]
         if verbose:
             print(" ".join(cmd), flush=True)

@@ -368,6 +368,7 @@ struct ltl_batch {
     uint8_t* staging = nullptr;
     long long total_cells = 0;
     bool cur_is_a = true;
+    bool no_graph = false;
     cudaStream_t own = nullptr, stream = nullptr, aux = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
     // graph cache: (steps, parity) -> exec
@@ -438,7 +439,7 @@ static int batch_build(ltl_batch* b, int flags) {
     }
     b->arena_words = words + 64;
     b->total_cells = cells;
-    const bool no_resident = (flags & 1) != 0;
+    const bool no_resident = (flags & LTL_BATCH_STREAM_ALL) != 0;
     std::vector<int> streamed_all;
     for (int i = 0; i < count; ++i) {
         BatchClass& c = b->classes[cls_id[i]];
@@ -525,6 +526,7 @@ extern "C" int ltl_batch_create(ltl_batch** out, int device, const ltl_grid_desc
         return LTL_ECUDA;
     }
     b->stream = b->own;
+    b->no_graph = (flags & LTL_BATCH_NO_GRAPH) != 0;
     int rc = batch_build(b, flags);
     if (rc != LTL_OK) {
         batch_release(b);
@@ -634,34 +636,50 @@ extern "C" int ltl_batch_download(ltl_batch* b, int grid, uint8_t* inner, size_t
 }
 
 // Enqueue `steps` generations of every grid (stream-ordered on b->stream).
-static cudaError_t enqueue_steps(ltl_batch* b, int steps) {
+// On failure, `what` names the call that failed.
+static cudaError_t enqueue_steps(ltl_batch* b, int steps, const char** what) {
     cudaError_t e = cudaSuccess;
     uint32_t* a0 = cur_arena(b);
     uint32_t* a1 = nxt_arena(b);
     bool any_res = false;
     for (auto& c : b->classes) any_res |= !c.resident.empty();
     if (any_res) {
+        *what = "fork event record";
         e = cudaEventRecord(b->fork, b->stream);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->aux, b->fork, 0);
+        if (e == cudaSuccess) {
+            *what = "fork stream wait";
+            e = cudaStreamWaitEvent(b->aux, b->fork, 0);
+        }
         uint32_t* dst = (steps % 2) ? a1 : a0;
         for (auto& c : b->classes) {
             if (c.resident.empty() || e != cudaSuccess) continue;
+            *what = "resident kernel launch";
             e = batch_resident_dispatch(c.rule.radius, a0, dst, b->d_grids, c.d_resident, (int)c.resident.size(),
                                         steps, c.pr, c.res_smem, b->sms, b->aux);
         }
-        if (e == cudaSuccess) e = cudaEventRecord(b->join, b->aux);
+        if (e == cudaSuccess) {
+            *what = "join event record";
+            e = cudaEventRecord(b->join, b->aux);
+        }
     }
     for (int s = 0; s < steps && e == cudaSuccess; ++s) {
         const uint32_t* src = (s % 2) ? a1 : a0;
         uint32_t* dst = (s % 2) ? a0 : a1;
         for (auto& c : b->classes) {
             if (c.n_items == 0 || e != cudaSuccess) continue;
+            *what = "streamed step kernel launch";
             e = batch_step_dispatch(c.rule.radius, src, dst, b->d_grids, c.d_items, c.n_items, c.pr, b->sms,
                                     b->stream);
         }
-        if (e == cudaSuccess) e = refresh_streamed_halo(b, dst, b->stream);
+        if (e == cudaSuccess) {
+            *what = "halo kernel launch";
+            e = refresh_streamed_halo(b, dst, b->stream);
+        }
     }
-    if (any_res && e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join, 0);
+    if (any_res && e == cudaSuccess) {
+        *what = "join stream wait";
+        e = cudaStreamWaitEvent(b->stream, b->join, 0);
+    }
     return e;
 }
 
@@ -672,16 +690,28 @@ extern "C" int ltl_batch_step(ltl_batch* b, int steps) {
     }
     if (steps == 0) return LTL_OK;
     BATCH_CUDA(cudaSetDevice(b->device));
+    const char* what = "";
+    if (b->no_graph) {
+        cudaError_t e = enqueue_steps(b, steps, &what);
+        if (e != cudaSuccess) {
+            ltl_set_error("ltl_batch_step: %s failed: %s", what, cudaGetErrorString(e));
+            return LTL_ECUDA;
+        }
+        if (steps % 2) b->cur_is_a = !b->cur_is_a;
+        return LTL_OK;
+    }
     const std::pair<int, int> key(steps, b->cur_is_a ? 0 : 1);
     auto it = b->graphs.find(key);
     if (it == b->graphs.end()) {
         cudaGraph_t g = nullptr;
         BATCH_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e = enqueue_steps(b, steps);
+        cudaError_t e = enqueue_steps(b, steps, &what);
         cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
         if (e != cudaSuccess || e2 != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
-            ltl_set_error("ltl_batch_step: graph capture failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+            ltl_set_error("ltl_batch_step: graph capture failed at %s: %s / end capture: %s", what,
+                          cudaGetErrorString(e), cudaGetErrorString(e2));
+            cudaGetLastError();
             return LTL_ECUDA;
         }
         cudaGraphExec_t ex = nullptr;

@@ -138,6 +138,10 @@ typedef struct {
 
 typedef struct ltl_batch ltl_batch;
 
+/* ltl_batch_create flags */
+#define LTL_BATCH_STREAM_ALL 1  /* no shared-memory-resident grids: stream every grid every step */
+#define LTL_BATCH_NO_GRAPH 2    /* launch the step loop directly instead of replaying a CUDA graph */
+
 int ltl_batch_create(ltl_batch** out, int device, const ltl_grid_desc* descs, int count, int flags);
 int ltl_batch_destroy(ltl_batch* b);
 int ltl_batch_set_stream(ltl_batch* b, void* stream);
