@@ -199,7 +199,7 @@ k_batch_resident(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, c
 #pragma unroll 1
                 for (int dy = -R; dy <= R; ++dy) {
                     uint32_t h[PH];
-                    hcount<R, PH>(rowp(r0 + dy), fw, active, lane, h);
+                    hcount<R, PH, false>(rowp(r0 + dy), fw, active, lane, h);
                     planes_add<PB, PH>(B, h);
                 }
 #pragma unroll 1
@@ -212,9 +212,9 @@ k_batch_resident(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, c
                     }
                     if (r + 1 < r1) {
                         uint32_t h[PH];
-                        hcount<R, PH>(rowp(r - R), fw, active, lane, h);
+                        hcount<R, PH, false>(rowp(r - R), fw, active, lane, h);
                         planes_sub<PB, PH>(B, h);
-                        hcount<R, PH>(rowp(r + R + 1), fw, active, lane, h);
+                        hcount<R, PH, false>(rowp(r + R + 1), fw, active, lane, h);
                         planes_add<PB, PH>(B, h);
                     }
                 }
@@ -460,9 +460,13 @@ static int batch_build(ltl_batch* b, int flags) {
         BATCH_CUDA(cudaMemcpy(b->d_streamed_all, streamed_all.data(), sizeof(int) * streamed_all.size(),
                               cudaMemcpyHostToDevice));
     }
+    // one shared-memory limit per kernel instantiation (radius): the largest any class of that radius needs
+    std::map<int, size_t> smem_by_radius;
+    for (auto& c : b->classes)
+        if (!c.resident.empty()) smem_by_radius[c.rule.radius] = std::max(smem_by_radius[c.rule.radius], c.res_smem);
+    for (auto& kv : smem_by_radius) BATCH_CUDA(batch_prepare_dispatch(kv.first, kv.second));
     for (auto& c : b->classes) {
         if (!c.resident.empty()) {
-            BATCH_CUDA(batch_prepare_dispatch(c.rule.radius, c.res_smem));
             BATCH_CUDA(cudaMalloc(&c.d_resident, sizeof(int) * c.resident.size()));
             BATCH_CUDA(cudaMemcpy(c.d_resident, c.resident.data(), sizeof(int) * c.resident.size(),
                                   cudaMemcpyHostToDevice));
@@ -517,11 +521,12 @@ extern "C" int ltl_batch_create(ltl_batch** out, int device, const ltl_grid_desc
     b->descs.assign(descs, descs + count);
     cudaSetDevice(device);
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
-    if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess) {
-        ltl_set_error("ltl_batch_create: stream/event creation failed");
+    cudaError_t se = cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking);
+    if (se == cudaSuccess) se = cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking);
+    if (se == cudaSuccess) se = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    if (se == cudaSuccess) se = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
+    if (se != cudaSuccess) {
+        ltl_set_error("ltl_batch_create: stream/event creation failed: %s", cudaGetErrorString(se));
         batch_release(b);
         return LTL_ECUDA;
     }

@@ -119,15 +119,23 @@ inline PackedRule make_packed_rule(const Rule& r) {
 }
 
 // Horizontal window count of one frame row for word column fw (frame column).
-// All lanes of the warp must call it together (shuffles).
-template <int R, int PH>
+// All lanes of the warp must call it together (shuffles).  kGlobal selects the
+// read-only global load path; rows in shared memory use plain loads.
+template <int R, int PH, bool kGlobal = true>
 __device__ __forceinline__ void hcount(const uint32_t* __restrict__ row, int fw, bool active, int lane,
                                        uint32_t (&h)[PH]) {
-    uint32_t own = active ? __ldg(row + fw) : 0u;
+    auto ld = [&](int i) -> uint32_t {
+        if constexpr (kGlobal) {
+            return __ldg(row + i);
+        } else {
+            return row[i];
+        }
+    };
+    uint32_t own = active ? ld(fw) : 0u;
     uint32_t left = __shfl_up_sync(0xffffffffu, own, 1);
     uint32_t right = __shfl_down_sync(0xffffffffu, own, 1);
-    if (lane == 0 && active) left = __ldg(row + fw - 1);
-    if (lane == 31 && active) right = __ldg(row + fw + 1);
+    if (lane == 0 && active) left = ld(fw - 1);
+    if (lane == 31 && active) right = ld(fw + 1);
     uint32_t x[2 * R + 1];
 #pragma unroll
     for (int d = -R; d <= R; ++d) {
