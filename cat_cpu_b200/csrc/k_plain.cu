@@ -150,6 +150,15 @@ constexpr int kRingRows = 32;  // power of two >= 2R + 2 + kAhead
 constexpr int kAhead = 8;
 constexpr int kPlainWarps = 4;
 
+// Store the first `count` (< 16) bytes of v; compile-time lane indices only, so
+// v stays in registers.
+__device__ __forceinline__ void store_partial16(uint8_t* dst, uint4 v, int count) {
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+        if (j < count) dst[j] = (uint8_t)(w[j >> 2] >> (8 * (j & 3)));
+}
+
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
                  "l"(gmem)
@@ -214,8 +223,7 @@ k_plain_swar8(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n,
                 if (x + 16 <= n) {
                     *(uint4*)dst = o;
                 } else {
-                    const uint32_t ow[4] = {o.x, o.y, o.z, o.w};
-                    for (int j = 0; j < n - x; ++j) dst[j] = (uint8_t)(ow[j >> 2] >> (8 * (j & 3)));
+                    store_partial16(dst, o, n - x);
                 }
             }
             if (rr + 1 < r1) {

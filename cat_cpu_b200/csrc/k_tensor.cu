@@ -428,7 +428,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
                     const int xc = PADC + cb + 16 * h;  // X column of these 16 cells
                     const int atom = xc >> 7, ch = (xc & 127) >> 4;
                     const uint4 s4 = *(const uint4*)(xrow + atom * kAtomBytes + ((ch ^ (xr & 7)) << 4));
-                    const uint32_t sw[4] = {s4.x, s4.y, s4.z, s4.w};
+                    const uint32_t sw[4] = {s4.x, s4.y, s4.z, s4.w};  // compile-time indices only
                     uint32_t o[4];
 #pragma unroll
                     for (int qq = 0; qq < 4; ++qq) {
@@ -451,8 +451,10 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
                     if (gj + 16 <= p.n) {
                         *(uint4*)(orow + cb + 16 * h) = make_uint4(o[0], o[1], o[2], o[3]);
                     } else if (gj < p.n) {
-                        for (int e = 0; e < p.n - gj; ++e)
-                            orow[cb + 16 * h + e] = (uint8_t)((o[e >> 2] >> (8 * (e & 3))) & 0xff);
+                        const int cnt = p.n - gj;
+#pragma unroll
+                        for (int e = 0; e < 16; ++e)
+                            if (e < cnt) orow[cb + 16 * h + e] = (uint8_t)((o[e >> 2] >> (8 * (e & 3))) & 0xff);
                     }
                 }
             }
