@@ -1,0 +1,134 @@
+"""Shape autotuner: sweeps the kernels' work-item shapes on the device and writes
+the winners to cat_cpu_b200/tuning/ltl_tuning.txt, which libltl_b200 reads at
+ltl_create / ltl_batch_create.
+
+    python -m cat_cpu_b200.autotune [--quick] [--out DIR]
+
+This is the analogue of the reference project's region-count landscape search
+(NREGIONS_H/V over 1..30 x 1..30, scripts/exploreRegionSizesLandscape.py:21-39,
+scripts/extractBestRegionSize.py): here the swept shapes are
+  plain / packed   band_rows: rows a warp walks down per work item (the vertical
+                   window is restarted once per band, so longer bands re-read less
+                   but leave fewer items to balance over 148 SMs);
+  batch            stream_band_rows of the streamed per-step kernels, and
+                   resident_max_bytes: which grids are kept in shared memory for
+                   a whole multi-step launch and which are streamed each step.
+The full landscape (every candidate's time) is written next to the table.
+"""
+import argparse
+import concurrent.futures as cf
+import os
+import time
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+
+
+def _time_steps(torch, solver, stream, steps, reps=3):
+    best = None
+    for _ in range(reps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        solver.doSteps(steps)
+        b.record(stream)
+        stream.synchronize()
+        ms = a.elapsed_time(b) / steps
+        best = ms if best is None else min(best, ms)
+    return best
+
+
+def tune_single(torch, C, variant, n, radius, rule, candidates, steps):
+    vcode = {"plain": C.VARIANT_PLAIN, "packed": C.VARIANT_PACKED}[variant]
+    g = C.generate_state(n, 12345, 0.5, 1)
+    stream = torch.cuda.Stream()
+    s = C.CUDASolver(n, radius, rule, variant=vcode)
+    s.set_stream(stream.cuda_stream)
+    rows = []
+    try:
+        for br in candidates:
+            s.set_param("band_rows", br)
+            s.setState(g)
+            s.doSteps(16)
+            ms = _time_steps(torch, s, stream, steps)
+            rows.append((br, ms))
+    finally:
+        s.close()
+    best = min(rows, key=lambda x: x[1])
+    return best, rows
+
+
+def tune_batch(torch, C, band_candidates, resident_candidates, steps):
+    from cat_cpu_b200.workloads import batch_config
+    cfg = batch_config()
+    with cf.ThreadPoolExecutor(os.cpu_count() or 8) as ex:
+        grids = list(ex.map(lambda c: C.generate_state(c[0], c[4], c[3], 1), cfg))
+    flat = np.concatenate([g.ravel() for g in grids])
+    stream = torch.cuda.Stream()
+    b = C.Batch([(n, r, rule) for (n, r, rule, d, s) in cfg])
+    rows = []
+    try:
+        b.set_stream(stream.cuda_stream)
+        for rm in resident_candidates:
+            for br in band_candidates:
+                b.set_param("resident_max_bytes", rm)
+                b.set_param("stream_band_rows", br)
+                b.upload_all(flat)
+                b.step(steps)          # builds and warms the graph
+                b.synchronize()
+                a = torch.cuda.Event(enable_timing=True)
+                e = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                b.step(steps)
+                e.record(stream)
+                stream.synchronize()
+                rows.append(((br, rm), a.elapsed_time(e)))
+    finally:
+        b.close()
+    best = min(rows, key=lambda x: x[1])
+    return best, rows
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--quick", action="store_true", help="fewer candidates")
+    ap.add_argument("--out", default=os.path.join(PKG, "tuning"))
+    args = ap.parse_args()
+    import torch
+    import cat_cpu_b200 as C
+    from cat_cpu_b200.workloads import scaled_rule, BOSCO_R5
+
+    os.makedirs(args.out, exist_ok=True)
+    dev = torch.cuda.get_device_name(0)
+    table = [f"# autotuned on {dev} by cat_cpu_b200/autotune.py, {time.strftime('%Y-%m-%d %H:%M:%S')}"]
+    land = [f"# landscape ({dev}): candidate -> ms per step (single grids) or per 256-step batch run"]
+    plain_c = [64, 128, 256, 512] if args.quick else [64, 96, 128, 192, 256, 384, 512]
+    packed_c = [32, 64, 128] if args.quick else [32, 48, 64, 96, 128, 192, 256]
+    jobs = [("plain", 16384, 5, BOSCO_R5, plain_c), ("plain", 4096, 5, BOSCO_R5, plain_c),
+            ("packed", 16384, 5, BOSCO_R5, packed_c), ("packed", 32768, 5, BOSCO_R5, packed_c)]
+    for r in (1, 2, 4, 8, 16, 32):
+        if not args.quick or r in (1, 8):
+            jobs.append(("packed", 32768, r, scaled_rule(r), packed_c))
+    for variant, n, r, rule, cands in jobs:
+        (br, ms), rows = tune_single(torch, C, variant, n, r, rule, cands, 20)
+        lo, hi = (8192, 1 << 30) if n >= 16384 else (1, 8191)
+        table.append(f"variant={variant} radius={r} nmin={lo} nmax={hi} band_rows={br}")
+        land.append(f"{variant} n={n} R={r}: " + ", ".join(f"{c}:{t:.4f}" for c, t in rows) + f"  -> {br}")
+        print(land[-1], flush=True)
+    band_c = [32, 64, 128] if args.quick else [32, 48, 64, 96, 128]
+    res_c = [0, 225280] if args.quick else [0, 65536, 131072, 225280]
+    ((br, rm), ms), rows = tune_batch(torch, C, band_c, res_c, 256)
+    table.append(f"variant=batch radius=* stream_band_rows={br} resident_max_bytes={rm}")
+    land.append("batch (stream_band_rows, resident_max_bytes): " +
+                ", ".join(f"{c}:{t:.2f}" for c, t in rows) + f"  -> {(br, rm)}")
+    print(land[-1], flush=True)
+    with open(os.path.join(args.out, "ltl_tuning.txt"), "w") as f:
+        f.write("\n".join(table) + "\n")
+    with open(os.path.join(args.out, "landscape.txt"), "w") as f:
+        f.write("\n".join(land) + "\n")
+    print("wrote", os.path.join(args.out, "ltl_tuning.txt"))
+
+
+if __name__ == "__main__":
+    main()

@@ -17,6 +17,7 @@
 //     batched halo refresh; the whole step loop is captured in a CUDA graph, and
 //     the resident launches run concurrently on a forked stream.
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <new>
 #include <vector>
@@ -360,6 +361,9 @@ struct ltl_batch {
     std::vector<BatchGrid> grids;
     std::vector<ltl_grid_desc> descs;
     std::vector<BatchClass> classes;
+    std::vector<int> cls_id;
+    int stream_band_rows = 64;
+    long long resident_max = 0;
     BatchGrid* d_grids = nullptr;
     int* d_streamed_all = nullptr;
     int n_streamed_all = 0;
@@ -404,47 +408,29 @@ static void batch_release(ltl_batch* b) {
         }                                                                                          \
     } while (0)
 
-static int batch_build(ltl_batch* b, int flags) {
-    const int count = (int)b->descs.size();
-    // rule classes
-    std::map<std::vector<int>, int> cls_of;
-    size_t words = 0;
-    long long cells = 0;
-    b->grids.resize(count);
-    std::vector<int> cls_id(count);
-    for (int i = 0; i < count; ++i) {
-        const ltl_grid_desc& d = b->descs[i];
-        std::vector<int> key = {d.radius, d.smin, d.smax, d.bmin, d.bmax};
-        auto it = cls_of.find(key);
-        if (it == cls_of.end()) {
-            BatchClass c;
-            c.rule = Rule{d.radius, d.smin, d.smax, d.bmin, d.bmax};
-            c.pr = make_packed_rule(c.rule);
-            it = cls_of.emplace(key, (int)b->classes.size()).first;
-            b->classes.push_back(c);
-        }
-        cls_id[i] = it->second;
-        BatchGrid g{};
-        g.n = d.n;
-        g.nw = (d.n + 31) / 32;
-        g.HR = d.radius + 1;
-        g.wp = (g.nw + 3 + 3) / 4 * 4;
-        g.R = d.radius;
-        g.off = (long long)words;
-        g.cell_off = cells;
-        words += (size_t)(g.n + 2 * g.HR) * g.wp;
-        words = (words + 31) / 32 * 32;
-        cells += (long long)g.n * g.n;
-        b->grids[i] = g;
+// Work plan: which grids are resident, and the streamed work lists.  Rebuilt
+// when a shape parameter changes (the arenas' layout does not depend on it).
+static int batch_plan(ltl_batch* b) {
+    for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    b->graphs.clear();
+    for (auto& c : b->classes) {
+        if (c.d_resident) cudaFree(c.d_resident);
+        if (c.d_items) cudaFree(c.d_items);
+        c.d_resident = nullptr;
+        c.d_items = nullptr;
+        c.resident.clear();
+        c.streamed.clear();
+        c.n_items = 0;
+        c.res_smem = 0;
     }
-    b->arena_words = words + 64;
-    b->total_cells = cells;
-    const bool no_resident = (flags & LTL_BATCH_STREAM_ALL) != 0;
+    if (b->d_streamed_all) cudaFree(b->d_streamed_all);
+    b->d_streamed_all = nullptr;
+    const int count = (int)b->grids.size();
     std::vector<int> streamed_all;
     for (int i = 0; i < count; ++i) {
-        BatchClass& c = b->classes[cls_id[i]];
+        BatchClass& c = b->classes[b->cls_id[i]];
         const size_t need = res_smem_dispatch(b->grids[i].R, b->grids[i].n);
-        if (!no_resident && need <= (size_t)kResSmemLimit) {
+        if (need <= (size_t)b->resident_max) {
             c.resident.push_back(i);
             c.res_smem = std::max(c.res_smem, need);
         } else {
@@ -452,8 +438,6 @@ static int batch_build(ltl_batch* b, int flags) {
             streamed_all.push_back(i);
         }
     }
-    BATCH_CUDA(cudaMalloc(&b->d_grids, sizeof(BatchGrid) * count));
-    BATCH_CUDA(cudaMemcpy(b->d_grids, b->grids.data(), sizeof(BatchGrid) * count, cudaMemcpyHostToDevice));
     b->n_streamed_all = (int)streamed_all.size();
     if (!streamed_all.empty()) {
         BATCH_CUDA(cudaMalloc(&b->d_streamed_all, sizeof(int) * streamed_all.size()));
@@ -475,7 +459,7 @@ static int batch_build(ltl_batch* b, int flags) {
         for (int gi : c.streamed) {
             const BatchGrid& g = b->grids[gi];
             const int strips = (g.nw + 1 + 31) / 32;
-            const int band_rows = 64;
+            const int band_rows = b->stream_band_rows;
             for (int r0 = 0; r0 < g.n; r0 += band_rows)
                 for (int ws = 0; ws < strips; ++ws) items.push_back(make_int4(gi, r0, std::min(g.n, r0 + band_rows), ws));
         }
@@ -485,12 +469,83 @@ static int batch_build(ltl_batch* b, int flags) {
             BATCH_CUDA(cudaMemcpy(c.d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
         }
     }
+    return LTL_OK;
+}
+
+static int batch_build(ltl_batch* b, int flags) {
+    const int count = (int)b->descs.size();
+    // rule classes
+    std::map<std::vector<int>, int> cls_of;
+    size_t words = 0;
+    long long cells = 0;
+    b->grids.resize(count);
+    b->cls_id.resize(count);
+    int rmax = 1;
+    for (int i = 0; i < count; ++i) {
+        const ltl_grid_desc& d = b->descs[i];
+        std::vector<int> key = {d.radius, d.smin, d.smax, d.bmin, d.bmax};
+        auto it = cls_of.find(key);
+        if (it == cls_of.end()) {
+            BatchClass c;
+            c.rule = Rule{d.radius, d.smin, d.smax, d.bmin, d.bmax};
+            c.pr = make_packed_rule(c.rule);
+            it = cls_of.emplace(key, (int)b->classes.size()).first;
+            b->classes.push_back(c);
+        }
+        b->cls_id[i] = it->second;
+        BatchGrid g{};
+        g.n = d.n;
+        g.nw = (d.n + 31) / 32;
+        g.HR = d.radius + 1;
+        g.wp = (g.nw + 3 + 3) / 4 * 4;
+        g.R = d.radius;
+        g.off = (long long)words;
+        g.cell_off = cells;
+        words += (size_t)(g.n + 2 * g.HR) * g.wp;
+        words = (words + 31) / 32 * 32;
+        cells += (long long)g.n * g.n;
+        b->grids[i] = g;
+        rmax = std::max(rmax, d.radius);
+    }
+    b->arena_words = words + 64;
+    b->total_cells = cells;
+    b->stream_band_rows = (int)tuning_lookup("batch", -1, 0, "stream_band_rows", 64);
+    b->resident_max = (flags & LTL_BATCH_STREAM_ALL) ? 0
+                                                     : tuning_lookup("batch", -1, 0, "resident_max_bytes", kResSmemLimit);
+    BATCH_CUDA(cudaMalloc(&b->d_grids, sizeof(BatchGrid) * count));
+    BATCH_CUDA(cudaMemcpy(b->d_grids, b->grids.data(), sizeof(BatchGrid) * count, cudaMemcpyHostToDevice));
     for (auto& a : b->arena) {
         BATCH_CUDA(cudaMalloc(&a, b->arena_words * sizeof(uint32_t)));
         BATCH_CUDA(cudaMemset(a, 0, b->arena_words * sizeof(uint32_t)));
     }
     BATCH_CUDA(cudaMalloc(&b->staging, (size_t)std::max<long long>(cells, 1)));
-    return LTL_OK;
+    return batch_plan(b);
+}
+
+extern "C" int ltl_batch_set_param(ltl_batch* b, const char* name, long long value) {
+    if (!b || !name) {
+        ltl_set_error("ltl_batch_set_param: bad arguments");
+        return LTL_EINVAL;
+    }
+    BATCH_CUDA(cudaSetDevice(b->device));
+    BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    if (std::strcmp(name, "stream_band_rows") == 0) {
+        if (value < 8 || value > 4096) {
+            ltl_set_error("ltl_batch_set_param: stream_band_rows must be in [8, 4096]");
+            return LTL_EINVAL;
+        }
+        b->stream_band_rows = (int)value;
+    } else if (std::strcmp(name, "resident_max_bytes") == 0) {
+        if (value < 0 || value > kResSmemLimit) {
+            ltl_set_error("ltl_batch_set_param: resident_max_bytes must be in [0, %d]", kResSmemLimit);
+            return LTL_EINVAL;
+        }
+        b->resident_max = value;
+    } else {
+        ltl_set_error("ltl_batch_set_param: unknown parameter '%s'", name);
+        return LTL_EINVAL;
+    }
+    return batch_plan(b);
 }
 
 extern "C" int ltl_batch_create(ltl_batch** out, int device, const ltl_grid_desc* descs, int count, int flags) {

@@ -116,12 +116,12 @@ bool packed_supported(int n, int radius) { return radius >= 1 && radius <= 32 &&
 
 template <int R>
 static cudaError_t launch_packed_r(const PackedFrame& c, const PackedFrame& x, const PackedRule& pr,
-                                   cudaStream_t s) {
+                                   int band_override, cudaStream_t s) {
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int n_wstrips = (c.nw + 1 + 31) / 32;
-    const int band_rows = packed_band_rows(c.n, n_wstrips, sms);
+    const int band_rows = band_override > 0 ? band_override : packed_band_rows(c.n, n_wstrips, sms);
     const int bands = (c.n + band_rows - 1) / band_rows;
     const int items = n_wstrips * bands;
     const int smem = PackedRing<R>::fits ? PackedRing<R>::BYTES : 0;
@@ -153,12 +153,12 @@ cudaError_t packed_prepare(int radius) {
     }
 }
 
-cudaError_t launch_packed_step(const PackedFrame& cur, const PackedFrame& nxt, const Rule& rule,
+cudaError_t launch_packed_step(const PackedFrame& cur, const PackedFrame& nxt, const Rule& rule, int band_rows,
                                cudaStream_t s) {
     PackedRule pr = make_packed_rule(rule);
     switch (rule.radius) {
 #define LTL_PR(r) \
-    case r: return launch_packed_r<r>(cur, nxt, pr, s);
+    case r: return launch_packed_r<r>(cur, nxt, pr, band_rows, s);
         LTL_PR(1) LTL_PR(2) LTL_PR(3) LTL_PR(4) LTL_PR(5) LTL_PR(6) LTL_PR(7) LTL_PR(8)
         LTL_PR(9) LTL_PR(10) LTL_PR(11) LTL_PR(12) LTL_PR(13) LTL_PR(14) LTL_PR(15) LTL_PR(16)
         LTL_PR(17) LTL_PR(18) LTL_PR(19) LTL_PR(20) LTL_PR(21) LTL_PR(22) LTL_PR(23) LTL_PR(24)

@@ -155,23 +155,24 @@ __host__ __device__ constexpr uint32_t idesc_u8(int N, bool b_mn_major) {
 // Tile geometry and the persistent, warp-specialised kernel
 //
 // One CTA per SM walks a strided list of tiles.  Warp roles:
-//   warp 0  TMA producer: X tiles into a 3-stage ring (x_full / x_empty);
-//   warp 1  MMA issuer:   product 1 of tile t into TMEM stage t % 2, then
-//                          product 2 of tile t-1 once its H is back in smem;
-//   warps 2.. epilogue:  kEpiGroups groups of 4 warps (one warp per TMEM lane
-//                          quarter); group g handles the 32-column blocks
-//                          g, g + kEpiGroups, ... of every tile: re-quantise
-//                          H(t+1), then rule + store C(t).
-// TMEM: two accumulator stages of 256 columns (H and then C of one tile share
-// a stage).  All mbarrier waits are bounded.
+//   warp 0    TMA producer: X tiles into a kXStages ring (x_full / x_empty);
+//   warp 1    MMA issuer, per tile j:  product 2 of tile j-1 (once H(j-1) is in
+//             shared memory and C of tile j-2 has been read), then product 1 of
+//             tile j (H's TMEM columns are free as soon as H(j-1) was read);
+//   warps 2.. epilogue: kEpiGroups groups of 4 warps (one warp per TMEM lane
+//             quarter); group g handles the 32-column blocks g, g + kEpiGroups,
+//             ... of every tile: re-quantise H(j), then rule + store C(j).
+// TMEM holds H (columns [0, Tc)) and C (columns [256, 256 + Tc)) separately, so
+// product 1 of the next tile overlaps the rule of the current one and only
+// product 2's latency is on the epilogue's critical path.  All waits are bounded.
 // ---------------------------------------------------------------------------
 constexpr int kAtomBytes = 128 * 128;  // one 128-row x 128-byte swizzle atom
 constexpr int kAtoms = 2;              // X tile = 128 rows x 256 columns
 constexpr int kXBytes = kAtoms * kAtomBytes;
 constexpr int kXCols = 128 * kAtoms;
-constexpr int kXStages = 3;
-constexpr int kAccStages = 2;
-constexpr int kAccCols = 256;          // TMEM columns per accumulator stage
+constexpr int kXStages = 4;
+constexpr int kHCol = 0;               // TMEM column of H
+constexpr int kCCol = 256;             // TMEM column of C
 constexpr int kN1 = 32;                // product-1 column chunk
 constexpr int kEpiGroups = 4;          // epilogue warp groups (column blocks round-robin)
 constexpr int kEpiWarps = 4 * kEpiGroups;
@@ -195,15 +196,15 @@ struct SmemLayout {
     int x_off, hs_off, bh_off, bv_off, bar_off, tmem_off, total;
 };
 
-enum Bar { X_FULL = 0, X_EMPTY = 3, H_FULL = 6, HS_FULL = 8, C_FULL = 10, ACC_EMPTY = 12, NBARS = 14 };
+enum Bar { X_FULL = 0, X_EMPTY = kXStages, H_FULL = 2 * kXStages, HS_FULL, C_FULL, C_EMPTY, NBARS };
 
 __host__ __device__ inline SmemLayout smem_layout(int Tc, int K1c) {
     SmemLayout L{};
     int o = 0;
     L.x_off = o;
-    o += kXStages * kXBytes;                // 96 KB, 1024-aligned stages
+    o += kXStages * kXBytes;                // 1024-aligned stages
     L.hs_off = o;
-    o += kAccStages * 128 * Tc;             // H as u8, MN-major, one buffer per accumulator stage
+    o += 128 * Tc;                          // H as u8, MN-major
     L.bh_off = o;
     o += kN1 * K1c;                         // B_h
     L.bv_off = o;
@@ -242,19 +243,19 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int R = p.R, PADC = p.PADC, Tc = p.Tc, K1c = p.K1c;
     const int ntiles = p.tiles_x * p.tiles_y;
-    constexpr uint32_t kTmemCols = kAccStages * kAccCols;
+    int mine = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) ++mine;
+    constexpr uint32_t kTmemCols = 512;
 
     if (tid == 0) {
         for (int i = 0; i < kXStages; ++i) {
             mbar_init(&bars[X_FULL + i], 1);
             mbar_init(&bars[X_EMPTY + i], kEpiWarps);
         }
-        for (int i = 0; i < kAccStages; ++i) {
-            mbar_init(&bars[H_FULL + i], 1);
-            mbar_init(&bars[HS_FULL + i], kEpiWarps);
-            mbar_init(&bars[C_FULL + i], 1);
-            mbar_init(&bars[ACC_EMPTY + i], kEpiWarps);
-        }
+        mbar_init(&bars[H_FULL], 1);
+        mbar_init(&bars[HS_FULL], kEpiWarps);
+        mbar_init(&bars[C_FULL], 1);
+        mbar_init(&bars[C_EMPTY], kEpiWarps);
         fence_mbar_init();
     }
     if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
@@ -318,39 +319,30 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
     } else if (warp == 1) {
         // --------------------------- MMA issuer -----------------------------
         if (lane == 0) {
-            const uint32_t ba = smem_u32(bh), va = smem_u32(bv), ha0 = smem_u32(hs);
+            const uint32_t ba = smem_u32(bh), va = smem_u32(bv), ha = smem_u32(hs);
             const uint32_t id1 = idesc_u8(kN1, false);
             const uint32_t id2 = idesc_u8(Tc, true);
             bool ok = true;
-            int it = 0;
+            // product 2 of tile j: C = B_v * H(j)
             auto product2 = [&](int j) -> bool {
-                const int as = j % kAccStages;
-                const uint32_t ph = (uint32_t)(j / kAccStages) & 1u;
-                if (!mbar_wait(&bars[HS_FULL + as], ph, kWaitLimitNs)) {
-                    atomicOr(p.err, 2u);
-                    return false;
-                }
+                if (!mbar_wait(&bars[HS_FULL], (uint32_t)j & 1u, kWaitLimitNs)) return false;
+                if (j >= 1 && !mbar_wait(&bars[C_EMPTY], (uint32_t)(j - 1) & 1u, kWaitLimitNs)) return false;
                 tc_fence_after();
-                const uint32_t ha = ha0 + as * 128 * Tc;
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
                     const uint64_t ad = desc_noswz(va + s * 2 * 128 * 16, 128 * 16, 128);
                     const uint64_t bd = desc_noswz(ha + s * 32 * 16, 128, 128 * 16);
-                    mma_i8(tmem + as * kAccCols, ad, bd, id2, s > 0 ? 1u : 0u);
+                    mma_i8(tmem + kCCol, ad, bd, id2, s > 0 ? 1u : 0u);
                 }
-                mma_commit(&bars[C_FULL + as]);
+                mma_commit(&bars[C_FULL]);
                 return true;
             };
-            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
-                const int st = it % kXStages, as = it % kAccStages;
-                // product 1 of tile `it`: needs its X tile and a drained TMEM stage
-                ok = mbar_wait(&bars[X_FULL + st], (uint32_t)(it / kXStages) & 1u, kWaitLimitNs);
-                if (ok && it >= kAccStages)
-                    ok = mbar_wait(&bars[ACC_EMPTY + as], ((uint32_t)(it / kAccStages) & 1u) ^ 1u, kWaitLimitNs);
-                if (!ok) {
-                    atomicOr(p.err, 4u);
-                    break;
-                }
+            for (int j = 0; j < mine && ok; ++j) {
+                const int st = j % kXStages;
+                // product 2 of the previous tile; its wait on HS_FULL also frees H's TMEM columns
+                if (j >= 1) ok = product2(j - 1);
+                if (ok) ok = mbar_wait(&bars[X_FULL + st], (uint32_t)(j / kXStages) & 1u, kWaitLimitNs);
+                if (!ok) break;
                 tc_fence_after();
                 const uint32_t xa = smem_u32(xs + st * kXBytes);
                 for (int n0 = 0; n0 < Tc; n0 += kN1) {
@@ -359,17 +351,13 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
                         const uint32_t a_addr = xa + (col >> 7) * kAtomBytes + (col & 127);
                         const uint64_t ad = desc_k_sw128(a_addr);
                         const uint64_t bd = desc_noswz(ba + s * 2 * kN1 * 16, kN1 * 16, 128);
-                        mma_i8(tmem + as * kAccCols + n0, ad, bd, id1, s > 0 ? 1u : 0u);
+                        mma_i8(tmem + kHCol + n0, ad, bd, id1, s > 0 ? 1u : 0u);
                     }
                 }
-                mma_commit(&bars[H_FULL + as]);
-                // product 2 of the previous tile (its H was re-quantised meanwhile)
-                if (it >= 1 && !product2(it - 1)) {
-                    ok = false;
-                    break;
-                }
+                mma_commit(&bars[H_FULL]);
             }
-            if (ok && it >= 1) product2(it - 1);
+            if (ok && mine >= 1) ok = product2(mine - 1);
+            if (!ok) atomicOr(p.err, 2u);
         }
     } else {
         // ---------------------------- epilogue ------------------------------
@@ -378,39 +366,43 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
         const int row = q * 32 + lane;          // H row / output row within the tile
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
         const bool small = (2 * R + 1) * (2 * R + 1) <= 127;
-        int ntile_mine = 0;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) ++ntile_mine;
         bool ok = true;
-        auto requant = [&](int j) -> bool {
-            const int as = j % kAccStages;
-            if (!mbar_wait(&bars[H_FULL + as], (uint32_t)(j / kAccStages) & 1u, kWaitLimitNs)) return false;
+        int t = blockIdx.x;
+        for (int j = 0; j < mine && ok; ++j, t += gridDim.x) {
+            // re-quantise H(j) to u8, MN-major B operand of product 2
+            if (!mbar_wait(&bars[H_FULL], (uint32_t)j & 1u, kWaitLimitNs)) {
+                ok = false;
+                break;
+            }
             tc_fence_after();
-            uint8_t* hsb = hs + as * 128 * Tc;
-            const uint32_t trow = tmem + as * kAccCols + lane_off;
-            for (int cb = 32 * grp; cb < Tc; cb += 32 * kEpiGroups) {
-                uint32_t v[32];
-                tmem_ld32(trow + cb, v);
+            {
+                const uint32_t trow = tmem + kHCol + lane_off;
+                for (int cb = 32 * grp; cb < Tc; cb += 32 * kEpiGroups) {
+                    uint32_t v[32];
+                    tmem_ld32(trow + cb, v);
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    uint4 w;
-                    w.x = pack4(v[16 * h + 0], v[16 * h + 1], v[16 * h + 2], v[16 * h + 3]);
-                    w.y = pack4(v[16 * h + 4], v[16 * h + 5], v[16 * h + 6], v[16 * h + 7]);
-                    w.z = pack4(v[16 * h + 8], v[16 * h + 9], v[16 * h + 10], v[16 * h + 11]);
-                    w.w = pack4(v[16 * h + 12], v[16 * h + 13], v[16 * h + 14], v[16 * h + 15]);
-                    const int chunk = (cb >> 4) + h;
-                    *(uint4*)(hsb + (chunk * 128 + row) * 16) = w;
+                    for (int h = 0; h < 2; ++h) {
+                        uint4 w;
+                        w.x = pack4(v[16 * h + 0], v[16 * h + 1], v[16 * h + 2], v[16 * h + 3]);
+                        w.y = pack4(v[16 * h + 4], v[16 * h + 5], v[16 * h + 6], v[16 * h + 7]);
+                        w.z = pack4(v[16 * h + 8], v[16 * h + 9], v[16 * h + 10], v[16 * h + 11]);
+                        w.w = pack4(v[16 * h + 12], v[16 * h + 13], v[16 * h + 14], v[16 * h + 15]);
+                        const int chunk = (cb >> 4) + h;
+                        *(uint4*)(hs + (chunk * 128 + row) * 16) = w;
+                    }
                 }
             }
             fence_proxy_async();
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bars[HS_FULL + as]);
-            return true;
-        };
-        auto rule_store = [&](int j, int t) -> bool {
-            const int as = j % kAccStages, st = j % kXStages;
-            if (!mbar_wait(&bars[C_FULL + as], (uint32_t)(j / kAccStages) & 1u, kWaitLimitNs)) return false;
+            if (lane == 0) mbar_arrive(&bars[HS_FULL]);
+            // rule + store C(j)
+            if (!mbar_wait(&bars[C_FULL], (uint32_t)j & 1u, kWaitLimitNs)) {
+                ok = false;
+                break;
+            }
             tc_fence_after();
+            const int st = j % kXStages;
             const int ty = t / p.tiles_x, tx = t % p.tiles_x;
             const int r0 = ty * p.Tr, c0 = tx * Tc;
             const int gi = r0 + row;
@@ -418,7 +410,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             const int xr = row + R;
             const uint8_t* xrow = xs + st * kXBytes + (xr & 127) * 128;
             uint8_t* orow = p.out + (size_t)(p.H + gi) * (size_t)p.pitch + p.H + c0;
-            const uint32_t trow = tmem + as * kAccCols + lane_off;
+            const uint32_t trow = tmem + kCCol + lane_off;
             for (int cb = 32 * grp; cb < Tc; cb += 32 * kEpiGroups) {
                 uint32_t v[32];
                 tmem_ld32(trow + cb, v);
@@ -461,17 +453,9 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             tc_fence_before();
             __syncwarp();
             if (lane == 0) {
-                mbar_arrive(&bars[ACC_EMPTY + as]);
+                mbar_arrive(&bars[C_EMPTY]);
                 mbar_arrive(&bars[X_EMPTY + st]);
             }
-            return true;
-        };
-        // requant(0); for j: requant(j+1); rule(j)
-        if (ntile_mine > 0) ok = requant(0);
-        int t = blockIdx.x;
-        for (int j = 0; j < ntile_mine && ok; ++j, t += gridDim.x) {
-            if (j + 1 < ntile_mine) ok = requant(j + 1);
-            if (ok) ok = rule_store(j, t);
         }
         if (!ok) atomicOr(p.err, 8u);
     }

@@ -52,7 +52,8 @@ struct ltl_ctx {
     unsigned long long* scratch = nullptr;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
-    int band_rows = 64;
+    int band_rows = 64;         // plain: rows per work item
+    int packed_band_rows = 0;   // packed: rows per work item (0: heuristic)
     // packed variant
     PackedFrame pa{}, pb{};
     uint32_t* pwords = nullptr;
@@ -200,7 +201,9 @@ extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin
             return LTL_ENOMEM;
         }
     }
-    if (variant == LTL_VARIANT_PLAIN) c->band_rows = plain_swar8_band_rows(n, device);
+    if (variant == LTL_VARIANT_PLAIN)
+        c->band_rows = (int)tuning_lookup("plain", radius, n, "band_rows", plain_swar8_band_rows(n, device));
+    if (variant == LTL_VARIANT_PACKED) c->packed_band_rows = (int)tuning_lookup("packed", radius, n, "band_rows", 0);
     if (variant == LTL_VARIANT_PLAIN) e = plain_prepare(radius);
     if (variant == LTL_VARIANT_PACKED) e = packed_prepare(radius);
     if (e != cudaSuccess) {
@@ -406,7 +409,7 @@ static cudaError_t enqueue_pass(ltl_ctx* c) {
             break;
         }
         case LTL_VARIANT_PACKED: {
-            e = launch_packed_step(cur_packed(c), nxt_packed(c), c->rule, c->stream);
+            e = launch_packed_step(cur_packed(c), nxt_packed(c), c->rule, c->packed_band_rows, c->stream);
             step_kernels = 1;
             if (c->timing && e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
             if (e == cudaSuccess) e = launch_packed_halo(nxt_packed(c), c->stream);
@@ -552,6 +555,30 @@ extern "C" int ltl_unpack_device(const uint64_t* dev_words, size_t word_pitch_by
     LTL_CUDA(launch_unpack(dev_words, word_pitch_bytes / 8, rows, cols, dev_cells, cell_pitch,
                            (cudaStream_t)stream));
     return LTL_OK;
+}
+
+extern "C" int ltl_set_param(ltl_ctx* c, const char* name, long long value) {
+    if (int r = check_ctx(c)) return r;
+    if (!name) {
+        ltl_set_error("ltl_set_param: name is NULL");
+        return LTL_EINVAL;
+    }
+    if (std::strcmp(name, "band_rows") == 0) {
+        if (value < 16 || value > 4096) {
+            ltl_set_error("ltl_set_param: band_rows must be in [16, 4096]");
+            return LTL_EINVAL;
+        }
+        if (c->variant == LTL_VARIANT_PLAIN) c->band_rows = (int)value;
+        else if (c->variant == LTL_VARIANT_PACKED) c->packed_band_rows = (int)value;
+        else {
+            ltl_set_error("ltl_set_param: band_rows applies to the plain and packed variants");
+            return LTL_EUNSUPPORTED;
+        }
+        drop_graphs(c);
+        return LTL_OK;
+    }
+    ltl_set_error("ltl_set_param: unknown parameter '%s'", name);
+    return LTL_EINVAL;
 }
 
 extern "C" int ltl_set_timing(ltl_ctx* c, int enable) {

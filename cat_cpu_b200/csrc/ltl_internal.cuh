@@ -92,19 +92,6 @@ __device__ __forceinline__ int wrap_mod(int v, int n) {
     return r < 0 ? r + n : r;
 }
 
-// Byte window starting at byte offset o of a little-endian word array w
-// (o >= 0 here; callers bias indices so that o is non-negative at compile time).
-template <int O>
-__device__ __forceinline__ uint32_t window_at(const uint32_t* w) {
-    constexpr int idx = O >> 2;
-    constexpr int sh = O & 3;
-    if constexpr (sh == 0) {
-        return w[idx];
-    } else {
-        return __byte_perm(w[idx], w[idx + 1], 0x3210 + 0x1111 * sh);
-    }
-}
-
 }  // namespace ltl
 
 // Host-side error reporting (ltl_abi.cu).

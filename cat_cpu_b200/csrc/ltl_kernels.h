@@ -51,7 +51,8 @@ struct PackedFrame {
     size_t wpitch;  // words per frame row
 };
 bool packed_supported(int n, int radius);
-cudaError_t launch_packed_step(const PackedFrame& cur, const PackedFrame& nxt, const Rule& rule,
+// band_rows <= 0: built-in heuristic; > 0: rows per work item (tuning table / ltl_set_param)
+cudaError_t launch_packed_step(const PackedFrame& cur, const PackedFrame& nxt, const Rule& rule, int band_rows,
                                cudaStream_t s);
 cudaError_t launch_packed_halo(const PackedFrame& f, cudaStream_t s);
 cudaError_t launch_pack_frame(const Frame& src, const PackedFrame& dst, cudaStream_t s);
@@ -73,5 +74,12 @@ int tensor_plan_halo_needed(int radius);
 // Advance one pass (tensor_plan_depth generations) from frame `src_is_a ? a : b`.
 cudaError_t launch_tensor_pass(TensorPlan* p, bool src_is_a, cudaStream_t s);
 unsigned int* tensor_plan_error_flag(TensorPlan* p);
+
+// Tuning table (written by cat_cpu_b200/autotune.py): the value of `param` for
+// (variant name, radius, n), or `fallback` when no line matches.  Lines look like
+//   variant=plain radius=5 nmin=8192 nmax=65536 band_rows=128
+// radius=* matches every radius.  The file is $LTL_TUNING_FILE, else
+// tuning/ltl_tuning.txt next to libltl_b200.so.
+long long tuning_lookup(const char* variant, int radius, long long n, const char* param, long long fallback);
 
 }  // namespace ltl

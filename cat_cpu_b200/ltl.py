@@ -32,7 +32,7 @@ ABI_SYMBOLS = [
     "ltl_compare_device", "ltl_benchmark_seed", "ltl_generate_state", "ltl_pack_device", "ltl_unpack_device",
     "ltl_batch_create", "ltl_batch_destroy", "ltl_batch_set_stream", "ltl_batch_upload", "ltl_batch_download",
     "ltl_batch_upload_all", "ltl_batch_download_all", "ltl_batch_step", "ltl_batch_synchronize",
-    "ltl_batch_info", "ltl_set_timing", "ltl_get_timing", "ltl_last_error", "ltl_version",
+    "ltl_batch_info", "ltl_batch_set_param", "ltl_set_param", "ltl_set_timing", "ltl_get_timing", "ltl_last_error", "ltl_version",
 ]
 
 
@@ -94,6 +94,8 @@ def lib():
     L.ltl_batch_synchronize.argtypes = [vp]
     L.ltl_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                                  ctypes.POINTER(ctypes.c_int)]
+    L.ltl_set_param.argtypes = [vp, ctypes.c_char_p, ctypes.c_longlong]
+    L.ltl_batch_set_param.argtypes = [vp, ctypes.c_char_p, ctypes.c_longlong]
     L.ltl_set_timing.argtypes = [vp, i]
     L.ltl_get_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                                  ctypes.POINTER(ctypes.c_longlong)]
@@ -199,6 +201,9 @@ class CUDASolver:
         for row in g:
             print(" ".join("-" if v == 0 else str(int(v)) for v in row))
 
+    def set_param(self, name, value):
+        check(lib().ltl_set_param(self._h, name.encode(), int(value)))
+
     def set_timing(self, enable):
         check(lib().ltl_set_timing(self._h, int(bool(enable))))
 
@@ -302,6 +307,9 @@ class Batch:
 
     def step(self, steps):
         check(lib().ltl_batch_step(self._h, int(steps)))
+
+    def set_param(self, name, value):
+        check(lib().ltl_batch_set_param(self._h, name.encode(), int(value)))
 
     def synchronize(self):
         check(lib().ltl_batch_synchronize(self._h))

@@ -152,9 +152,20 @@ int ltl_batch_download(ltl_batch* b, int grid, uint8_t* inner, size_t pitch);
 int ltl_batch_upload_all(ltl_batch* b, const uint8_t* cells);
 int ltl_batch_download_all(ltl_batch* b, uint8_t* cells);
 int ltl_batch_step(ltl_batch* b, int steps);
+/* Batch shape parameters (autotuned; also read from the tuning table):
+ *   "stream_band_rows"    rows per work item of the streamed per-step kernels
+ *   "resident_max_bytes"  shared-memory budget deciding which grids stay resident
+ * Setting one rebuilds the work lists before the next step. */
+int ltl_batch_set_param(ltl_batch* b, const char* name, long long value);
 int ltl_batch_synchronize(ltl_batch* b);
 /* Total cells of the batch (sum of n^2) and its device bytes. */
 int ltl_batch_info(const ltl_batch* b, long long* cells, long long* device_bytes, int* temporal_depth);
+
+/* Shape parameters (what cat_cpu_b200/autotune.py sweeps; the autotuned table
+ * tuning/ltl_tuning.txt next to the library sets them at ltl_create):
+ *   "band_rows"  rows per work item of the plain and packed step kernels.
+ * The analogue of the reference project's NREGIONS_H/V region counts. */
+int ltl_set_param(ltl_ctx* ctx, const char* name, long long value);
 
 /* Kernel timing for benchmarks (the reference times whole runs with a
  * host clock, CpuTimer.cpp:7-19 / CPUBenchmark.cpp:71-84).  While enabled,
