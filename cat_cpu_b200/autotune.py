@@ -39,6 +39,15 @@ def _time_steps(torch, solver, stream, steps, reps=3):
     return best
 
 
+def size_class(n):
+    """Grid-side class a tuned value applies to: [1, 8191], [8192, 24575], [24576, 2^30]."""
+    if n < 8192:
+        return 1, 8191
+    if n < 24576:
+        return 8192, 24575
+    return 24576, 1 << 30
+
+
 def tune_single(torch, C, variant, n, radius, rule, candidates, steps):
     vcode = {"plain": C.VARIANT_PLAIN, "packed": C.VARIANT_PACKED}[variant]
     g = C.generate_state(n, 12345, 0.5, 1)
@@ -112,7 +121,7 @@ def main():
             jobs.append(("packed", 32768, r, scaled_rule(r), packed_c))
     for variant, n, r, rule, cands in jobs:
         (br, ms), rows = tune_single(torch, C, variant, n, r, rule, cands, 20)
-        lo, hi = (8192, 1 << 30) if n >= 16384 else (1, 8191)
+        lo, hi = size_class(n)
         table.append(f"variant={variant} radius={r} nmin={lo} nmax={hi} band_rows={br}")
         land.append(f"{variant} n={n} R={r}: " + ", ".join(f"{c}:{t:.4f}" for c, t in rows) + f"  -> {br}")
         print(land[-1], flush=True)

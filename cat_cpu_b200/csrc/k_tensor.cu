@@ -204,7 +204,7 @@ __host__ __device__ inline SmemLayout smem_layout(int Tc, int K1c) {
     L.x_off = o;
     o += kXStages * kXBytes;                // 1024-aligned stages
     L.hs_off = o;
-    o += 128 * Tc;                          // H as u8, MN-major
+    o += 2 * 128 * Tc;                      // H as u8, MN-major, two buffers (tile parity)
     L.bh_off = o;
     o += kN1 * K1c;                         // B_h
     L.bv_off = o;
@@ -319,30 +319,13 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
     } else if (warp == 1) {
         // --------------------------- MMA issuer -----------------------------
         if (lane == 0) {
-            const uint32_t ba = smem_u32(bh), va = smem_u32(bv), ha = smem_u32(hs);
+            const uint32_t ba = smem_u32(bh), va = smem_u32(bv), ha0 = smem_u32(hs);
             const uint32_t id1 = idesc_u8(kN1, false);
             const uint32_t id2 = idesc_u8(Tc, true);
             bool ok = true;
-            // product 2 of tile j: C = B_v * H(j)
-            auto product2 = [&](int j) -> bool {
-                if (!mbar_wait(&bars[HS_FULL], (uint32_t)j & 1u, kWaitLimitNs)) return false;
-                if (j >= 1 && !mbar_wait(&bars[C_EMPTY], (uint32_t)(j - 1) & 1u, kWaitLimitNs)) return false;
-                tc_fence_after();
-#pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    const uint64_t ad = desc_noswz(va + s * 2 * 128 * 16, 128 * 16, 128);
-                    const uint64_t bd = desc_noswz(ha + s * 32 * 16, 128, 128 * 16);
-                    mma_i8(tmem + kCCol, ad, bd, id2, s > 0 ? 1u : 0u);
-                }
-                mma_commit(&bars[C_FULL]);
-                return true;
-            };
-            for (int j = 0; j < mine && ok; ++j) {
+            auto product1 = [&](int j) -> bool {
                 const int st = j % kXStages;
-                // product 2 of the previous tile; its wait on HS_FULL also frees H's TMEM columns
-                if (j >= 1) ok = product2(j - 1);
-                if (ok) ok = mbar_wait(&bars[X_FULL + st], (uint32_t)(j / kXStages) & 1u, kWaitLimitNs);
-                if (!ok) break;
+                if (!mbar_wait(&bars[X_FULL + st], (uint32_t)(j / kXStages) & 1u, kWaitLimitNs)) return false;
                 tc_fence_after();
                 const uint32_t xa = smem_u32(xs + st * kXBytes);
                 for (int n0 = 0; n0 < Tc; n0 += kN1) {
@@ -355,8 +338,30 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
                     }
                 }
                 mma_commit(&bars[H_FULL]);
+                return true;
+            };
+            // product 2 of tile j: C = B_v * H(j), H(j) in shared-memory buffer j % 2
+            auto product2 = [&](int j) -> bool {
+                if (j >= 1 && !mbar_wait(&bars[C_EMPTY], (uint32_t)(j - 1) & 1u, kWaitLimitNs)) return false;
+                tc_fence_after();
+                const uint32_t ha = ha0 + (j & 1) * 128 * Tc;
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const uint64_t ad = desc_noswz(va + s * 2 * 128 * 16, 128 * 16, 128);
+                    const uint64_t bd = desc_noswz(ha + s * 32 * 16, 128, 128 * 16);
+                    mma_i8(tmem + kCCol, ad, bd, id2, s > 0 ? 1u : 0u);
+                }
+                mma_commit(&bars[C_FULL]);
+                return true;
+            };
+            // Order per tile j: product 1 of tile j+1 as soon as H(j) has been read
+            // back, then product 2 of tile j once C(j-1) has been read.
+            ok = mine >= 1 ? product1(0) : true;
+            for (int j = 0; j < mine && ok; ++j) {
+                ok = mbar_wait(&bars[HS_FULL], (uint32_t)j & 1u, kWaitLimitNs);
+                if (ok && j + 1 < mine) ok = product1(j + 1);
+                if (ok) ok = product2(j);
             }
-            if (ok && mine >= 1) ok = product2(mine - 1);
             if (!ok) atomicOr(p.err, 2u);
         }
     } else {
@@ -367,35 +372,39 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
         const bool small = (2 * R + 1) * (2 * R + 1) <= 127;
         bool ok = true;
-        int t = blockIdx.x;
-        for (int j = 0; j < mine && ok; ++j, t += gridDim.x) {
-            // re-quantise H(j) to u8, MN-major B operand of product 2
-            if (!mbar_wait(&bars[H_FULL], (uint32_t)j & 1u, kWaitLimitNs)) {
-                ok = false;
-                break;
-            }
+        // re-quantise H(j) to u8 into shared-memory buffer j % 2 (MN-major B operand of product 2)
+        auto requant = [&](int j) -> bool {
+            if (!mbar_wait(&bars[H_FULL], (uint32_t)j & 1u, kWaitLimitNs)) return false;
             tc_fence_after();
-            {
-                const uint32_t trow = tmem + kHCol + lane_off;
-                for (int cb = 32 * grp; cb < Tc; cb += 32 * kEpiGroups) {
-                    uint32_t v[32];
-                    tmem_ld32(trow + cb, v);
+            uint8_t* hsb = hs + (j & 1) * 128 * Tc;
+            const uint32_t trow = tmem + kHCol + lane_off;
+            for (int cb = 32 * grp; cb < Tc; cb += 32 * kEpiGroups) {
+                uint32_t v[32];
+                tmem_ld32(trow + cb, v);
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        uint4 w;
-                        w.x = pack4(v[16 * h + 0], v[16 * h + 1], v[16 * h + 2], v[16 * h + 3]);
-                        w.y = pack4(v[16 * h + 4], v[16 * h + 5], v[16 * h + 6], v[16 * h + 7]);
-                        w.z = pack4(v[16 * h + 8], v[16 * h + 9], v[16 * h + 10], v[16 * h + 11]);
-                        w.w = pack4(v[16 * h + 12], v[16 * h + 13], v[16 * h + 14], v[16 * h + 15]);
-                        const int chunk = (cb >> 4) + h;
-                        *(uint4*)(hs + (chunk * 128 + row) * 16) = w;
-                    }
+                for (int h = 0; h < 2; ++h) {
+                    uint4 w;
+                    w.x = pack4(v[16 * h + 0], v[16 * h + 1], v[16 * h + 2], v[16 * h + 3]);
+                    w.y = pack4(v[16 * h + 4], v[16 * h + 5], v[16 * h + 6], v[16 * h + 7]);
+                    w.z = pack4(v[16 * h + 8], v[16 * h + 9], v[16 * h + 10], v[16 * h + 11]);
+                    w.w = pack4(v[16 * h + 12], v[16 * h + 13], v[16 * h + 14], v[16 * h + 15]);
+                    const int chunk = (cb >> 4) + h;
+                    *(uint4*)(hsb + (chunk * 128 + row) * 16) = w;
                 }
             }
             fence_proxy_async();
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&bars[HS_FULL]);
+            return true;
+        };
+        if (mine >= 1) ok = requant(0);
+        int t = blockIdx.x;
+        for (int j = 0; j < mine && ok; ++j, t += gridDim.x) {
+            if (j + 1 < mine && !requant(j + 1)) {
+                ok = false;
+                break;
+            }
             // rule + store C(j)
             if (!mbar_wait(&bars[C_FULL], (uint32_t)j & 1u, kWaitLimitNs)) {
                 ok = false;
