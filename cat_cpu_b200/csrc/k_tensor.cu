@@ -190,6 +190,8 @@ struct TensorParams {
     RuleSwar8 q;       // rule on the box count (used when (2R+1)^2 <= 127)
     int slo, shi, blo, bhi;  // rule on the box count, scalar form
     unsigned int* err;
+    unsigned long long wait_ns;  // limit of every mbarrier wait
+    int inject_missing_commit;   // test hook: product 1 of the first tile never signals
 };
 
 struct SmemLayout {
@@ -296,7 +298,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
                 const int st = it % kXStages;
                 const uint32_t ph = (uint32_t)(it / kXStages) & 1u;
-                if (it >= kXStages) ok = mbar_wait(&bars[X_EMPTY + st], ph ^ 1u, kWaitLimitNs);
+                if (it >= kXStages) ok = mbar_wait(&bars[X_EMPTY + st], ph ^ 1u, p.wait_ns);
                 if (!ok) {
                     atomicOr(p.err, 1u);
                     break;
@@ -312,7 +314,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             // never leave with a copy in flight into this CTA's shared memory
             const int issued = it;
             for (int j = (issued > kXStages ? issued - kXStages : 0); j < issued; ++j) {
-                if (!mbar_wait(&bars[X_FULL + j % kXStages], (uint32_t)(j / kXStages) & 1u, kWaitLimitNs))
+                if (!mbar_wait(&bars[X_FULL + j % kXStages], (uint32_t)(j / kXStages) & 1u, p.wait_ns))
                     atomicOr(p.err, 16u);
             }
         }
@@ -325,7 +327,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             bool ok = true;
             auto product1 = [&](int j) -> bool {
                 const int st = j % kXStages;
-                if (!mbar_wait(&bars[X_FULL + st], (uint32_t)(j / kXStages) & 1u, kWaitLimitNs)) return false;
+                if (!mbar_wait(&bars[X_FULL + st], (uint32_t)(j / kXStages) & 1u, p.wait_ns)) return false;
                 tc_fence_after();
                 const uint32_t xa = smem_u32(xs + st * kXBytes);
                 for (int n0 = 0; n0 < Tc; n0 += kN1) {
@@ -337,12 +339,12 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
                         mma_i8(tmem + kHCol + n0, ad, bd, id1, s > 0 ? 1u : 0u);
                     }
                 }
-                mma_commit(&bars[H_FULL]);
+                if (!(p.inject_missing_commit && j == 0)) mma_commit(&bars[H_FULL]);
                 return true;
             };
             // product 2 of tile j: C = B_v * H(j), H(j) in shared-memory buffer j % 2
             auto product2 = [&](int j) -> bool {
-                if (j >= 1 && !mbar_wait(&bars[C_EMPTY], (uint32_t)(j - 1) & 1u, kWaitLimitNs)) return false;
+                if (j >= 1 && !mbar_wait(&bars[C_EMPTY], (uint32_t)(j - 1) & 1u, p.wait_ns)) return false;
                 tc_fence_after();
                 const uint32_t ha = ha0 + (j & 1) * 128 * Tc;
 #pragma unroll
@@ -358,7 +360,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             // back, then product 2 of tile j once C(j-1) has been read.
             ok = mine >= 1 ? product1(0) : true;
             for (int j = 0; j < mine && ok; ++j) {
-                ok = mbar_wait(&bars[HS_FULL], (uint32_t)j & 1u, kWaitLimitNs);
+                ok = mbar_wait(&bars[HS_FULL], (uint32_t)j & 1u, p.wait_ns);
                 if (ok && j + 1 < mine) ok = product1(j + 1);
                 if (ok) ok = product2(j);
             }
@@ -374,7 +376,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
         bool ok = true;
         // re-quantise H(j) to u8 into shared-memory buffer j % 2 (MN-major B operand of product 2)
         auto requant = [&](int j) -> bool {
-            if (!mbar_wait(&bars[H_FULL], (uint32_t)j & 1u, kWaitLimitNs)) return false;
+            if (!mbar_wait(&bars[H_FULL], (uint32_t)j & 1u, p.wait_ns)) return false;
             tc_fence_after();
             uint8_t* hsb = hs + (j & 1) * 128 * Tc;
             const uint32_t trow = tmem + kHCol + lane_off;
@@ -406,7 +408,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
                 break;
             }
             // rule + store C(j)
-            if (!mbar_wait(&bars[C_FULL], (uint32_t)j & 1u, kWaitLimitNs)) {
+            if (!mbar_wait(&bars[C_FULL], (uint32_t)j & 1u, p.wait_ns)) {
                 ok = false;
                 break;
             }
@@ -580,7 +582,11 @@ TensorPlan* tensor_plan_create(const Frame& a, const Frame& b, const Rule& rule,
         return nullptr;
     }
     cudaMemset(P->err, 0, sizeof(unsigned int));
-    for (auto& q : P->prm) q.err = P->err;
+    for (auto& q : P->prm) {
+        q.err = P->err;
+        q.wait_ns = kWaitLimitNs;
+        q.inject_missing_commit = 0;
+    }
     P->smem_bytes = smem_layout(Tc, K1c).total + 1024;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -602,6 +608,13 @@ void tensor_plan_destroy(TensorPlan* p) {
 }
 
 int tensor_plan_depth(const TensorPlan*) { return 1; }
+
+void tensor_plan_set_wait(TensorPlan* p, unsigned long long ns, int inject_missing_commit) {
+    for (auto& q : p->prm) {
+        q.wait_ns = ns;
+        q.inject_missing_commit = inject_missing_commit;
+    }
+}
 int tensor_plan_operand_bits(const TensorPlan*) { return 8; }
 unsigned int* tensor_plan_error_flag(TensorPlan* p) { return p ? p->err : nullptr; }
 

@@ -61,6 +61,8 @@ struct ltl_ctx {
     bool packed_valid = false;  // packed frames hold the current state
     // tensor variant
     TensorPlan* tplan = nullptr;
+    unsigned long long wait_ns = 2000000000ull;
+    bool inject = false;
     // graphs of kGraphPasses passes, one per starting buffer
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     // optional per-kernel timing (ltl_set_timing): event pairs around the main
@@ -493,7 +495,12 @@ extern "C" int ltl_synchronize(ltl_ctx* c) {
         unsigned int flag = 0;
         LTL_CUDA(cudaMemcpy(&flag, tensor_plan_error_flag(c->tplan), sizeof(flag), cudaMemcpyDeviceToHost));
         if (flag) {
-            ltl_set_error("tensor kernel reported a bounded-wait timeout (flag 0x%x)", flag);
+            // clear it, so that the context stays usable after the caller re-uploads a state
+            const unsigned int zero = 0;
+            cudaMemcpy(tensor_plan_error_flag(c->tplan), &zero, sizeof(zero), cudaMemcpyHostToDevice);
+            ltl_set_error("tensor kernel reported a bounded-wait timeout (flag 0x%x); the grid state is "
+                          "unspecified until the next upload",
+                          flag);
             return LTL_ETIMEOUT;
         }
     }
@@ -574,6 +581,24 @@ extern "C" int ltl_set_param(ltl_ctx* c, const char* name, long long value) {
             ltl_set_error("ltl_set_param: band_rows applies to the plain and packed variants");
             return LTL_EUNSUPPORTED;
         }
+        drop_graphs(c);
+        return LTL_OK;
+    }
+    if (std::strcmp(name, "wait_limit_ns") == 0 || std::strcmp(name, "inject_missing_commit") == 0) {
+        if (c->variant != LTL_VARIANT_TENSOR) {
+            ltl_set_error("ltl_set_param: %s applies to the tensor variant", name);
+            return LTL_EUNSUPPORTED;
+        }
+        if (std::strcmp(name, "wait_limit_ns") == 0) {
+            if (value < 1000000 || value > 10000000000ll) {
+                ltl_set_error("ltl_set_param: wait_limit_ns must be in [1e6, 1e10]");
+                return LTL_EINVAL;
+            }
+            c->wait_ns = (unsigned long long)value;
+        } else {
+            c->inject = value != 0;
+        }
+        tensor_plan_set_wait(c->tplan, c->wait_ns, c->inject ? 1 : 0);
         drop_graphs(c);
         return LTL_OK;
     }

@@ -74,6 +74,10 @@ int tensor_plan_halo_needed(int radius);
 // Advance one pass (tensor_plan_depth generations) from frame `src_is_a ? a : b`.
 cudaError_t launch_tensor_pass(TensorPlan* p, bool src_is_a, cudaStream_t s);
 unsigned int* tensor_plan_error_flag(TensorPlan* p);
+// Limit of the kernel's bounded waits, and a test hook that withholds one
+// completion signal so that the waits run out (no fault, no hang: the kernel
+// returns after the limit with an error bit set).
+void tensor_plan_set_wait(TensorPlan* p, unsigned long long ns, int inject_missing_commit);
 
 // Tuning table (written by cat_cpu_b200/autotune.py): the value of `param` for
 // (variant name, radius, n), or `fallback` when no line matches.  Lines look like

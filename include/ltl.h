@@ -164,7 +164,13 @@ int ltl_batch_info(const ltl_batch* b, long long* cells, long long* device_bytes
 /* Shape parameters (what cat_cpu_b200/autotune.py sweeps; the autotuned table
  * tuning/ltl_tuning.txt next to the library sets them at ltl_create):
  *   "band_rows"  rows per work item of the plain and packed step kernels.
- * The analogue of the reference project's NREGIONS_H/V region counts. */
+ * The analogue of the reference project's NREGIONS_H/V region counts.
+ * Failure-path controls of the tensor variant (its kernel waits on mbarriers,
+ * every wait bounded):
+ *   "wait_limit_ns"          limit of each wait (default 2e9);
+ *   "inject_missing_commit"  1 = withhold one completion signal, so the next
+ *                            pass's waits run out and ltl_synchronize returns
+ *                            LTL_ETIMEOUT (used by the failure-detection test). */
 int ltl_set_param(ltl_ctx* ctx, const char* name, long long value);
 
 /* Kernel timing for benchmarks (the reference times whole runs with a

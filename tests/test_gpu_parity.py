@@ -209,3 +209,27 @@ def test_errors_on_device():
     with pytest.raises(C.LtlError) as e:
         C.CUDASolver(64, 5, O.BOSCO_R5, device=99)
     assert e.value.code == C.ltl.ECUDA
+
+
+def test_tensor_bounded_wait_reports_timeout_and_recovers():
+    """Failure detection without a fault: a withheld completion signal makes the
+    tensor kernel's bounded waits run out; the host sees LTL_ETIMEOUT, and the
+    same context computes correctly after a fresh upload."""
+    n, r = 300, 5
+    g = C.start_grid(n, 8, 0.5, 1)
+    s = make("tensor", n, r, O.BOSCO_R5)
+    try:
+        s.set_param("wait_limit_ns", 20_000_000)
+        s.set_param("inject_missing_commit", 1)
+        s.setState(g)
+        s.doStep()
+        with pytest.raises(C.LtlError) as e:
+            s.synchronize()
+        assert e.value.code == C.ltl.ETIMEOUT
+        s.set_param("inject_missing_commit", 0)
+        s.setState(g)
+        s.doSteps(3)
+        s.synchronize()
+        assert np.array_equal(s.getCurrentState(), O.run(g, r, O.BOSCO_R5, 3))
+    finally:
+        s.close()
