@@ -32,7 +32,7 @@ ABI_SYMBOLS = [
     "ltl_compare_device", "ltl_benchmark_seed", "ltl_generate_state", "ltl_pack_device", "ltl_unpack_device",
     "ltl_batch_create", "ltl_batch_destroy", "ltl_batch_set_stream", "ltl_batch_upload", "ltl_batch_download",
     "ltl_batch_upload_all", "ltl_batch_download_all", "ltl_batch_step", "ltl_batch_synchronize",
-    "ltl_batch_info", "ltl_batch_set_param", "ltl_set_param", "ltl_set_timing", "ltl_get_timing", "ltl_last_error", "ltl_version",
+    "ltl_batch_info", "ltl_batch_set_param", "ltl_set_param", "ltl_set_timing", "ltl_get_timing", "ltl_step_noalloc", "ltl_last_error", "ltl_version",
 ]
 
 
@@ -99,6 +99,7 @@ def lib():
     L.ltl_set_timing.argtypes = [vp, i]
     L.ltl_get_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                                  ctypes.POINTER(ctypes.c_longlong)]
+    L.ltl_step_noalloc.argtypes = [vp, sz, vp, sz, i, i, i, i, i, i, i, vp]
     L.ltl_last_error.restype = ctypes.c_char_p
     L.ltl_version.restype = ctypes.c_char_p
     _lib = L

@@ -184,6 +184,27 @@ int ltl_set_timing(ltl_ctx* ctx, int enable);
 int ltl_get_timing(ltl_ctx* ctx, double* step_kernel_ms, long long* step_kernel_launches,
                    long long* all_launches);
 
+/* One plain CUDA-core run for callers that cannot allocate device memory
+ * (a host framework that owns all device memory through its own pool, a
+ * real-time service that forbids allocation after start-up, a plug-in that is
+ * handed buffers and a stream and nothing else).  No counterpart in the
+ * reference: it is an addition of this library.
+ *
+ * Advances the n x n grid `dev_in` (device memory, rows `in_pitch` bytes
+ * apart, cells 0/1) by `steps` generations and writes it to `dev_out` (may be
+ * the same buffer), stream-ordered on `stream` (NULL: the default stream) of
+ * the current device.  It calls no cudaMalloc/cudaFree: the two halo'd grids it
+ * needs live in a fixed 32 MiB array in device memory that every GPU loading
+ * the library holds until the process exits.  Grids needing more return
+ * LTL_EINVAL with a message (R <= 5: n up to 4000; larger R: smaller n).
+ * The first call on a device looks up that array's address and sets the
+ * kernels' shared-memory limits; make that first call before any stream
+ * capture.  All calls share the one array and it keeps the last call's data:
+ * calls that can overlap on the GPU (different streams, or different threads
+ * without ordering) race and corrupt each other's results. */
+int ltl_step_noalloc(const uint8_t* dev_in, size_t in_pitch, uint8_t* dev_out, size_t out_pitch, int n, int radius,
+                     int smin, int smax, int bmin, int bmax, int steps, void* stream);
+
 /* Message for the calling thread's last failed call ("" if none). */
 const char* ltl_last_error(void);
 
