@@ -10,6 +10,8 @@ scripts/extractBestRegionSize.py): here the swept shapes are
   plain / packed   band_rows: rows a warp walks down per work item (the vertical
                    window is restarted once per band, so longer bands re-read less
                    but leave fewer items to balance over 148 SMs);
+  plain            depth: generations per pass of the temporally blocked kernel
+                   (1, 2 or 3), swept jointly with band_rows;
   batch            stream_band_rows of the streamed per-step kernels, and
                    resident_max_bytes: which grids are kept in shared memory for
                    a whole multi-step launch and which are streamed each step.
@@ -48,7 +50,8 @@ def size_class(n):
     return 24576, 1 << 30
 
 
-def tune_single(torch, C, variant, n, radius, rule, candidates, steps):
+def tune_single(torch, C, variant, n, radius, rule, candidates, steps, depths=(1,)):
+    """Times every (depth, band_rows) pair; `steps` should be a multiple of every depth."""
     vcode = {"plain": C.VARIANT_PLAIN, "packed": C.VARIANT_PACKED}[variant]
     g = C.generate_state(n, 12345, 0.5, 1)
     stream = torch.cuda.Stream()
@@ -56,12 +59,15 @@ def tune_single(torch, C, variant, n, radius, rule, candidates, steps):
     s.set_stream(stream.cuda_stream)
     rows = []
     try:
-        for br in candidates:
-            s.set_param("band_rows", br)
-            s.setState(g)
-            s.doSteps(16)
-            ms = _time_steps(torch, s, stream, steps)
-            rows.append((br, ms))
+        for d in depths:
+            if variant == "plain":
+                s.set_param("depth", d)
+            for br in candidates:
+                s.set_param("band_rows", br)
+                s.setState(g)
+                s.doSteps(12)
+                ms = _time_steps(torch, s, stream, steps)
+                rows.append(((d, br), ms))
     finally:
         s.close()
     best = min(rows, key=lambda x: x[1])
@@ -120,10 +126,13 @@ def main():
         if not args.quick or r in (1, 8):
             jobs.append(("packed", 32768, r, scaled_rule(r), packed_c))
     for variant, n, r, rule, cands in jobs:
-        (br, ms), rows = tune_single(torch, C, variant, n, r, rule, cands, 20)
+        depths = [d for d in (1, 2, 3) if d == 1 or (r <= 5 and d * r <= 16)] if variant == "plain" else [1]
+        ((d, br), ms), rows = tune_single(torch, C, variant, n, r, rule, cands, 24, depths)
         lo, hi = size_class(n)
-        table.append(f"variant={variant} radius={r} nmin={lo} nmax={hi} band_rows={br}")
-        land.append(f"{variant} n={n} R={r}: " + ", ".join(f"{c}:{t:.4f}" for c, t in rows) + f"  -> {br}")
+        extra = f" depth={d}" if variant == "plain" else ""
+        table.append(f"variant={variant} radius={r} nmin={lo} nmax={hi} band_rows={br}{extra}")
+        land.append(f"{variant} n={n} R={r} (depth, band_rows): " + ", ".join(f"{c}:{t:.4f}" for c, t in rows) +
+                    f"  -> {(d, br)}")
         print(land[-1], flush=True)
     band_c = [32, 64, 128] if args.quick else [32, 48, 64, 96, 128]
     res_c = [0, 225280] if args.quick else [0, 65536, 131072, 225280]

@@ -45,47 +45,20 @@ template <int R>
 __global__ void __launch_bounds__(kBatchWarps * 32)
 k_batch_step(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, const BatchGrid* __restrict__ grids,
              const int4* __restrict__ items, int n_items, const __grid_constant__ PackedRule pr) {
-    constexpr int PH = bits_for(2 * R + 1);
-    constexpr int PB = bits_for((2 * R + 1) * (2 * R + 1));
+    using Ring = PackedRing<R, kBatchWarps>;
+    extern __shared__ uint32_t ring_all[];
     const int lane = threadIdx.x & 31;
-    const int gwarp = blockIdx.x * kBatchWarps + (threadIdx.x >> 5);
+    const int wid = threadIdx.x >> 5;
+    uint32_t* ring_lane = ring_all + (size_t)wid * Ring::WARP_WORDS + lane;
+    const int gwarp = blockIdx.x * kBatchWarps + wid;
     const int gwarps = gridDim.x * kBatchWarps;
     for (int it = gwarp; it < n_items; it += gwarps) {
         const int4 item = items[it];  // grid, r0, r1, word strip
         const BatchGrid g = grids[item.x];
-        const uint32_t* base = cur + g.off;
-        uint32_t* obase = nxt + g.off;
-        const int r0 = item.y, r1 = item.z;
         const int w = item.w * 32 + lane;
-        const bool active = w <= g.nw;
-        const bool outputs = w < g.nw;
-        const int fw = 1 + w;
-        auto rowp = [&](int r) { return base + (size_t)(g.HR + r) * g.wp; };
-        uint32_t B[PB];
-#pragma unroll
-        for (int i = 0; i < PB; ++i) B[i] = 0u;
-#pragma unroll 1
-        for (int dy = -R; dy <= R; ++dy) {
-            uint32_t h[PH];
-            hcount<R, PH>(rowp(r0 + dy), fw, active, lane, h);
-            planes_add<PB, PH>(B, h);
-        }
-#pragma unroll 1
-        for (int r = r0; r < r1; ++r) {
-            if (outputs) {
-                const uint32_t s = __ldg(rowp(r) + fw);
-                const uint32_t in1 = planes_in<PB>(B, pr.lo[1], pr.hi[1]) & pr.keep[1];
-                const uint32_t in0 = planes_in<PB>(B, pr.lo[0], pr.hi[0]) & pr.keep[0];
-                obase[(size_t)(g.HR + r) * g.wp + fw] = (s & in1) | (~s & in0);
-            }
-            if (r + 1 < r1) {
-                uint32_t h[PH];
-                hcount<R, PH>(rowp(r - R), fw, active, lane, h);
-                planes_sub<PB, PH>(B, h);
-                hcount<R, PH>(rowp(r + R + 1), fw, active, lane, h);
-                planes_add<PB, PH>(B, h);
-            }
-        }
+        packed_band<R, Ring::fits>(cur + g.off, nxt + g.off, (size_t)g.wp, g.HR, item.y, item.z, 1 + w, w <= g.nw,
+                                   w < g.nw, lane, ring_lane, pr);
+        __syncwarp();
     }
 }
 
@@ -99,8 +72,8 @@ __device__ __forceinline__ uint32_t frame_bit(const uint32_t* row, int cell) {
     return (row[p >> 5] >> (p & 31)) & 1u;
 }
 
-__device__ __forceinline__ uint32_t halo_word(const uint32_t* row, int fw, int n, int nw) {
-    // frame word fw (0 = left halo, nw = last inner, nw + 1 = right halo)
+__device__ __forceinline__ uint32_t halo_word_bits(const uint32_t* row, int fw, int n, int nw) {
+    // frame word fw (0 = left halo, nw = last inner, nw + 1 = right halo), bit by bit
     if (fw == nw) {
         const int inner_bits = n - 32 * (nw - 1);
         uint32_t v = inner_bits >= 32 ? row[fw] : (row[fw] & ((1u << inner_bits) - 1u));
@@ -113,6 +86,10 @@ __device__ __forceinline__ uint32_t halo_word(const uint32_t* row, int fw, int n
         v |= frame_bit(row, ((cell % n) + n) % n) << b;
     }
     return v;
+}
+
+__device__ __forceinline__ uint32_t halo_word(const uint32_t* row, int fw, int n, int nw) {
+    return packed_halo_word(row, fw, n, nw, [&] { return halo_word_bits(row, fw, n, nw); });
 }
 
 __global__ void k_batch_halo_cols(uint32_t* __restrict__ arena, const BatchGrid* __restrict__ grids,
@@ -273,12 +250,23 @@ static size_t res_smem_bytes(int n) {
 template <int R>
 static cudaError_t launch_batch_step_r(const uint32_t* cur, uint32_t* nxt, const BatchGrid* grids, const int4* items,
                                        int n_items, const PackedRule& pr, int sms, cudaStream_t s) {
+    using Ring = PackedRing<R, kBatchWarps>;
+    const int smem = Ring::fits ? Ring::BYTES : 0;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<R>, kBatchWarps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<R>, kBatchWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
     const int ctas = std::max(1, std::min((n_items + kBatchWarps - 1) / kBatchWarps, sms * per_sm));
-    k_batch_step<R><<<ctas, kBatchWarps * 32, 0, s>>>(cur, nxt, grids, items, n_items, pr);
+    k_batch_step<R><<<ctas, kBatchWarps * 32, smem, s>>>(cur, nxt, grids, items, n_items, pr);
     return cudaGetLastError();
+}
+
+// Shared-memory limit of the streamed step kernel (its h ring), set once per
+// radius outside any stream capture.
+template <int R>
+static cudaError_t prepare_batch_step_r() {
+    using Ring = PackedRing<R, kBatchWarps>;
+    if (!Ring::fits || Ring::BYTES <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(k_batch_step<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, Ring::BYTES);
 }
 
 template <int R>
@@ -318,6 +306,16 @@ static cudaError_t batch_resident_dispatch(int R, const uint32_t* src, uint32_t*
 template <int R>
 static cudaError_t prepare_resident_r(size_t smem) {
     return cudaFuncSetAttribute(k_batch_resident<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+static cudaError_t batch_step_prepare_dispatch(int R) {
+    switch (R) {
+#define LTL_BSP(r) \
+    case r: return prepare_batch_step_r<r>();
+        LTL_BATCH_RADII(LTL_BSP)
+#undef LTL_BSP
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 static cudaError_t batch_prepare_dispatch(int R, size_t smem) {
@@ -449,6 +447,8 @@ static int batch_plan(ltl_batch* b) {
     for (auto& c : b->classes)
         if (!c.resident.empty()) smem_by_radius[c.rule.radius] = std::max(smem_by_radius[c.rule.radius], c.res_smem);
     for (auto& kv : smem_by_radius) BATCH_CUDA(batch_prepare_dispatch(kv.first, kv.second));
+    for (auto& c : b->classes)
+        if (!c.streamed.empty()) BATCH_CUDA(batch_step_prepare_dispatch(c.rule.radius));
     for (auto& c : b->classes) {
         if (!c.resident.empty()) {
             BATCH_CUDA(cudaMalloc(&c.d_resident, sizeof(int) * c.resident.size()));

@@ -30,28 +30,15 @@ static int packed_band_rows(int n, int n_wstrips, int sms) {
     return (rows + 15) / 16 * 16;
 }
 
-// Shared-memory ring of the last 2R+2 row counts h (PH planes per lane), so each
-// row's horizontal count is computed once on entry and read back on exit.
-template <int R>
-struct PackedRing {
-    static constexpr int PH = bits_for(2 * R + 1);
-    static constexpr int ROWS = 2 * R + 2;
-    static constexpr int BYTES = ROWS * PH * 32 * 4 * kPackedWarps;
-    static constexpr bool fits = BYTES <= 96 * 1024;
-};
-
 template <int R>
 __global__ void __launch_bounds__(kPackedWarps * 32)
 k_packed_step(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int n, int nw, int HR, int HW,
               size_t wp, int n_wstrips, int n_items, int band_rows, const __grid_constant__ PackedRule pr) {
-    constexpr int PH = bits_for(2 * R + 1);
-    constexpr int PB = bits_for((2 * R + 1) * (2 * R + 1));
-    constexpr bool kRing = PackedRing<R>::fits;
-    constexpr int RING = 2 * R + 2;
+    using Ring = PackedRing<R, kPackedWarps>;
     extern __shared__ uint32_t ring_all[];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
-    uint32_t* ring = ring_all + (size_t)wid * RING * PH * 32;
+    uint32_t* ring_lane = ring_all + (size_t)wid * Ring::WARP_WORDS + lane;
     const int gwarp = blockIdx.x * kPackedWarps + wid;
     const int gwarps = gridDim.x * kPackedWarps;
 
@@ -63,51 +50,7 @@ k_packed_step(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int 
         const int w = ws * 32 + lane;     // inner word
         const bool active = w <= nw;      // w == nw is the right halo word (neighbour of the last word)
         const bool outputs = w < nw;
-        const int fw = HW + w;
-        auto rowp = [&](int r) { return cur + (size_t)(HR + r) * wp; };
-        auto slot = [&](int r) { return ring + (((r % RING) + RING) % RING) * PH * 32 + lane; };
-
-        uint32_t B[PB];
-#pragma unroll
-        for (int i = 0; i < PB; ++i) B[i] = 0u;
-#pragma unroll 1
-        for (int dy = -R; dy <= R; ++dy) {
-            uint32_t h[PH];
-            hcount<R, PH>(rowp(r0 + dy), fw, active, lane, h);
-            planes_add<PB, PH>(B, h);
-            if constexpr (kRing) {
-                uint32_t* sl = slot(r0 + dy);
-#pragma unroll
-                for (int i = 0; i < PH; ++i) sl[32 * i] = h[i];
-            }
-        }
-#pragma unroll 1
-        for (int r = r0; r < r1; ++r) {
-            if (outputs) {
-                const uint32_t s = __ldg(rowp(r) + fw);
-                const uint32_t in1 = planes_in<PB>(B, pr.lo[1], pr.hi[1]) & pr.keep[1];
-                const uint32_t in0 = planes_in<PB>(B, pr.lo[0], pr.hi[0]) & pr.keep[0];
-                nxt[(size_t)(HR + r) * wp + fw] = (s & in1) | (~s & in0);
-            }
-            if (r + 1 < r1) {
-                uint32_t h[PH];
-                if constexpr (kRing) {
-                    const uint32_t* sl = slot(r - R);
-#pragma unroll
-                    for (int i = 0; i < PH; ++i) h[i] = sl[32 * i];
-                } else {
-                    hcount<R, PH>(rowp(r - R), fw, active, lane, h);
-                }
-                planes_sub<PB, PH>(B, h);
-                hcount<R, PH>(rowp(r + R + 1), fw, active, lane, h);
-                planes_add<PB, PH>(B, h);
-                if constexpr (kRing) {
-                    uint32_t* sl = slot(r + R + 1);
-#pragma unroll
-                    for (int i = 0; i < PH; ++i) sl[32 * i] = h[i];
-                }
-            }
-        }
+        packed_band<R, Ring::fits>(cur, nxt, wp, HR, r0, r1, HW + w, active, outputs, lane, ring_lane, pr);
         __syncwarp();
     }
 }
@@ -124,7 +67,7 @@ static cudaError_t launch_packed_r(const PackedFrame& c, const PackedFrame& x, c
     const int band_rows = band_override > 0 ? band_override : packed_band_rows(c.n, n_wstrips, sms);
     const int bands = (c.n + band_rows - 1) / band_rows;
     const int items = n_wstrips * bands;
-    const int smem = PackedRing<R>::fits ? PackedRing<R>::BYTES : 0;
+    const int smem = PackedRing<R, kPackedWarps>::fits ? PackedRing<R, kPackedWarps>::BYTES : 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_packed_step<R>, kPackedWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
     int ctas = std::min((items + kPackedWarps - 1) / kPackedWarps, sms * per_sm);
@@ -135,7 +78,7 @@ static cudaError_t launch_packed_r(const PackedFrame& c, const PackedFrame& x, c
 
 template <int R>
 static cudaError_t prepare_packed_r() {
-    const int smem = PackedRing<R>::fits ? PackedRing<R>::BYTES : 0;
+    const int smem = PackedRing<R, kPackedWarps>::fits ? PackedRing<R, kPackedWarps>::BYTES : 0;
     if (smem <= 48 * 1024) return cudaSuccess;
     return cudaFuncSetAttribute(k_packed_step<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
@@ -188,22 +131,26 @@ __global__ void k_packed_halo_cols(uint32_t* __restrict__ g, int n, int nw, int 
         const int k = (int)(t % per_row);
         const int fw = k < HW ? k : HW + nw - 1 + (k - HW);
         uint32_t* row = g + (size_t)(HR + i) * wp;
-        uint32_t v = 0u;
-        if (fw == HW + nw - 1) {
-            // last inner word: keep its inner bits, rewrite the bits past n
-            const int inner_bits = n - 32 * (nw - 1);
-            v = inner_bits >= 32 ? row[fw] : (row[fw] & ((1u << inner_bits) - 1u));
-            for (int b = inner_bits; b < 32; ++b) {
-                int cell = 32 * (nw - 1) + b;
-                v |= packed_bit(row, HW, cell % n) << b;
+        auto slow = [&]() -> uint32_t {
+            uint32_t v = 0u;
+            if (fw == HW + nw - 1) {
+                // last inner word: keep its inner bits, rewrite the bits past n
+                const int inner_bits = n - 32 * (nw - 1);
+                v = inner_bits >= 32 ? row[fw] : (row[fw] & ((1u << inner_bits) - 1u));
+                for (int b = inner_bits; b < 32; ++b) {
+                    int cell = 32 * (nw - 1) + b;
+                    v |= packed_bit(row, HW, cell % n) << b;
+                }
+            } else {
+                for (int b = 0; b < 32; ++b) {
+                    int cell = 32 * (fw - HW) + b;
+                    int src = ((cell % n) + n) % n;
+                    v |= packed_bit(row, HW, src) << b;
+                }
             }
-        } else {
-            for (int b = 0; b < 32; ++b) {
-                int cell = 32 * (fw - HW) + b;
-                int src = ((cell % n) + n) % n;
-                v |= packed_bit(row, HW, src) << b;
-            }
-        }
+            return v;
+        };
+        const uint32_t v = HW == 1 ? packed_halo_word(row, fw, n, nw, slow) : slow();
         // the halo words only read inner bits (< n), never bits written here
         row[fw] = v;
     }

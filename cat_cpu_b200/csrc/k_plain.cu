@@ -301,6 +301,231 @@ cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& r
 }
 
 // ---------------------------------------------------------------------------
+// K1 temporally blocked (R <= 5, D = 2 or 3 generations per pass, D*R <= 16).
+//
+// The same SWAR row step as k_plain_swar8, stacked D times inside one warp so
+// that a pass reads the grid once and writes it once for D generations.  Stage
+// 1 slides its vertical window over the input rows (shared-memory ring 0, fed
+// by cp.async); stage k > 1 slides over the rows stage k-1 has just produced
+// (ring k-1), one row behind per R rows of lag.  All 32 lanes run the inner
+// stages: lane 0's bytes [kR, 16) and lane 31's bytes [0, 16 - kR) of stage k
+// are exact (the rest read past the strip), and D*R <= 16 keeps every byte
+// lanes 1..30 of stage D read inside that exact part.  Rows: stage k
+// produces rows [r0 - (D-k)R, r1 - 1 + (D-k)R] of the band, so the inputs are
+// rows [r0 - DR, r1 - 1 + DR], inside the frame's halo (H >= D*R).  Stage
+// values in halo rows and columns are exact torus values because the halo is
+// an exact copy to depth H.
+// ---------------------------------------------------------------------------
+constexpr int kTbRing = 16;  // rows of the input ring (power of two >= 2R + 2 + ahead)
+
+template <int R>
+constexpr int tb_ahead() {
+    return (kTbRing - (2 * R + 2)) < 8 ? (kTbRing - (2 * R + 2)) : 8;
+}
+
+// The input ring has kTbRing rows; each inner stage's ring has 2R + 2 (the
+// rows its successor's window spans plus the one leaving it).
+template <int R, int D>
+constexpr int tb_ring_rows() {
+    return kTbRing + (D - 1) * (2 * R + 2);
+}
+
+template <int R, int D>
+constexpr int tb_smem_bytes() {
+    return kPlainWarps * tb_ring_rows<R, D>() * 32 * (int)sizeof(uint4);
+}
+
+// One SWAR row of the interval rule for all lanes: V = the lane's vertical
+// window sums, c = the lane's centre cells.  Every lane of the warp must call it.
+template <int R>
+__device__ __forceinline__ uint4 swar8_row(const uint32_t (&V)[4], uint4 c, const RuleSwar8& q) {
+    uint32_t w[8];
+    w[0] = __shfl_up_sync(0xffffffffu, V[2], 1);
+    w[1] = __shfl_up_sync(0xffffffffu, V[3], 1);
+    w[2] = V[0]; w[3] = V[1]; w[4] = V[2]; w[5] = V[3];
+    w[6] = __shfl_down_sync(0xffffffffu, V[0], 1);
+    w[7] = __shfl_down_sync(0xffffffffu, V[1], 1);
+    uint32_t box[4];
+    row_boxes<R>(w, box);
+    uint4 o;
+    o.x = rule_swar8(box[0], c.x, q);
+    o.y = rule_swar8(box[1], c.y, q);
+    o.z = rule_swar8(box[2], c.z, q);
+    o.w = rule_swar8(box[3], c.w, q);
+    return o;
+}
+
+template <int R, int D>
+__global__ void __launch_bounds__(kPlainWarps * 32)
+k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n, int H, size_t pitch,
+                 int band_rows, int n_strips, int n_items, RuleSwar8 q) {
+    constexpr int kAh = tb_ahead<R>();
+    constexpr int kRS = 2 * R + 2;  // rows per inner-stage ring
+    static_assert(D >= 2 && D * R <= 16 && kAh >= 1, "unsupported depth");
+    extern __shared__ uint4 ring_all[];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    uint4* ring0 = ring_all + (size_t)wid * tb_ring_rows<R, D>() * 32 + lane;  // input rows
+    auto slot0 = [&](int r) { return ring0 + (r & (kTbRing - 1)) * 32; };
+    // ring k >= 1 (rows of stage k), slot s in [0, kRS)
+    auto slotk = [&](int k, int sl) { return ring0 + (kTbRing + (k - 1) * kRS + sl) * 32; };
+    auto wrap = [](int v) { return v >= kRS ? v - kRS : v; };
+    const int gwarp = blockIdx.x * kPlainWarps + wid;
+    const int gwarps = gridDim.x * kPlainWarps;
+
+    for (int item = gwarp; item < n_items; item += gwarps) {
+        const int strip = item % n_strips;
+        const int band = item / n_strips;
+        const int r0 = band * band_rows;
+        const int r1 = min(r0 + band_rows, n);
+        const int x = strip * kStripOut - 16 + 16 * lane;
+        const bool loads = x < n + 16;  // (D*R <= 16: columns >= n + 16 feed no output)
+        const bool outputs = lane >= 1 && lane <= 30 && x < n;
+        const uint8_t* col = cur + (size_t)H + (loads ? x : 0);
+        const int rlast = r1 - 1 + D * R;          // last input row of the band
+        const int yfirst = r0 - (D - 1) * R;        // first and last stage-1 rows
+        const int ylast = r1 - 1 + (D - 1) * R;
+        auto issue = [&](int r) {
+            if (loads && r <= rlast) cp_async16(slot0(r), col + (size_t)(H + r) * pitch);
+            cp_async_commit();
+        };
+        for (int r = yfirst - R; r <= yfirst + R + kAh; ++r) issue(r);
+        cp_async_wait<kAh>();
+        uint32_t V[D][4];
+#pragma unroll
+        for (int k = 0; k < D; ++k) V[k][0] = V[k][1] = V[k][2] = V[k][3] = 0u;
+#pragma unroll 1
+        for (int dy = -R; dy <= R; ++dy) v_add(V[0], *slot0(yfirst + dy));
+        // sl[k] = ring-k slot of the row stage k produces in this iteration,
+        // y - (k-1)R, modulo kRS (rows may be negative: start from a non-negative
+        // representative)
+        int sl[D];
+#pragma unroll
+        for (int k = 1; k < D; ++k) sl[k] = ((yfirst - (k - 1) * R) % kRS + kRS) % kRS;
+
+#pragma unroll 1
+        for (int y = yfirst; y <= ylast; ++y) {
+            // stage 1: row y
+            uint4 prod = swar8_row<R>(V[0], *slot0(y), q);
+            *slotk(1, sl[1]) = prod;
+            // stages 2..D: stage k absorbs row yin = y - (k-2)R of stage k-1 and, once
+            // its window is full, produces row yin - R.  In ring k-1 the leaving row
+            // yin - 2R - 1 sits one slot after yin, and row yin - R sits R + 2 after.
+            bool live = true;
+#pragma unroll
+            for (int k = 2; k <= D; ++k) {
+                if (live) {
+                    const int yin = y - (k - 2) * R;
+                    const int absorbed = yin - (r0 - (D - k + 1) * R) + 1;  // rows of stage k-1 so far
+                    v_add(V[k - 1], prod);
+                    if (absorbed > 2 * R + 1) {
+                        const uint4 out = *slotk(k - 1, wrap(sl[k - 1] + 1));
+                        V[k - 1][0] -= out.x; V[k - 1][1] -= out.y; V[k - 1][2] -= out.z; V[k - 1][3] -= out.w;
+                    }
+                    if (absorbed >= 2 * R + 1) {
+                        const int yk = yin - R;
+                        const uint4 c = *slotk(k - 1, wrap(sl[k - 1] + R + 2));
+                        if (k < D) {
+                            prod = swar8_row<R>(V[k - 1], c, q);
+                            *slotk(k, sl[k]) = prod;
+                        } else {
+                            const uint4 o = swar8_row<R>(V[k - 1], c, q);
+                            if (outputs) {
+                                uint8_t* dst = nxt + (size_t)(H + yk) * pitch + H + x;
+                                if (x + 16 <= n) {
+                                    *(uint4*)dst = o;
+                                } else {
+                                    store_partial16(dst, o, n - x);
+                                }
+                            }
+                        }
+                    } else {
+                        live = false;
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 1; k < D; ++k) sl[k] = wrap(sl[k] + 1);
+            if (y < ylast) {
+                issue(y + R + 1 + kAh);
+                cp_async_wait<kAh>();  // input row y + R + 1 has landed
+                v_slide(V[0], *slot0(y + R + 1), *slot0(y - R));
+            }
+        }
+        cp_async_wait<0>();
+    }
+}
+
+bool plain_tb_supported(int radius, int depth) {
+    return plain_swar8_supported(radius) && (depth == 2 || depth == 3) && depth * radius <= 16;
+}
+
+template <int R, int D>
+static cudaError_t launch_tb_rd(const Frame& cur, const Frame& nxt, const RuleSwar8& q, int band_rows,
+                                cudaStream_t s) {
+    const int n = cur.n;
+    const int strips = (n + kStripOut - 1) / kStripOut;
+    const int bands = (n + band_rows - 1) / band_rows;
+    const int items = strips * bands;
+    constexpr int smem = tb_smem_bytes<R, D>();
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_plain_swar8_tb<R, D>, kPlainWarps * 32, smem);
+    if (per_sm < 1) per_sm = 1;
+    int ctas = std::min((items + kPlainWarps - 1) / kPlainWarps, sms * per_sm);
+    k_plain_swar8_tb<R, D><<<ctas, kPlainWarps * 32, smem, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch,
+                                                               band_rows, strips, items, q);
+    return cudaGetLastError();
+}
+
+template <int R, int D>
+static cudaError_t prepare_tb_rd() {
+    if constexpr (D * R <= 16) {
+        return cudaFuncSetAttribute(k_plain_swar8_tb<R, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    tb_smem_bytes<R, D>());
+    } else {
+        return cudaSuccess;
+    }
+}
+
+template <int R>
+static cudaError_t launch_tb_r(const Frame& cur, const Frame& nxt, const RuleSwar8& q, int band_rows, int depth,
+                               cudaStream_t s) {
+    if (depth == 2) return launch_tb_rd<R, 2>(cur, nxt, q, band_rows, s);
+    if constexpr (3 * R <= 16) {
+        if (depth == 3) return launch_tb_rd<R, 3>(cur, nxt, q, band_rows, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t plain_tb_prepare(int radius) {
+    cudaError_t e = cudaSuccess;
+    switch (radius) {
+#define LTL_TBP(r) \
+    case r: e = prepare_tb_rd<r, 2>(); if (e == cudaSuccess) e = prepare_tb_rd<r, 3>(); break;
+        LTL_TBP(1) LTL_TBP(2) LTL_TBP(3) LTL_TBP(4) LTL_TBP(5)
+#undef LTL_TBP
+        default: break;
+    }
+    return e;
+}
+
+cudaError_t launch_plain_tb(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows, int depth,
+                            cudaStream_t s) {
+    if (!plain_tb_supported(rule.radius, depth) || cur.H < depth * rule.radius) return cudaErrorInvalidValue;
+    RuleSwar8 q = make_rule_swar8(rule);
+    switch (rule.radius) {
+        case 1: return launch_tb_r<1>(cur, nxt, q, band_rows, depth, s);
+        case 2: return launch_tb_r<2>(cur, nxt, q, band_rows, depth, s);
+        case 3: return launch_tb_r<3>(cur, nxt, q, band_rows, depth, s);
+        case 4: return launch_tb_r<4>(cur, nxt, q, band_rows, depth, s);
+        case 5: return launch_tb_r<5>(cur, nxt, q, band_rows, depth, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // K1 generic path (any R >= 1), two passes:
 //  (a) k_vsum: V[r][c] = sum_{dy=-R..R} X[r+dy][c] for every frame column c,
 //      as uint16 (two cells per 32-bit register, SWAR), one thread per 4

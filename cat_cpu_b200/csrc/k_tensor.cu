@@ -65,12 +65,19 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
     return done != 0;
 }
 
-// Bounded wait for `phase` of `bar`: false after `limit_ns` of wall time.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint64_t limit_ns) {
+// Bounded wait for `phase` of `bar`: false after `limit_ns` of wall time.  The
+// clock is read once per 16 tries, so that a waiting warp spends few issue
+// slots per try; `sleep_ns` > 0 backs off between tries (for warps whose wait
+// is not on the critical path).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint64_t limit_ns, uint32_t sleep_ns = 0) {
     if (mbar_try(bar, phase)) return true;
     const uint64_t t0 = globaltimer();
     while (true) {
-        if (mbar_try(bar, phase)) return true;
+#pragma unroll 4
+        for (int i = 0; i < 16; ++i) {
+            if (mbar_try(bar, phase)) return true;
+            if (sleep_ns) __nanosleep(sleep_ns);
+        }
         if (globaltimer() - t0 > limit_ns) return false;
     }
 }
@@ -114,18 +121,58 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
-// 32 consecutive TMEM columns of this thread's lane (32-bit each).
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+// 16 consecutive TMEM columns of this thread's lane (32-bit each).  The
+// registers are defined only after tmem_wait16 on the same array: the wait
+// takes them as read-write operands so that the compiler cannot move a use of
+// them above it.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Waits for every tcgen05.ld this thread issued.
+__device__ __forceinline__ void tmem_wait16(uint32_t (&v)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+                   "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
+                   "+r"(v[15])
+                 :
+                 : "memory");
+}
+
+// Walks this warp's 16-column chunks of a TMEM accumulator row, loading chunk
+// c + 1 while f(values, column) processes chunk c.  The chunks are the halves
+// of 32-column blocks grp, grp + groups, grp + 2*groups, ... below `cols`;
+// `max_chunks` bounds the unrolled loop.  Every argument is warp-uniform, as
+// tcgen05.ld requires.
+template <int max_chunks, class F>
+__device__ __forceinline__ void tmem_walk16(uint32_t trow, int grp, int groups, int cols, F&& f) {
+    const int blocks = grp * 32 < cols ? (cols / 32 - grp + groups - 1) / groups : 0;
+    const int nc = 2 * blocks < max_chunks ? 2 * blocks : max_chunks;
+    auto col = [&](int c) { return 32 * (grp + groups * (c >> 1)) + 16 * (c & 1); };
+    if (nc == 0) return;
+    uint32_t a[16], b[16];
+    tmem_ld16(trow + col(0), a);
+    tmem_wait16(a);
+#pragma unroll
+    for (int c = 0; c < max_chunks; ++c) {
+        if (c < nc) {
+            const bool more = c + 1 < nc;
+            if ((c & 1) == 0) {
+                if (more) tmem_ld16(trow + col(c + 1), b);
+                f(a, col(c));
+                if (more) tmem_wait16(b);
+            } else {
+                if (more) tmem_ld16(trow + col(c + 1), a);
+                f(b, col(c));
+                if (more) tmem_wait16(a);
+            }
+        }
+    }
 }
 
 // Shared-memory matrix descriptors (tcgen05 "version 1" format).
@@ -175,6 +222,7 @@ constexpr int kHCol = 0;               // TMEM column of H
 constexpr int kCCol = 256;             // TMEM column of C
 constexpr int kN1 = 32;                // product-1 column chunk
 constexpr int kEpiGroups = 4;          // epilogue warp groups (column blocks round-robin)
+constexpr int kMaxChunks = 4;          // 16-column chunks per epilogue warp: 2 blocks of 32 (Tc <= 256)
 constexpr int kEpiWarps = 4 * kEpiGroups;
 constexpr int kThreads = 64 + 32 * kEpiWarps;  // producer + MMA + epilogue warps
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any legitimate wait
@@ -298,7 +346,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
                 const int st = it % kXStages;
                 const uint32_t ph = (uint32_t)(it / kXStages) & 1u;
-                if (it >= kXStages) ok = mbar_wait(&bars[X_EMPTY + st], ph ^ 1u, p.wait_ns);
+                if (it >= kXStages) ok = mbar_wait(&bars[X_EMPTY + st], ph ^ 1u, p.wait_ns, 128);
                 if (!ok) {
                     atomicOr(p.err, 1u);
                     break;
@@ -379,21 +427,15 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             if (!mbar_wait(&bars[H_FULL], (uint32_t)j & 1u, p.wait_ns)) return false;
             tc_fence_after();
             uint8_t* hsb = hs + (j & 1) * 128 * Tc;
-            const uint32_t trow = tmem + kHCol + lane_off;
-            for (int cb = 32 * grp; cb < Tc; cb += 32 * kEpiGroups) {
-                uint32_t v[32];
-                tmem_ld32(trow + cb, v);
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    uint4 w;
-                    w.x = pack4(v[16 * h + 0], v[16 * h + 1], v[16 * h + 2], v[16 * h + 3]);
-                    w.y = pack4(v[16 * h + 4], v[16 * h + 5], v[16 * h + 6], v[16 * h + 7]);
-                    w.z = pack4(v[16 * h + 8], v[16 * h + 9], v[16 * h + 10], v[16 * h + 11]);
-                    w.w = pack4(v[16 * h + 12], v[16 * h + 13], v[16 * h + 14], v[16 * h + 15]);
-                    const int chunk = (cb >> 4) + h;
-                    *(uint4*)(hsb + (chunk * 128 + row) * 16) = w;
-                }
-            }
+            tmem_walk16<kMaxChunks>(tmem + kHCol + lane_off, grp, kEpiGroups, Tc,
+                                    [&](const uint32_t (&v)[16], int col) {
+                                        uint4 w;
+                                        w.x = pack4(v[0], v[1], v[2], v[3]);
+                                        w.y = pack4(v[4], v[5], v[6], v[7]);
+                                        w.z = pack4(v[8], v[9], v[10], v[11]);
+                                        w.w = pack4(v[12], v[13], v[14], v[15]);
+                                        *(uint4*)(hsb + ((col >> 4) * 128 + row) * 16) = w;
+                                    });
             fence_proxy_async();
             tc_fence_before();
             __syncwarp();
@@ -421,46 +463,40 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             const int xr = row + R;
             const uint8_t* xrow = xs + st * kXBytes + (xr & 127) * 128;
             uint8_t* orow = p.out + (size_t)(p.H + gi) * (size_t)p.pitch + p.H + c0;
-            const uint32_t trow = tmem + kCCol + lane_off;
-            for (int cb = 32 * grp; cb < Tc; cb += 32 * kEpiGroups) {
-                uint32_t v[32];
-                tmem_ld32(trow + cb, v);
-                if (!row_ok) continue;
+            tmem_walk16<kMaxChunks>(tmem + kCCol + lane_off, grp, kEpiGroups, Tc, [&](const uint32_t (&v)[16], int col) {
+                if (!row_ok) return;
+                const int xc = PADC + col;  // X column of these 16 cells
+                const int atom = xc >> 7, ch = (xc & 127) >> 4;
+                const uint4 s4 = *(const uint4*)(xrow + atom * kAtomBytes + ((ch ^ (xr & 7)) << 4));
+                const uint32_t sw[4] = {s4.x, s4.y, s4.z, s4.w};  // compile-time indices only
+                uint32_t o[4];
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int xc = PADC + cb + 16 * h;  // X column of these 16 cells
-                    const int atom = xc >> 7, ch = (xc & 127) >> 4;
-                    const uint4 s4 = *(const uint4*)(xrow + atom * kAtomBytes + ((ch ^ (xr & 7)) << 4));
-                    const uint32_t sw[4] = {s4.x, s4.y, s4.z, s4.w};  // compile-time indices only
-                    uint32_t o[4];
+                for (int qq = 0; qq < 4; ++qq) {
+                    const uint32_t* b = &v[4 * qq];
+                    if (small) {
+                        o[qq] = rule_swar8(pack4(b[0], b[1], b[2], b[3]), sw[qq], p.q);
+                    } else {
+                        uint32_t r = 0;
 #pragma unroll
-                    for (int qq = 0; qq < 4; ++qq) {
-                        const uint32_t* b = &v[16 * h + 4 * qq];
-                        if (small) {
-                            o[qq] = rule_swar8(pack4(b[0], b[1], b[2], b[3]), sw[qq], p.q);
-                        } else {
-                            uint32_t r = 0;
-#pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                const int B = (int)b[e];
-                                const int sv = (sw[qq] >> (8 * e)) & 1;
-                                const int lo = sv ? p.slo : p.blo, hi = sv ? p.shi : p.bhi;
-                                r |= (uint32_t)((B >= lo) & (B <= hi)) << (8 * e);
-                            }
-                            o[qq] = r;
+                        for (int e = 0; e < 4; ++e) {
+                            const int B = (int)b[e];
+                            const int sv = (sw[qq] >> (8 * e)) & 1;
+                            const int lo = sv ? p.slo : p.blo, hi = sv ? p.shi : p.bhi;
+                            r |= (uint32_t)((B >= lo) & (B <= hi)) << (8 * e);
                         }
-                    }
-                    const int gj = c0 + cb + 16 * h;
-                    if (gj + 16 <= p.n) {
-                        *(uint4*)(orow + cb + 16 * h) = make_uint4(o[0], o[1], o[2], o[3]);
-                    } else if (gj < p.n) {
-                        const int cnt = p.n - gj;
-#pragma unroll
-                        for (int e = 0; e < 16; ++e)
-                            if (e < cnt) orow[cb + 16 * h + e] = (uint8_t)((o[e >> 2] >> (8 * (e & 3))) & 0xff);
+                        o[qq] = r;
                     }
                 }
-            }
+                const int gj = c0 + col;
+                if (gj + 16 <= p.n) {
+                    *(uint4*)(orow + col) = make_uint4(o[0], o[1], o[2], o[3]);
+                } else if (gj < p.n) {
+                    const int cnt = p.n - gj;
+#pragma unroll
+                    for (int e = 0; e < 16; ++e)
+                        if (e < cnt) orow[col + e] = (uint8_t)((o[e >> 2] >> (8 * (e & 3))) & 0xff);
+                }
+            });
             tc_fence_before();
             __syncwarp();
             if (lane == 0) {
@@ -537,7 +573,7 @@ TensorPlan* tensor_plan_create(const Frame& a, const Frame& b, const Rule& rule,
     const int Tc = ((kXCols - 2 * PADC) / kN1) * kN1;  // 224 for R <= 16, 192 for R <= 32
     const int Tr = 128 - 2 * R;
     const int K1c = (int)round_up((size_t)(kN1 + PADC + R), 32);
-    if (Tc < kN1 || Tr < 1 || K1c > kN1 + 2 * PADC) {
+    if (Tc < kN1 || Tc > 16 * kEpiGroups * kMaxChunks || Tr < 1 || K1c > kN1 + 2 * PADC) {
         snprintf(why, why_len, "no tile shape for R=%d", R);
         delete P;
         return nullptr;

@@ -203,10 +203,16 @@ extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin
             return LTL_ENOMEM;
         }
     }
-    if (variant == LTL_VARIANT_PLAIN)
+    if (variant == LTL_VARIANT_PLAIN && plain_swar8_supported(radius)) {
+        // generations per pass: the tuning table's value, else 2 where the
+        // temporally blocked kernel applies (grids below 256 gain nothing)
+        const int want = (int)tuning_lookup("plain", radius, n, "depth", n >= 256 ? 2 : 1);
+        if (want > 1 && plain_tb_supported(radius, want) && H >= want * radius) depth = want;
         c->band_rows = (int)tuning_lookup("plain", radius, n, "band_rows", plain_swar8_band_rows(n, device));
+    }
     if (variant == LTL_VARIANT_PACKED) c->packed_band_rows = (int)tuning_lookup("packed", radius, n, "band_rows", 0);
     if (variant == LTL_VARIANT_PLAIN) e = plain_prepare(radius);
+    if (variant == LTL_VARIANT_PLAIN && e == cudaSuccess) e = plain_tb_prepare(radius);
     if (variant == LTL_VARIANT_PACKED) e = packed_prepare(radius);
     if (e != cudaSuccess) {
         ltl_set_error("ltl_create: kernel setup failed: %s", cudaGetErrorString(e));
@@ -383,9 +389,10 @@ extern "C" int ltl_download_device(ltl_ctx* c, uint8_t* dev_inner, size_t pitch)
     return LTL_OK;
 }
 
-// One pass = `c->depth` generations (1 except for the temporally blocked
-// tensor path).  Leaves the result in nxt and swaps.
-static cudaError_t enqueue_pass(ltl_ctx* c) {
+// One pass = `gens` generations (c->depth, or fewer for the remainder of a
+// step count; only the temporally blocked plain kernel takes more than 1).
+// Leaves the result in nxt and swaps.
+static cudaError_t enqueue_pass(ltl_ctx* c, int gens) {
     cudaError_t e = cudaSuccess;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c->timing) {
@@ -399,7 +406,10 @@ static cudaError_t enqueue_pass(ltl_ctx* c) {
         case LTL_VARIANT_PLAIN: {
             Frame& a = cur_frame(c);
             Frame& b = nxt_frame(c);
-            if (plain_swar8_supported(c->rule.radius)) {
+            if (gens > 1) {
+                e = launch_plain_tb(a, b, c->rule, c->band_rows, gens, c->stream);
+                step_kernels = 1;
+            } else if (plain_swar8_supported(c->rule.radius)) {
                 e = launch_plain_swar8(a, b, c->rule, c->band_rows, c->stream);
                 step_kernels = 1;
             } else {
@@ -440,7 +450,7 @@ static int build_graph(ltl_ctx* c, int which) {
     cudaGraph_t g = nullptr;
     LTL_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
-    for (int p = 0; p < kGraphPasses && e == cudaSuccess; ++p) e = enqueue_pass(c);
+    for (int p = 0; p < kGraphPasses && e == cudaSuccess; ++p) e = enqueue_pass(c, c->depth);
     cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
     c->cur_is_a = saved;
     if (e != cudaSuccess || e2 != cudaSuccess) {
@@ -469,11 +479,8 @@ extern "C" int ltl_step(ltl_ctx* c, int steps) {
     if (c->variant == LTL_VARIANT_PACKED && !c->packed_valid) {
         if (int r = sync_to_packed(c)) return r;
     }
-    if (steps % c->depth != 0) {
-        ltl_set_error("ltl_step: %d steps is not a multiple of the temporal depth %d", steps, c->depth);
-        return LTL_EINVAL;
-    }
     int passes = steps / c->depth;
+    const int rest = steps % c->depth;  // a last, shorter pass
     while (!c->timing && passes >= kGraphPasses) {
         int which = c->cur_is_a ? 0 : 1;
         if (!c->graph[which]) {
@@ -483,7 +490,8 @@ extern "C" int ltl_step(ltl_ctx* c, int steps) {
         // kGraphPasses is even: the parity of the current buffer is unchanged
         passes -= kGraphPasses;
     }
-    for (int p = 0; p < passes; ++p) LTL_CUDA(enqueue_pass(c));
+    for (int p = 0; p < passes; ++p) LTL_CUDA(enqueue_pass(c, c->depth));
+    if (rest > 0) LTL_CUDA(enqueue_pass(c, rest));
     return LTL_OK;
 }
 
@@ -581,6 +589,20 @@ extern "C" int ltl_set_param(ltl_ctx* c, const char* name, long long value) {
             ltl_set_error("ltl_set_param: band_rows applies to the plain and packed variants");
             return LTL_EUNSUPPORTED;
         }
+        drop_graphs(c);
+        return LTL_OK;
+    }
+    if (std::strcmp(name, "depth") == 0) {
+        if (c->variant != LTL_VARIANT_PLAIN) {
+            ltl_set_error("ltl_set_param: depth applies to the plain variant");
+            return LTL_EUNSUPPORTED;
+        }
+        if (value != 1 && !(plain_tb_supported(c->rule.radius, (int)value) && c->fa.H >= value * c->rule.radius)) {
+            ltl_set_error("ltl_set_param: depth %lld is not supported for R=%d (1, or 2..3 with depth*R <= 16 and R <= 5)",
+                          value, c->rule.radius);
+            return LTL_EINVAL;
+        }
+        c->depth = (int)value;
         drop_graphs(c);
         return LTL_OK;
     }

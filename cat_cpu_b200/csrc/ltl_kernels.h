@@ -21,6 +21,12 @@ cudaError_t packed_prepare(int radius);
 cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows,
                                cudaStream_t s);
 int plain_swar8_band_rows(int n, int device);
+// Temporally blocked SWAR step: `depth` (2 or 3, depth * R <= 16) generations per
+// pass; the frames' halo must be at least depth * R.
+bool plain_tb_supported(int radius, int depth);
+cudaError_t plain_tb_prepare(int radius);
+cudaError_t launch_plain_tb(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows, int depth,
+                            cudaStream_t s);
 
 // K1 generic path (any R): vertical sliding sums into `vbuf` (uint16, n rows x
 // pitch entries), then a prefix-sum horizontal pass with the rule fused.

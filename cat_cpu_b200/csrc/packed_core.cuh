@@ -151,4 +151,102 @@ __device__ __forceinline__ void hcount(const uint32_t* __restrict__ row, int fw,
     wallace<2 * R + 1, 0, PH>(x, h);
 }
 
+// Shared-memory ring of the last 2R+2 row counts h (PH planes per lane, one
+// ring per warp), so that each row's horizontal count is computed once on
+// entry and read back on exit.  Without it (kRing = false) the leaving row is
+// counted again.
+template <int R, int kWarps>
+struct PackedRing {
+    static constexpr int PH = bits_for(2 * R + 1);
+    static constexpr int ROWS = 2 * R + 2;
+    static constexpr int WARP_WORDS = ROWS * PH * 32;
+    static constexpr int BYTES = WARP_WORDS * 4 * kWarps;
+    static constexpr bool fits = BYTES <= 96 * 1024;
+};
+
+// One warp's band of output rows [r0, r1) of a packed frame, word column fw
+// of each lane: next = s ? [smin+1 <= B <= smax+1] : [bmin <= B <= bmax] with
+// B the box count (centre included), kept as PB bit planes and slid down the
+// band (B -= h(r - R), B += h(r + R + 1)).  `cur`/`nxt` point at frame row 0,
+// `HR` halo rows, `wp` words per frame row.  ring_lane = this warp's ring + lane
+// (unused when !kRing).  All lanes of the warp must call it together.
+template <int R, bool kRing>
+__device__ __forceinline__ void packed_band(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, size_t wp,
+                                            int HR, int r0, int r1, int fw, bool active, bool outputs, int lane,
+                                            uint32_t* ring_lane, const PackedRule& pr) {
+    constexpr int PH = bits_for(2 * R + 1);
+    constexpr int PB = bits_for((2 * R + 1) * (2 * R + 1));
+    constexpr int RING = 2 * R + 2;
+    // row pointers advance by one frame row per output row; the ring slots of
+    // rows r - R (read back) and r + R + 1 (written) advance with them
+    const uint32_t* rin = cur + (size_t)(HR + r0 - R) * wp;   // next row to count
+    const uint32_t* rs = cur + (size_t)(HR + r0) * wp + fw;   // centre row
+    uint32_t* ro = nxt + (size_t)(HR + r0) * wp + fw;         // output row
+    uint32_t B[PB];
+#pragma unroll
+    for (int i = 0; i < PB; ++i) B[i] = 0u;
+#pragma unroll 1
+    for (int k = 0; k < 2 * R + 1; ++k, rin += wp) {
+        uint32_t h[PH];
+        hcount<R, PH>(rin, fw, active, lane, h);
+        planes_add<PB, PH>(B, h);
+        if constexpr (kRing) {
+            uint32_t* sl = ring_lane + k * PH * 32;
+#pragma unroll
+            for (int i = 0; i < PH; ++i) sl[32 * i] = h[i];
+        }
+    }
+    int out_slot = 0;  // ring slot of row r - R; row r + R + 1 goes to the slot before it
+#pragma unroll 1
+    for (int r = r0; r < r1; ++r, rs += wp, ro += wp, rin += wp) {
+        if (outputs) {
+            const uint32_t sv = __ldg(rs);
+            const uint32_t in1 = planes_in<PB>(B, pr.lo[1], pr.hi[1]) & pr.keep[1];
+            const uint32_t in0 = planes_in<PB>(B, pr.lo[0], pr.hi[0]) & pr.keep[0];
+            *ro = (sv & in1) | (~sv & in0);
+        }
+        if (r + 1 < r1) {
+            uint32_t h[PH];
+            const int in_slot = out_slot == 0 ? RING - 1 : out_slot - 1;
+            if constexpr (kRing) {
+                const uint32_t* sl = ring_lane + out_slot * PH * 32;
+#pragma unroll
+                for (int i = 0; i < PH; ++i) h[i] = sl[32 * i];
+            } else {
+                hcount<R, PH>(rin - (size_t)(2 * R + 1) * wp, fw, active, lane, h);
+            }
+            planes_sub<PB, PH>(B, h);
+            hcount<R, PH>(rin, fw, active, lane, h);
+            planes_add<PB, PH>(B, h);
+            if constexpr (kRing) {
+                uint32_t* sl = ring_lane + in_slot * PH * 32;
+#pragma unroll
+                for (int i = 0; i < PH; ++i) sl[32 * i] = h[i];
+            }
+            out_slot = out_slot + 1 == RING ? 0 : out_slot + 1;
+        }
+    }
+}
+
+// Halo word fw of a packed frame row with one halo word per side (inner word w
+// at frame word 1 + w): fw = 0 is the left halo (cells n-32 .. n-1), fw = nw
+// the last inner word with its bits past n rewritten (cells 0 ..), fw = nw + 1
+// the right halo (cells 32 nw - n .. 32 nw - n + 31).  For n >= 64 each is a
+// funnel shift of two inner words; `slow` handles smaller grids bit by bit.
+// Only inner bits (< n) are read, so concurrent writers of other halo words
+// of the same row do not matter.
+template <class Slow>
+__device__ __forceinline__ uint32_t packed_halo_word(const uint32_t* row, int fw, int n, int nw, Slow&& slow) {
+    if (n >= 64) {
+        if (fw == nw) {
+            const int ib = n - 32 * (nw - 1);  // inner bits of the last word, 1..32
+            return ib >= 32 ? row[fw] : ((row[fw] & ((1u << ib) - 1u)) | (row[1] << ib));
+        }
+        const int c = fw == 0 ? n - 32 : 32 * nw - n;  // first cell of the word
+        const uint32_t lo = row[1 + (c >> 5)];
+        return (c & 31) ? __funnelshift_r(lo, row[2 + (c >> 5)], c & 31) : lo;
+    }
+    return slow();
+}
+
 }  // namespace ltl

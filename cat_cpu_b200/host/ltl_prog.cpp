@@ -1,14 +1,15 @@
 // ltl_prog.cpp -- native CLI with the reference's shape for the GPU solvers.
 //
 //   ltl_prog n solver steps [-g deviceId] -d density [--seed S] [--threads T]
-//            [--doVerify] [--radius R] [--rule SMIN SMAX BMIN BMAX]
+//            [--doVerify] [--radius R] [--rule SMIN SMAX BMIN BMAX] [--depth D]
 //
 // Mirrors kezada94/CAT_cpu src/main.cpp:31-130 with solver codes 7 (plain
 // CUDA-core), 8 (tcgen05 tensor core), 9 (bit-packed).  The start grid is the
 // reference benchmark's (CPUBenchmark.cpp:21-32), the timed region is
 // doSteps(steps) plus device completion (CPUBenchmark.cpp:63-85), and stdout is
 // the mean ms per step (StatsCollector.cpp:65-68).  --doVerify repeats the run on
-// the plain GPU solver and compares every cell (main.cpp:64-90).
+// the plain GPU solver, one generation per pass, and compares every cell
+// (main.cpp:64-90).  --depth sets solver 7's generations per pass (0: default).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -19,7 +20,7 @@
 #include "ltl_solver.hpp"
 
 struct Args {
-    int n = 0, solver = -1, steps = 0, device = 0, seed = 0, threads = 1, radius = 1;
+    int n = 0, solver = -1, steps = 0, device = 0, seed = 0, threads = 1, radius = 1, depth = 0;
     float density = -1.f;
     bool verify = false;
     int rule[4] = {2, 3, 3, 3};
@@ -28,7 +29,7 @@ struct Args {
 static void usage() {
     std::printf(
         "usage: ltl_prog n solver steps [-g deviceId] -d density [--seed S] [--threads T] [--doVerify]\n"
-        "                [--radius R] [--rule SMIN SMAX BMIN BMAX]\n"
+        "                [--radius R] [--rule SMIN SMAX BMIN BMAX] [--depth D]\n"
         "  solver: 7 - GPU plain CUDA-core, 8 - GPU tcgen05 tensor core, 9 - GPU bit-packed\n");
 }
 
@@ -43,6 +44,7 @@ static bool parse(int argc, char** argv, Args& a) {
         else if (s == "--threads" && need(1)) a.threads = std::atoi(argv[++i]);
         else if (s == "--radius" && need(1)) a.radius = std::atoi(argv[++i]);
         else if (s == "--rule" && need(4)) for (int k = 0; k < 4; ++k) a.rule[k] = std::atoi(argv[++i]);
+        else if (s == "--depth" && need(1)) a.depth = std::atoi(argv[++i]);
         else if (s == "--doVerify") a.verify = true;
         else if (s == "-h" || s == "--help") return false;
         else pos.push_back(s);
@@ -76,10 +78,10 @@ int main(int argc, char** argv) {
     }
     try {
         ltl::GpuSolver s(a.device, a.n, a.radius, a.rule[0], a.rule[1], a.rule[2], a.rule[3], variant, a.threads);
+        if (a.depth > 0) s.setParam("depth", a.depth);
         const int state_seed = ltl_benchmark_seed(a.seed);
         s.resetState(state_seed, a.density);
-        const int depth = s.info().temporal_depth;
-        const int steps = a.steps - a.steps % depth;
+        const int steps = a.steps;
         auto t0 = std::chrono::high_resolution_clock::now();
         s.doSteps(steps);
         s.synchronize();
@@ -90,6 +92,7 @@ int main(int argc, char** argv) {
             std::printf("\n[VERIFY] verifying...\n\n");
             ltl::GpuSolver ref(a.device, a.n, a.radius, a.rule[0], a.rule[1], a.rule[2], a.rule[3],
                                LTL_VARIANT_PLAIN, a.threads);
+            ref.setParam("depth", 1);
             ref.resetState(state_seed, a.density);
             ref.doSteps(steps);
             if (s.getCurrentState() != ref.getCurrentState()) {

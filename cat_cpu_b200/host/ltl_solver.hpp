@@ -58,6 +58,8 @@ class GpuSolver {
             std::printf("\n");
         }
     }
+    // Shape parameters (ltl_set_param): "band_rows", "depth", ...
+    void setParam(const char* name, long long value) { check(ltl_set_param(ctx_, name, value), "ltl_set_param"); }
     ltl_info info() const {
         ltl_info i{};
         check(ltl_get_info(ctx_, &i), "ltl_get_info");

@@ -204,6 +204,7 @@ class CUDASolver:
 
     def set_param(self, name, value):
         check(lib().ltl_set_param(self._h, name.encode(), int(value)))
+        self.info = self.get_info()
 
     def set_timing(self, enable):
         check(lib().ltl_set_timing(self._h, int(bool(enable))))

@@ -2,7 +2,7 @@
 
     python -m cat_cpu_b200.prog n solver steps [-g deviceId] [-d density] [--seed S]
                                 [--threads T] [--doVerify] [--radius R]
-                                [--rule SMIN SMAX BMIN BMAX]
+                                [--rule SMIN SMAX BMIN BMAX] [--depth D]
 
 Mirrors the reference's main.cpp (kezada94/CAT_cpu src/main.cpp:31-130):
 `solver` selects the GPU solver (7 = plain CUDA-core, 8 = tcgen05 tensor core,
@@ -13,8 +13,9 @@ milliseconds per step (StatsCollector::printShortStats, StatsCollector.cpp:65-68
 Radius and rule default to the reference's compile-time defaults (Makefile:10-14:
 R=1, S2-3, B3-3) and are run-time options here.
 
---doVerify re-runs the same start grid on the plain GPU solver (code 7) and
-compares every cell, printing the reference's "[VERIFY] ..." lines; exit 1 on a
+--depth sets solver 7's generations per kernel pass (temporal blocking; 0 keeps
+the tuned default).  --doVerify re-runs the same start grid on the plain GPU
+solver (code 7, one generation per pass) and compares every cell, printing the reference's "[VERIFY] ..." lines; exit 1 on a
 mismatch (main.cpp:64-90).
 """
 import argparse
@@ -35,6 +36,8 @@ def parse(argv):
     ap.add_argument("--doVerify", action="store_true")
     ap.add_argument("--radius", type=int, default=1)
     ap.add_argument("--rule", type=int, nargs=4, default=[2, 3, 3, 3], metavar=("SMIN", "SMAX", "BMIN", "BMAX"))
+    ap.add_argument("--depth", type=int, default=0,
+                    help="solver 7: generations per kernel pass (0 = the tuned default)")
     return ap.parse_args(argv)
 
 
@@ -48,14 +51,15 @@ def run(args):
     if solver is None:
         print("main(): solver is NULL")
         return 1, None, None
+    if args.depth:
+        solver.set_param("depth", args.depth)
     start = C.start_grid(args.n, args.seed, args.density, args.threads)
     solver.setState(start)
     stream = torch.cuda.Stream()
     solver.set_stream(stream.cuda_stream)
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
-    depth = solver.info.temporal_depth
-    steps = args.steps - args.steps % depth
+    steps = args.steps
     a.record(stream)
     solver.doSteps(steps)
     b.record(stream)
@@ -76,6 +80,8 @@ def main(argv=None):
         print("\n[VERIFY] verifying...\n")
         ref = C.CASolverFactory.createSolver(7, args.deviceId, args.n, args.radius, args.threads,
                                              tuple(args.rule))
+        if ref.radius <= 5:
+            ref.set_param("depth", 1)  # one generation per pass: independent of the temporally blocked kernel
         ref.setState(start)
         ref.doSteps(steps)
         if not np.array_equal(solver.getCurrentState(), ref.getCurrentState()):

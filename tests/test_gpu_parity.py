@@ -113,6 +113,57 @@ def test_random_vs_oracle_every_step(variant):
             s.close()
 
 
+def test_plain_temporal_depths_vs_oracle():
+    """The temporally blocked plain kernel (2 or 3 generations per pass) against
+    the oracle: every R it supports, ragged and tiny sides, several band heights
+    (bands that end inside the grid and bands longer than the grid), and step
+    counts that leave a shorter last pass."""
+    rng = np.random.default_rng(29)
+    for r in (1, 2, 3, 4, 5):
+        for depth in (2, 3):
+            if depth * r > 16:
+                continue
+            for trial in range(3):
+                n = int(rng.choice([r, r + 1, 17, 97, 130, 263, 600]))
+                band = int(rng.choice([16, 23, 64, 128, 700]))
+                steps = int(rng.integers(1, 8))
+                N = (2 * r + 1) ** 2
+                lo = int(rng.integers(0, N // 3))
+                rule = (lo, lo + int(rng.integers(1, N // 2)), int(rng.integers(0, N // 3)), int(rng.integers(N // 3, N)))
+                g = (rng.random((n, n)) < rng.uniform(0.25, 0.6)).astype(np.uint8)
+                s = make("plain", n, r, rule)
+                try:
+                    s.set_param("depth", depth)
+                    s.set_param("band_rows", band)
+                    assert s.info.temporal_depth == depth
+                    s.setState(g)
+                    s.doSteps(steps)
+                    want = O.run(g, r, rule, steps)
+                    got = s.getCurrentState()
+                    assert np.array_equal(got, want), \
+                        f"R={r} depth={depth} n={n} band={band} steps={steps} rule={rule}: " + describe_mismatch(got, want)
+                finally:
+                    s.close()
+
+
+def test_plain_default_depth_and_limits():
+    s = make("plain", 1024, 5, O.BOSCO_R5)
+    try:
+        assert s.info.temporal_depth in (1, 2, 3)
+        with pytest.raises(C.LtlError):
+            s.set_param("depth", 4)        # 4 * 5 > 16
+        s.set_param("depth", 1)
+        assert s.info.temporal_depth == 1
+    finally:
+        s.close()
+    s = make("plain", 300, 8, O.sweep_rule(8))
+    try:
+        with pytest.raises(C.LtlError):
+            s.set_param("depth", 2)        # R > 5 runs the generic kernel only
+    finally:
+        s.close()
+
+
 @pytest.mark.parametrize("variant", VARIANTS)
 def test_counts_near_thresholds_r5(variant):
     """Every count value 0..120 sits on a threshold at least once: sweep rules over
