@@ -9,6 +9,7 @@
 //   rule  transitionFunction [a <= k <= b], HostSolver.tpp:47-51
 //   halo  fillHorizontal/VerticalBoundaryConditions (torus), HostSolver.tpp:93-140
 #include <algorithm>
+#include <type_traits>
 
 #include "ltl_kernels.h"
 
@@ -385,11 +386,15 @@ k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int
         const int rlast = r1 - 1 + D * R;          // last input row of the band
         const int yfirst = r0 - (D - 1) * R;        // first and last stage-1 rows
         const int ylast = r1 - 1 + (D - 1) * R;
-        auto issue = [&](int r) {
+        for (int r = yfirst - R; r <= yfirst + R + kAh; ++r) {
             if (loads && r <= rlast) cp_async16(slot0(r), col + (size_t)(H + r) * pitch);
             cp_async_commit();
-        };
-        for (int r = yfirst - R; r <= yfirst + R + kAh; ++r) issue(r);
+        }
+        // next input row to request (y + R + 1 + kAh at iteration y), and the
+        // output row of stage D once it produces (y - (D-1)R)
+        int r_next = yfirst + R + 1 + kAh;
+        const uint8_t* src_next = col + (size_t)(H + r_next) * pitch;
+        uint8_t* dst = nxt + (size_t)(H + r0) * pitch + H + x;
         cp_async_wait<kAh>();
         uint32_t V[D][4];
 #pragma unroll
@@ -403,27 +408,26 @@ k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int
 #pragma unroll
         for (int k = 1; k < D; ++k) sl[k] = ((yfirst - (k - 1) * R) % kRS + kRS) % kRS;
 
-#pragma unroll 1
-        for (int y = yfirst; y <= ylast; ++y) {
-            // stage 1: row y
+        // One iteration (stage-1 row y).  Stage k >= 2 absorbs row yin = y - (k-2)R
+        // of stage k-1 and, once its window is full, produces row yin - R.  In ring
+        // k-1 the leaving row yin - 2R - 1 sits one slot after yin, and row yin - R
+        // sits R + 2 after.  kSteady: every stage's window is full and sliding (from
+        // y = yfirst + 2R(D-1) + 1 on), so no stage needs its fill checks.
+        auto iteration = [&](int y, auto steady) {
+            constexpr bool kSteady = decltype(steady)::value;
             uint4 prod = swar8_row<R>(V[0], *slot0(y), q);
             *slotk(1, sl[1]) = prod;
-            // stages 2..D: stage k absorbs row yin = y - (k-2)R of stage k-1 and, once
-            // its window is full, produces row yin - R.  In ring k-1 the leaving row
-            // yin - 2R - 1 sits one slot after yin, and row yin - R sits R + 2 after.
             bool live = true;
 #pragma unroll
             for (int k = 2; k <= D; ++k) {
-                if (live) {
-                    const int yin = y - (k - 2) * R;
-                    const int absorbed = yin - (r0 - (D - k + 1) * R) + 1;  // rows of stage k-1 so far
+                if (kSteady || live) {
+                    const int absorbed = kSteady ? 0 : (y - (k - 2) * R) - (r0 - (D - k + 1) * R) + 1;
                     v_add(V[k - 1], prod);
-                    if (absorbed > 2 * R + 1) {
+                    if (kSteady || absorbed > 2 * R + 1) {
                         const uint4 out = *slotk(k - 1, wrap(sl[k - 1] + 1));
                         V[k - 1][0] -= out.x; V[k - 1][1] -= out.y; V[k - 1][2] -= out.z; V[k - 1][3] -= out.w;
                     }
-                    if (absorbed >= 2 * R + 1) {
-                        const int yk = yin - R;
+                    if (kSteady || absorbed >= 2 * R + 1) {
                         const uint4 c = *slotk(k - 1, wrap(sl[k - 1] + R + 2));
                         if (k < D) {
                             prod = swar8_row<R>(V[k - 1], c, q);
@@ -431,13 +435,13 @@ k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int
                         } else {
                             const uint4 o = swar8_row<R>(V[k - 1], c, q);
                             if (outputs) {
-                                uint8_t* dst = nxt + (size_t)(H + yk) * pitch + H + x;
                                 if (x + 16 <= n) {
                                     *(uint4*)dst = o;
                                 } else {
                                     store_partial16(dst, o, n - x);
                                 }
                             }
+                            dst += pitch;
                         }
                     } else {
                         live = false;
@@ -447,11 +451,20 @@ k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int
 #pragma unroll
             for (int k = 1; k < D; ++k) sl[k] = wrap(sl[k] + 1);
             if (y < ylast) {
-                issue(y + R + 1 + kAh);
+                if (loads && r_next <= rlast) cp_async16(slot0(r_next), src_next);
+                cp_async_commit();
+                ++r_next;
+                src_next += pitch;
                 cp_async_wait<kAh>();  // input row y + R + 1 has landed
                 v_slide(V[0], *slot0(y + R + 1), *slot0(y - R));
             }
-        }
+        };
+        const int ysteady = yfirst + 2 * R * (D - 1) + 1;
+        int y = yfirst;
+#pragma unroll 1
+        for (; y < ysteady && y <= ylast; ++y) iteration(y, std::false_type{});
+#pragma unroll 1
+        for (; y <= ylast; ++y) iteration(y, std::true_type{});
         cp_async_wait<0>();
     }
 }
