@@ -222,6 +222,10 @@ constexpr int kHCol = 0;               // TMEM column of H
 constexpr int kCCol = 256;             // TMEM column of C
 constexpr int kN1 = 32;                // product-1 column chunk
 constexpr int kEpiGroups = 4;          // epilogue warp groups (column blocks round-robin)
+// The MMA warp waits for the epilogue most of the time; between its tries it
+// sleeps this long, so that it leaves issue slots to the epilogue warps that
+// share its scheduler.
+constexpr uint32_t kMmaSleepNs = 32;
 constexpr int kMaxChunks = 4;          // 16-column chunks per epilogue warp: 2 blocks of 32 (Tc <= 256)
 constexpr int kEpiWarps = 4 * kEpiGroups;
 constexpr int kThreads = 64 + 32 * kEpiWarps;  // producer + MMA + epilogue warps
@@ -392,7 +396,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             };
             // product 2 of tile j: C = B_v * H(j), H(j) in shared-memory buffer j % 2
             auto product2 = [&](int j) -> bool {
-                if (j >= 1 && !mbar_wait(&bars[C_EMPTY], (uint32_t)(j - 1) & 1u, p.wait_ns)) return false;
+                if (j >= 1 && !mbar_wait(&bars[C_EMPTY], (uint32_t)(j - 1) & 1u, p.wait_ns, kMmaSleepNs)) return false;
                 tc_fence_after();
                 const uint32_t ha = ha0 + (j & 1) * 128 * Tc;
 #pragma unroll
@@ -408,7 +412,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             // back, then product 2 of tile j once C(j-1) has been read.
             ok = mine >= 1 ? product1(0) : true;
             for (int j = 0; j < mine && ok; ++j) {
-                ok = mbar_wait(&bars[HS_FULL], (uint32_t)j & 1u, p.wait_ns);
+                ok = mbar_wait(&bars[HS_FULL], (uint32_t)j & 1u, p.wait_ns, kMmaSleepNs);
                 if (ok && j + 1 < mine) ok = product1(j + 1);
                 if (ok) ok = product2(j);
             }

@@ -18,6 +18,27 @@ __host__ __device__ constexpr int bits_for(int v) {
     return b;
 }
 
+// Three-input logic as single lop3 operations (the compiler does not always
+// fuse these bit-sliced expressions into one instruction on its own):
+//   xor3    a ^ b ^ c                       (sum of a full adder)     0x96
+//   maj3    (a & b) | (a & c) | (b & c)     (carry of a full adder)   0xE8
+//   borrow3 (~a & (b | c)) | (b & c)        (borrow out of a - b - c) 0x8E
+__device__ __forceinline__ uint32_t xor3(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t d;
+    asm("lop3.b32 %0, %1, %2, %3, 0x96;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+__device__ __forceinline__ uint32_t maj3(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t d;
+    asm("lop3.b32 %0, %1, %2, %3, 0xE8;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+__device__ __forceinline__ uint32_t borrow3(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t d;
+    asm("lop3.b32 %0, %1, %2, %3, 0x8E;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
 // Wallace reduction: out[0..P) = bit planes of the number of set inputs per lane.
 template <int M, int L, int P>
 __device__ __forceinline__ void wallace(const uint32_t* v, uint32_t* out) {
@@ -35,8 +56,8 @@ __device__ __forceinline__ void wallace(const uint32_t* v, uint32_t* out) {
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 uint32_t a = acc, b = v[1 + 2 * f], c = v[2 + 2 * f];
-                acc = a ^ b ^ c;
-                carry[f] = (a & b) | (a & c) | (b & c);
+                acc = xor3(a, b, c);
+                carry[f] = maj3(a, b, c);
             }
             if constexpr (NH == 1) {
                 uint32_t b = v[M - 1];
@@ -55,10 +76,14 @@ __device__ __forceinline__ void planes_sub(uint32_t (&B)[PB], const uint32_t (&h
     uint32_t br = 0u;
 #pragma unroll
     for (int i = 0; i < PB; ++i) {
-        uint32_t b = B[i];
-        uint32_t x = (i < PH) ? h[i] : 0u;
-        B[i] = b ^ x ^ br;
-        br = (~b & (x | br)) | (x & br);
+        const uint32_t b = B[i];
+        if (i < PH) {
+            B[i] = xor3(b, h[i], br);
+            br = borrow3(b, h[i], br);
+        } else {
+            B[i] = b ^ br;
+            br = ~b & br;
+        }
     }
 }
 
@@ -68,24 +93,43 @@ __device__ __forceinline__ void planes_add(uint32_t (&B)[PB], const uint32_t (&h
     uint32_t cy = 0u;
 #pragma unroll
     for (int i = 0; i < PB; ++i) {
-        uint32_t b = B[i];
-        uint32_t x = (i < PH) ? h[i] : 0u;
-        B[i] = b ^ x ^ cy;
-        cy = (b & x) | (b & cy) | (x & cy);
+        const uint32_t b = B[i];
+        if (i < PH) {
+            B[i] = xor3(b, h[i], cy);
+            cy = maj3(b, h[i], cy);
+        } else {
+            B[i] = b ^ cy;
+            cy = b & cy;
+        }
     }
 }
 
+// One step of each comparator chain as a single three-input logic operation
+// (written as lop3 so that the run-time mask operand costs one instruction):
+//   ge_step(m, b, ge) = m ? (b & ge) : (b | ge)      truth table 0x8E
+//   le_step(m, b, le) = m ? (~b | le) : (~b & le)    truth table 0xB2
+__device__ __forceinline__ uint32_t ge_step(uint32_t m, uint32_t b, uint32_t ge) {
+    uint32_t d;
+    asm("lop3.b32 %0, %1, %2, %3, 0x8E;" : "=r"(d) : "r"(m), "r"(b), "r"(ge));
+    return d;
+}
+__device__ __forceinline__ uint32_t le_step(uint32_t m, uint32_t b, uint32_t le) {
+    uint32_t d;
+    asm("lop3.b32 %0, %1, %2, %3, 0xB2;" : "=r"(d) : "r"(m), "r"(b), "r"(le));
+    return d;
+}
+
 // Lanes where lo <= B <= hi, given the thresholds as per-plane masks (all-ones
-// where the threshold's bit is set); lo, hi < 2^PB.  Two carry chains:
+// where the threshold's bit is set); lo, hi < 2^PB.  Two carry chains from the
+// least significant plane up:
 //   ge = carry out of B + ~lo + 1,  le = carry out of hi + ~B + 1.
 template <int PB>
 __device__ __forceinline__ uint32_t planes_in(const uint32_t (&B)[PB], const uint32_t* lm, const uint32_t* hm) {
     uint32_t ge = 0xffffffffu, le = 0xffffffffu;
 #pragma unroll
     for (int i = 0; i < PB; ++i) {
-        const uint32_t b = B[i];
-        ge = (lm[i] & (b & ge)) | (~lm[i] & (b | ge));
-        le = (hm[i] & (~b | le)) | (~hm[i] & (~b & le));
+        ge = ge_step(lm[i], B[i], ge);
+        le = le_step(hm[i], B[i], le);
     }
     return ge & le;
 }
