@@ -119,7 +119,7 @@ def main():
     table = [f"# autotuned on {dev} by cat_cpu_b200/autotune.py, {time.strftime('%Y-%m-%d %H:%M:%S')}"]
     land = [f"# landscape ({dev}): candidate -> ms per step (single grids) or per 256-step batch run"]
     plain_c = [64, 128, 256, 512] if args.quick else [64, 96, 128, 192, 256, 384, 512]
-    packed_c = [32, 64, 128] if args.quick else [32, 48, 64, 96, 128, 192, 256]
+    packed_c = [0, 32, 64, 128] if args.quick else [0, 32, 48, 64, 96, 128, 192, 256]  # 0: built-in choice
     jobs = [("plain", 16384, 5, BOSCO_R5, plain_c), ("plain", 4096, 5, BOSCO_R5, plain_c),
             ("packed", 16384, 5, BOSCO_R5, packed_c), ("packed", 32768, 5, BOSCO_R5, packed_c)]
     for r in (1, 2, 4, 8, 16, 32):

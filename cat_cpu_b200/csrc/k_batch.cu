@@ -158,7 +158,7 @@ k_batch_resident(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, c
         __syncthreads();
         smem_halo(bufA, g.n, g.nw, g.HR, g.wp);
         // work split: every warp owns a band of rows of one 32-word strip
-        const int strips = (g.nw + 1 + 31) / 32;
+        const int strips = (g.nw + 31) / 32;
         const int warps = blockDim.x >> 5;
         const int bands = max(1, warps / strips);
         const int band_rows = (g.n + bands - 1) / bands;
@@ -458,7 +458,7 @@ static int batch_plan(ltl_batch* b) {
         std::vector<int4> items;
         for (int gi : c.streamed) {
             const BatchGrid& g = b->grids[gi];
-            const int strips = (g.nw + 1 + 31) / 32;
+            const int strips = (g.nw + 31) / 32;
             const int band_rows = b->stream_band_rows;
             for (int r0 = 0; r0 < g.n; r0 += band_rows)
                 for (int ws = 0; ws < strips; ++ws) items.push_back(make_int4(gi, r0, std::min(g.n, r0 + band_rows), ws));

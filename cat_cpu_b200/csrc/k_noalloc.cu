@@ -9,9 +9,9 @@
 //     forbid allocation (and the implicit synchronisation cudaMalloc/cudaFree
 //     bring) on the hot path;
 //   - plug-ins that are handed device buffers and a stream and nothing else.
-// The regular entry points allocate two halo'd grids (and, for R > 5, a column
-// sum buffer) per solver.  This entry point instead keeps that scratch in one
-// fixed array in device global memory that is part of the library image:
+// The regular entry points allocate two halo'd grids per solver.  This entry
+// point instead keeps that scratch in one fixed array in device global memory
+// that is part of the library image:
 // every GPU that loads libltl_b200.so holds kNoAllocScratchBytes of it until
 // the process exits, and no call allocates or frees anything.
 #include <cstdio>
@@ -111,7 +111,7 @@ extern "C" int ltl_step_noalloc(const uint8_t* dev_in, size_t in_pitch, uint8_t*
     Frame* nxt = &fb;
     for (int i = 0; i < steps && e == cudaSuccess; ++i) {
         e = generic ? launch_plain_generic(*cur, *nxt, rule, vbuf, s)
-                    : launch_plain_swar8(*cur, *nxt, rule, band_rows, s);
+                    : launch_plain_swar8(*cur, *nxt, rule, band_rows, false, s);
         if (e == cudaSuccess) e = launch_halo_fill(*nxt, s);
         Frame* t = cur;
         cur = nxt;

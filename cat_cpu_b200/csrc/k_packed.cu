@@ -20,14 +20,15 @@ namespace ltl {
 
 constexpr int kPackedWarps = 4;
 
-// Rows per work item: enough items for ~32 resident warps per SM, but at least
-// 32 rows so that the (2R+1)-row start-up of each band stays a small fraction.
-static int packed_band_rows(int n, int n_wstrips, int sms) {
-    long long want_items = (long long)sms * 32;
-    long long bands = std::max<long long>(1, want_items / std::max(n_wstrips, 1));
-    int rows = (int)((n + bands - 1) / bands);
-    rows = std::max(32, std::min(rows, 256));
-    return (rows + 15) / 16 * 16;
+// Rows per work item when no tuned value applies: as few bands as fill every
+// resident warp once (each band re-counts 2R+1 rows to start its window, so
+// fewer, longer bands waste less), split further only where a band would be
+// longer than 256 rows.
+static int packed_band_rows(int n, int n_wstrips, int resident_warps) {
+    const int per_wave = std::max(1, resident_warps / std::max(n_wstrips, 1));
+    int bands = per_wave;
+    while ((n + bands - 1) / bands > 256) bands += per_wave;
+    return std::max(16, (n + bands - 1) / bands);
 }
 
 template <int R>
@@ -63,13 +64,17 @@ static cudaError_t launch_packed_r(const PackedFrame& c, const PackedFrame& x, c
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int n_wstrips = (c.nw + 1 + 31) / 32;
-    const int band_rows = band_override > 0 ? band_override : packed_band_rows(c.n, n_wstrips, sms);
-    const int bands = (c.n + band_rows - 1) / band_rows;
-    const int items = n_wstrips * bands;
+    // strips of 32 words cover the inner words; a lane whose word is the right
+    // halo word (w == nw) only feeds its left neighbour, and lane 31 loads the
+    // word past its own directly, so no strip is needed for the halo alone
+    const int n_wstrips = (c.nw + 31) / 32;
     const int smem = PackedRing<R, kPackedWarps>::fits ? PackedRing<R, kPackedWarps>::BYTES : 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_packed_step<R>, kPackedWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
+    const int band_rows =
+        band_override > 0 ? band_override : packed_band_rows(c.n, n_wstrips, sms * per_sm * kPackedWarps);
+    const int bands = (c.n + band_rows - 1) / band_rows;
+    const int items = n_wstrips * bands;
     int ctas = std::min((items + kPackedWarps - 1) / kPackedWarps, sms * per_sm);
     k_packed_step<R><<<ctas, kPackedWarps * 32, smem, s>>>(c.words, x.words, c.n, c.nw, c.HR, c.HW, c.wpitch,
                                                            n_wstrips, items, band_rows, pr);
@@ -179,15 +184,28 @@ cudaError_t launch_packed_halo(const PackedFrame& f, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // Byte frame <-> packed frame (inner cells only; halos are refilled after).
 // ---------------------------------------------------------------------------
+// Four 0/1 bytes of a word -> 4 bits: the multiply places byte k's bit at bit
+// 24 + k with no two partial products overlapping (so no carries), and back:
+// the 4 bits of a nibble spread to bit 0 of each byte by copies 7 bits apart.
+__device__ __forceinline__ uint32_t bytes4_to_bits(uint32_t w) { return ((w & 0x01010101u) * 0x01020408u) >> 24; }
+__device__ __forceinline__ uint32_t bits4_to_bytes(uint32_t nib) { return (nib * 0x00204081u) & 0x01010101u; }
+
 __global__ void k_pack_frame(const uint8_t* __restrict__ src, int n, int H, size_t pitch, uint32_t* __restrict__ dst,
                              int nw, int HR, int HW, size_t wp) {
     const long long total = (long long)n * nw;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(t / nw), w = (int)(t % nw);
-        const uint8_t* p = src + (size_t)(H + i) * pitch + H + 32 * w;
+        const uint8_t* p = src + (size_t)(H + i) * pitch + H + 32 * w;  // 16-byte aligned (H, pitch)
         uint32_t v = 0u;
-        for (int b = 0; b < 32 && 32 * w + b < n; ++b) v |= (uint32_t)(p[b] & 1u) << b;
+        if (32 * w + 32 <= n) {
+            const uint4 a = *(const uint4*)p, b = *(const uint4*)(p + 16);
+            const uint32_t q[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v |= bytes4_to_bits(q[k]) << (4 * k);
+        } else {
+            for (int b = 0; 32 * w + b < n; ++b) v |= (uint32_t)(p[b] & 1u) << b;
+        }
         dst[(size_t)(HR + i) * wp + HW + w] = v;
     }
 }
@@ -199,8 +217,16 @@ __global__ void k_unpack_frame(const uint32_t* __restrict__ src, int n, int nw, 
          t += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(t / nw), w = (int)(t % nw);
         const uint32_t v = src[(size_t)(HR + i) * wp + HW + w];
-        uint8_t* p = dst + (size_t)(H + i) * pitch + H + 32 * w;
-        for (int b = 0; b < 32 && 32 * w + b < n; ++b) p[b] = (uint8_t)((v >> b) & 1u);
+        uint8_t* p = dst + (size_t)(H + i) * pitch + H + 32 * w;  // 16-byte aligned (H, pitch)
+        if (32 * w + 32 <= n) {
+            uint32_t q[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) q[k] = bits4_to_bytes((v >> (4 * k)) & 0xFu);
+            *(uint4*)p = make_uint4(q[0], q[1], q[2], q[3]);
+            *(uint4*)(p + 16) = make_uint4(q[4], q[5], q[6], q[7]);
+        } else {
+            for (int b = 0; 32 * w + b < n; ++b) p[b] = (uint8_t)((v >> b) & 1u);
+        }
     }
 }
 

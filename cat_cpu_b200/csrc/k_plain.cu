@@ -78,6 +78,13 @@ cudaError_t launch_halo_fill(const Frame& f, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 constexpr int kStripOut = 480;  // output columns per warp
 
+// Torus wrap of a row or column index that is at most one side outside [0, n).
+// With `wrap` set, the SWAR kernels read every cell from its inner position
+// (row and column taken modulo n), so the frame's halo is not read and needs
+// no refresh.  Column chunks of 16 bytes stay 16-byte aligned only if n is a
+// multiple of 16, which the host checks before it sets `wrap`.
+__device__ __forceinline__ int wrap1(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
 __device__ __forceinline__ void v_add(uint32_t (&v)[4], uint4 a) {
     v[0] += a.x; v[1] += a.y; v[2] += a.z; v[3] += a.w;
 }
@@ -172,7 +179,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template <int R>
 __global__ void __launch_bounds__(kPlainWarps * 32)
 k_plain_swar8(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n, int H, size_t pitch,
-              int band_rows, int n_strips, int n_items, RuleSwar8 q) {
+              int band_rows, int n_strips, int n_items, RuleSwar8 q, int wrap) {
     static_assert(2 * R + 2 + kAhead <= kRingRows, "ring too small");
     extern __shared__ uint4 ring_all[];
     const int lane = threadIdx.x & 31;
@@ -189,11 +196,11 @@ k_plain_swar8(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n,
         const int x = strip * kStripOut - 16 + 16 * lane;      // inner column of this lane's chunk
         const bool loads = x < n + 16;                          // chunks past that feed no output
         const bool outputs = lane >= 1 && lane <= 30 && x < n;
-        const uint8_t* col = cur + (size_t)H + (loads ? x : 0);
+        const uint8_t* col = cur + (size_t)H + (loads ? (wrap ? wrap1(x, n) : x) : 0);
         const int rlast = min(r1 - 1 + R, n - 1 + R);           // last row any window of the band needs
         auto slot = [&](int r) { return ring + (r & (kRingRows - 1)) * 32; };
         auto issue = [&](int r) {
-            if (loads && r <= rlast) cp_async16(slot(r), col + (size_t)(H + r) * pitch);
+            if (loads && r <= rlast) cp_async16(slot(r), col + (size_t)(H + (wrap ? wrap1(r, n) : r)) * pitch);
             cp_async_commit();
         };
         // rows r0-R .. r0+R start the window; kAhead more go in flight behind them
@@ -253,7 +260,7 @@ int plain_swar8_band_rows(int n, int device) {
 }
 
 template <int R>
-static cudaError_t launch_swar8_r(const Frame& cur, const Frame& nxt, const RuleSwar8& q, int band_rows,
+static cudaError_t launch_swar8_r(const Frame& cur, const Frame& nxt, const RuleSwar8& q, int band_rows, int wrap,
                                   cudaStream_t s) {
     const int n = cur.n;
     const int strips = (n + kStripOut - 1) / kStripOut;
@@ -267,7 +274,7 @@ static cudaError_t launch_swar8_r(const Frame& cur, const Frame& nxt, const Rule
     if (per_sm < 1) per_sm = 1;
     int ctas = std::min((items + kPlainWarps - 1) / kPlainWarps, sms * per_sm);
     k_plain_swar8<R><<<ctas, kPlainWarps * 32, smem, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch, band_rows,
-                                                         strips, items, q);
+                                                         strips, items, q, wrap);
     return cudaGetLastError();
 }
 
@@ -288,15 +295,19 @@ cudaError_t plain_prepare(int radius) {
     }
 }
 
-cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows,
+bool plain_wrap_supported(int n) { return n >= 64 && n % 16 == 0; }
+
+cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows, bool wrap,
                                cudaStream_t s) {
+    if (wrap && !plain_wrap_supported(cur.n)) return cudaErrorInvalidValue;
     RuleSwar8 q = make_rule_swar8(rule);
+    const int w = wrap ? 1 : 0;
     switch (rule.radius) {
-        case 1: return launch_swar8_r<1>(cur, nxt, q, band_rows, s);
-        case 2: return launch_swar8_r<2>(cur, nxt, q, band_rows, s);
-        case 3: return launch_swar8_r<3>(cur, nxt, q, band_rows, s);
-        case 4: return launch_swar8_r<4>(cur, nxt, q, band_rows, s);
-        case 5: return launch_swar8_r<5>(cur, nxt, q, band_rows, s);
+        case 1: return launch_swar8_r<1>(cur, nxt, q, band_rows, w, s);
+        case 2: return launch_swar8_r<2>(cur, nxt, q, band_rows, w, s);
+        case 3: return launch_swar8_r<3>(cur, nxt, q, band_rows, w, s);
+        case 4: return launch_swar8_r<4>(cur, nxt, q, band_rows, w, s);
+        case 5: return launch_swar8_r<5>(cur, nxt, q, band_rows, w, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -359,7 +370,7 @@ __device__ __forceinline__ uint4 swar8_row(const uint32_t (&V)[4], uint4 c, cons
 template <int R, int D>
 __global__ void __launch_bounds__(kPlainWarps * 32)
 k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n, int H, size_t pitch,
-                 int band_rows, int n_strips, int n_items, RuleSwar8 q) {
+                 int band_rows, int n_strips, int n_items, RuleSwar8 q, int wrap) {
     constexpr int kAh = tb_ahead<R>();
     constexpr int kRS = 2 * R + 2;  // rows per inner-stage ring
     static_assert(D >= 2 && D * R <= 16 && kAh >= 1, "unsupported depth");
@@ -370,7 +381,7 @@ k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int
     auto slot0 = [&](int r) { return ring0 + (r & (kTbRing - 1)) * 32; };
     // ring k >= 1 (rows of stage k), slot s in [0, kRS)
     auto slotk = [&](int k, int sl) { return ring0 + (kTbRing + (k - 1) * kRS + sl) * 32; };
-    auto wrap = [](int v) { return v >= kRS ? v - kRS : v; };
+    auto wrap_rs = [](int v) { return v >= kRS ? v - kRS : v; };
     const int gwarp = blockIdx.x * kPlainWarps + wid;
     const int gwarps = gridDim.x * kPlainWarps;
 
@@ -382,18 +393,18 @@ k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int
         const int x = strip * kStripOut - 16 + 16 * lane;
         const bool loads = x < n + 16;  // (D*R <= 16: columns >= n + 16 feed no output)
         const bool outputs = lane >= 1 && lane <= 30 && x < n;
-        const uint8_t* col = cur + (size_t)H + (loads ? x : 0);
+        const uint8_t* col = cur + (size_t)H + (loads ? (wrap ? wrap1(x, n) : x) : 0);
         const int rlast = r1 - 1 + D * R;          // last input row of the band
         const int yfirst = r0 - (D - 1) * R;        // first and last stage-1 rows
         const int ylast = r1 - 1 + (D - 1) * R;
         for (int r = yfirst - R; r <= yfirst + R + kAh; ++r) {
-            if (loads && r <= rlast) cp_async16(slot0(r), col + (size_t)(H + r) * pitch);
+            if (loads && r <= rlast) cp_async16(slot0(r), col + (size_t)(H + (wrap ? wrap1(r, n) : r)) * pitch);
             cp_async_commit();
         }
-        // next input row to request (y + R + 1 + kAh at iteration y), and the
-        // output row of stage D once it produces (y - (D-1)R)
+        // next input row to request (y + R + 1 + kAh at iteration y, never
+        // negative), and the output row of stage D once it produces (y - (D-1)R)
         int r_next = yfirst + R + 1 + kAh;
-        const uint8_t* src_next = col + (size_t)(H + r_next) * pitch;
+        const uint8_t* src_next = col + (size_t)(H + (wrap ? wrap1(r_next, n) : r_next)) * pitch;
         uint8_t* dst = nxt + (size_t)(H + r0) * pitch + H + x;
         cp_async_wait<kAh>();
         uint32_t V[D][4];
@@ -424,11 +435,11 @@ k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int
                     const int absorbed = kSteady ? 0 : (y - (k - 2) * R) - (r0 - (D - k + 1) * R) + 1;
                     v_add(V[k - 1], prod);
                     if (kSteady || absorbed > 2 * R + 1) {
-                        const uint4 out = *slotk(k - 1, wrap(sl[k - 1] + 1));
+                        const uint4 out = *slotk(k - 1, wrap_rs(sl[k - 1] + 1));
                         V[k - 1][0] -= out.x; V[k - 1][1] -= out.y; V[k - 1][2] -= out.z; V[k - 1][3] -= out.w;
                     }
                     if (kSteady || absorbed >= 2 * R + 1) {
-                        const uint4 c = *slotk(k - 1, wrap(sl[k - 1] + R + 2));
+                        const uint4 c = *slotk(k - 1, wrap_rs(sl[k - 1] + R + 2));
                         if (k < D) {
                             prod = swar8_row<R>(V[k - 1], c, q);
                             *slotk(k, sl[k]) = prod;
@@ -449,12 +460,13 @@ k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int
                 }
             }
 #pragma unroll
-            for (int k = 1; k < D; ++k) sl[k] = wrap(sl[k] + 1);
+            for (int k = 1; k < D; ++k) sl[k] = wrap_rs(sl[k] + 1);
             if (y < ylast) {
                 if (loads && r_next <= rlast) cp_async16(slot0(r_next), src_next);
                 cp_async_commit();
                 ++r_next;
                 src_next += pitch;
+                if (wrap && r_next == n) src_next -= (size_t)n * pitch;  // the next row is inner row 0
                 cp_async_wait<kAh>();  // input row y + R + 1 has landed
                 v_slide(V[0], *slot0(y + R + 1), *slot0(y - R));
             }
@@ -474,7 +486,7 @@ bool plain_tb_supported(int radius, int depth) {
 }
 
 template <int R, int D>
-static cudaError_t launch_tb_rd(const Frame& cur, const Frame& nxt, const RuleSwar8& q, int band_rows,
+static cudaError_t launch_tb_rd(const Frame& cur, const Frame& nxt, const RuleSwar8& q, int band_rows, int wrap,
                                 cudaStream_t s) {
     const int n = cur.n;
     const int strips = (n + kStripOut - 1) / kStripOut;
@@ -488,7 +500,7 @@ static cudaError_t launch_tb_rd(const Frame& cur, const Frame& nxt, const RuleSw
     if (per_sm < 1) per_sm = 1;
     int ctas = std::min((items + kPlainWarps - 1) / kPlainWarps, sms * per_sm);
     k_plain_swar8_tb<R, D><<<ctas, kPlainWarps * 32, smem, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch,
-                                                               band_rows, strips, items, q);
+                                                               band_rows, strips, items, q, wrap);
     return cudaGetLastError();
 }
 
@@ -504,10 +516,10 @@ static cudaError_t prepare_tb_rd() {
 
 template <int R>
 static cudaError_t launch_tb_r(const Frame& cur, const Frame& nxt, const RuleSwar8& q, int band_rows, int depth,
-                               cudaStream_t s) {
-    if (depth == 2) return launch_tb_rd<R, 2>(cur, nxt, q, band_rows, s);
+                               int wrap, cudaStream_t s) {
+    if (depth == 2) return launch_tb_rd<R, 2>(cur, nxt, q, band_rows, wrap, s);
     if constexpr (3 * R <= 16) {
-        if (depth == 3) return launch_tb_rd<R, 3>(cur, nxt, q, band_rows, s);
+        if (depth == 3) return launch_tb_rd<R, 3>(cur, nxt, q, band_rows, wrap, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -525,152 +537,151 @@ cudaError_t plain_tb_prepare(int radius) {
 }
 
 cudaError_t launch_plain_tb(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows, int depth,
-                            cudaStream_t s) {
+                            bool wrap, cudaStream_t s) {
     if (!plain_tb_supported(rule.radius, depth) || cur.H < depth * rule.radius) return cudaErrorInvalidValue;
+    if (wrap && !plain_wrap_supported(cur.n)) return cudaErrorInvalidValue;
     RuleSwar8 q = make_rule_swar8(rule);
+    const int w = wrap ? 1 : 0;
     switch (rule.radius) {
-        case 1: return launch_tb_r<1>(cur, nxt, q, band_rows, depth, s);
-        case 2: return launch_tb_r<2>(cur, nxt, q, band_rows, depth, s);
-        case 3: return launch_tb_r<3>(cur, nxt, q, band_rows, depth, s);
-        case 4: return launch_tb_r<4>(cur, nxt, q, band_rows, depth, s);
-        case 5: return launch_tb_r<5>(cur, nxt, q, band_rows, depth, s);
+        case 1: return launch_tb_r<1>(cur, nxt, q, band_rows, depth, w, s);
+        case 2: return launch_tb_r<2>(cur, nxt, q, band_rows, depth, w, s);
+        case 3: return launch_tb_r<3>(cur, nxt, q, band_rows, depth, w, s);
+        case 4: return launch_tb_r<4>(cur, nxt, q, band_rows, depth, w, s);
+        case 5: return launch_tb_r<5>(cur, nxt, q, band_rows, depth, w, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 // ---------------------------------------------------------------------------
-// K1 generic path (any R >= 1), two passes:
-//  (a) k_vsum: V[r][c] = sum_{dy=-R..R} X[r+dy][c] for every frame column c,
-//      as uint16 (two cells per 32-bit register, SWAR), one thread per 4
-//      columns sliding down a band of rows;
-//  (b) k_hsum_rule: per row, an exclusive prefix of V over the window
-//      [H+j0-R, H+j0+T+R) in shared memory, B = P[q+2R+1] - P[q], k = B - s,
-//      interval rule, one output byte per cell.
-// Work per cell is independent of R.
+// K1 generic path (any R >= 1): one fused kernel, work per cell independent of R.
+//
+// A CTA of 256 threads owns a tile of T output columns [j0, j0 + T) and a band
+// of rows.  Its window columns are [c0, c0 + 1024K), c0 = j0 - R rounded down
+// to a multiple of 4; thread t owns the 4K consecutive columns starting at
+// c0 + 4Kt and keeps their vertical window sums V (2R+1 rows) in registers as
+// 16-bit SWAR lanes, sliding them down one row at a time (V += X(r+R+1) -
+// X(r-R)).  For every row the CTA scans V into prefix sums P in shared memory
+// (local sums, a warp scan, the warp totals), and each output reads
+//   B(j) = P[j - c0 + R + 1] - P[j - c0 - R],   k = B - centre,
+// then applies the interval rule.  P is double-buffered, so two barriers per
+// row suffice.  This replaces a two-kernel version that wrote V to HBM.
 // ---------------------------------------------------------------------------
-constexpr int kVBand = 128;
+constexpr int kWideThreads = 256;
 
-__global__ void k_vsum(const uint8_t* __restrict__ X, uint16_t* __restrict__ V, int n, int H, size_t pitch,
-                       int R, int nwords) {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    const int r0 = blockIdx.y * kVBand;
-    if (w >= nwords || r0 >= n) return;
-    const int r1 = min(r0 + kVBand, n);
-    const uint8_t* col = X + 4 * (size_t)w;
-    auto ldw = [&](int r) { return __ldg((const uint32_t*)(col + (size_t)(H + r) * pitch)); };
-    uint32_t lo = 0, hi = 0;
-    for (int dy = -R; dy <= R; ++dy) {
-        uint32_t x = ldw(r0 + dy);
-        lo += __byte_perm(x, 0, 0x4140);
-        hi += __byte_perm(x, 0, 0x4342);
-    }
-    uint16_t* out = V + 4 * (size_t)w;
-    for (int r = r0; r < r1; ++r) {
-        *(uint2*)(out + (size_t)r * pitch) = make_uint2(lo, hi);
-        if (r + 1 < r1) {
-            uint32_t a = ldw(r + R + 1), b = ldw(r - R);
-            lo += __byte_perm(a, 0, 0x4140) - __byte_perm(b, 0, 0x4140);
-            hi += __byte_perm(a, 0, 0x4342) - __byte_perm(b, 0, 0x4342);
-        }
-    }
-}
-
-constexpr int kHT = 1024;      // output columns per CTA row segment
-constexpr int kHThreads = 256;
-constexpr int kHRows = 4;      // rows per CTA
-
-__global__ void __launch_bounds__(kHThreads)
-k_hsum_rule(const uint8_t* __restrict__ X, const uint16_t* __restrict__ V, uint8_t* __restrict__ Y, int n,
-            int H, size_t pitch, Rule rule) {
-    extern __shared__ int P[];  // L + 1 entries, L = kHT + 2R
-    __shared__ int warp_tot[kHThreads / 32];
+template <int K>
+__global__ void __launch_bounds__(kWideThreads)
+k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int H, size_t pitch, int band_rows,
+             int T, Rule rule) {
+    constexpr int L = 1024 * K;  // window columns per CTA
+    __shared__ int P[2][L + 1];
+    __shared__ int wsum[kWideThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     const int R = rule.radius;
-    const int j0 = blockIdx.x * kHT;
-    const int L = kHT + 2 * R;
-    const int per = (L + kHThreads - 1) / kHThreads;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int s1 = H + j0 - R;  // frame column of P index 0
+    const int j0 = blockIdx.x * T;
+    const int r0 = blockIdx.y * band_rows;
+    const int r1 = min(r0 + band_rows, n);
+    const int c0 = (j0 - R) & ~3;                  // floor to a multiple of 4 (two's complement)
+    const int cstart = c0 + 4 * K * t;             // inner column of this thread's first window column
+    const bool need = cstart <= n - 1 + R;         // later columns feed no output (and may lie past the row)
+    const uint8_t* col = X + (size_t)H + cstart;   // 4-byte aligned: H, pitch and cstart are multiples of 4
+    auto ldw = [&](int r, int k) { return __ldg((const uint32_t*)(col + (size_t)(H + r) * pitch) + k); };
 
-    for (int rr = 0; rr < kHRows; ++rr) {
-        const int r = blockIdx.y * kHRows + rr;
-        if (r >= n) break;
-        const uint16_t* vrow = V + (size_t)r * pitch;
-        // thread-local sequential sums over [tid*per, tid*per+per)
-        int a0 = tid * per;
-        int local = 0;
-        for (int u = 0; u < per; ++u) {
-            int t = a0 + u;
-            if (t < L) {
-                int c = s1 + t;
-                local += (c < (int)pitch) ? vrow[c] : 0;
+    uint32_t V[2 * K];  // V[2k]: columns 4k, 4k+1; V[2k+1]: columns 4k+2, 4k+3 (16-bit lanes)
+#pragma unroll
+    for (int k = 0; k < 2 * K; ++k) V[k] = 0u;
+    if (need) {
+        for (int dy = -R; dy <= R; ++dy) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const uint32_t x = ldw(r0 + dy, k);
+                V[2 * k] += __byte_perm(x, 0, 0x4140);
+                V[2 * k + 1] += __byte_perm(x, 0, 0x4342);
             }
         }
-        // block exclusive scan of `local`
-        int incl = local;
+    }
+    for (int r = r0; r < r1; ++r) {
+        int* Pr = P[r & 1];
+        // this thread's values and their local sum
+        int v[4 * K];
+#pragma unroll
+        for (int k = 0; k < 2 * K; ++k) {
+            v[2 * k] = (int)(V[k] & 0xffffu);
+            v[2 * k + 1] = (int)(V[k] >> 16);
+        }
+        int sum = 0;
+#pragma unroll
+        for (int i = 0; i < 4 * K; ++i) sum += v[i];
+        int incl = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, incl, o);
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
         }
-        if (lane == 31) warp_tot[wid] = incl;
+        if (lane == 31) wsum[wid] = incl;
         __syncthreads();
-        int wpre = 0;
-        for (int k = 0; k < wid; ++k) wpre += warp_tot[k];
-        int run = wpre + incl - local;  // exclusive prefix at a0
-        for (int u = 0; u < per; ++u) {
-            int t = a0 + u;
-            if (t < L) {
-                P[t] = run;
-                int c = s1 + t;
-                run += (c < (int)pitch) ? vrow[c] : 0;
-            }
+        int run = incl - sum;
+#pragma unroll
+        for (int w = 0; w < kWideThreads / 32; ++w)
+            if (w < wid) run += wsum[w];
+#pragma unroll
+        for (int i = 0; i < 4 * K; ++i) {
+            Pr[4 * K * t + i] = run;
+            run += v[i];
         }
-        if (tid == kHThreads - 1) P[L] = run;  // last thread's running total is the grand total
+        if (t == kWideThreads - 1) Pr[L] = run;
         __syncthreads();
-        // outputs: 4 cells per thread
-        for (int q0 = tid * 4; q0 < kHT; q0 += kHThreads * 4) {
-            int j = j0 + q0;
+        // outputs: 4 consecutive cells per thread per pass
+        for (int q = 4 * t; q < T; q += 4 * kWideThreads) {
+            const int j = j0 + q;
             if (j >= n) break;
-            const uint8_t* xr = X + (size_t)(H + r) * pitch + H + j;
-            uint32_t sw = *(const uint32_t*)xr;
+            const uint32_t sw = __ldg((const uint32_t*)(X + (size_t)(H + r) * pitch + H + j));
+            const int base = j - c0;
             uint32_t ow = 0;
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                int q = q0 + u;
-                int B = P[q + 2 * R + 1] - P[q];
-                int sv = (sw >> (8 * u)) & 0xff;
-                int nv = rule_scalar(B - sv, sv, rule.smin, rule.smax, rule.bmin, rule.bmax);
-                ow |= (uint32_t)nv << (8 * u);
+                const int B = Pr[base + u + R + 1] - Pr[base + u - R];
+                const int sv = (sw >> (8 * u)) & 1;
+                ow |= (uint32_t)rule_scalar(B - sv, sv, rule.smin, rule.smax, rule.bmin, rule.bmax) << (8 * u);
             }
             uint8_t* yr = Y + (size_t)(H + r) * pitch + H + j;
             if (j + 4 <= n) {
                 *(uint32_t*)yr = ow;
             } else {
-                for (int u = 0; u < n - j; ++u) yr[u] = (uint8_t)((ow >> (8 * u)) & 0xff);
+                for (int u = 0; u < n - j; ++u) yr[u] = (uint8_t)((ow >> (8 * u)) & 0xffu);
             }
         }
-        __syncthreads();
+        if (r + 1 < r1 && need) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const uint32_t a = ldw(r + R + 1, k), b = ldw(r - R, k);
+                V[2 * k] += __byte_perm(a, 0, 0x4140) - __byte_perm(b, 0, 0x4140);
+                V[2 * k + 1] += __byte_perm(a, 0, 0x4342) - __byte_perm(b, 0, 0x4342);
+            }
+        }
     }
 }
 
-size_t plain_generic_vbuf_bytes(int n, size_t pitch) { return (size_t)n * pitch * sizeof(uint16_t); }
+size_t plain_generic_vbuf_bytes(int, size_t) { return 0; }  // the fused kernel needs no column-sum buffer
 
-cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, uint16_t* vbuf,
+cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, uint16_t* /*vbuf*/,
                                  cudaStream_t s) {
-    const int n = cur.n;
-    const int nwords = (int)(cur.pitch / 4);
-    dim3 gv((nwords + 127) / 128, (n + kVBand - 1) / kVBand);
-    k_vsum<<<gv, 128, 0, s>>>(cur.base, vbuf, n, cur.H, cur.pitch, rule.radius, nwords);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    const int L = kHT + 2 * rule.radius;
-    size_t smem = (size_t)(L + 1) * sizeof(int);
-    if (smem > 48 * 1024) {
-        e = cudaFuncSetAttribute(k_hsum_rule, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
+    const int n = cur.n, R = rule.radius;
+    if (cur.H < ((R + 3) & ~3) || (cur.H & 3) || (cur.pitch & 3)) return cudaErrorInvalidValue;
+    // T: outputs per tile, so that [j0 - R, j0 + T + R] (plus the rounding of c0)
+    // fits the window columns; bands long enough to amortise the 2R+1-row start
+    const int band = std::max(64, std::min(512, 4 * (2 * R + 1)));
+    const dim3 block(kWideThreads);
+    if (1024 - 2 * R - 3 >= 256) {
+        const int T = (1024 - 2 * R - 3) & ~3;
+        k_plain_wide<1><<<dim3((n + T - 1) / T, (n + band - 1) / band), block, 0, s>>>(
+            cur.base, nxt.base, n, cur.H, cur.pitch, band, T, rule);
+    } else if (2048 - 2 * R - 3 >= 256) {
+        const int T = (2048 - 2 * R - 3) & ~3;
+        k_plain_wide<2><<<dim3((n + T - 1) / T, (n + band - 1) / band), block, 0, s>>>(
+            cur.base, nxt.base, n, cur.H, cur.pitch, band, T, rule);
+    } else {
+        return cudaErrorInvalidValue;  // R > 893
     }
-    dim3 gh((n + kHT - 1) / kHT, (n + kHRows - 1) / kHRows);
-    k_hsum_rule<<<gh, kHThreads, smem, s>>>(cur.base, vbuf, nxt.base, n, cur.H, cur.pitch, rule);
     return cudaGetLastError();
 }
 

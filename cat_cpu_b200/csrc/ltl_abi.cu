@@ -53,6 +53,7 @@ struct ltl_ctx {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     int band_rows = 64;         // plain: rows per work item
+    bool plain_wrap = false;    // plain R <= 5: kernels apply the torus wrap, no halo refresh
     int packed_band_rows = 0;   // packed: rows per work item (0: heuristic)
     // packed variant
     PackedFrame pa{}, pb{};
@@ -194,7 +195,7 @@ extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin
     c->fa = Frame{c->frames, n, H, pitch};
     c->fb = Frame{c->frames + one, n, H, pitch};
 
-    if (variant == LTL_VARIANT_PLAIN && !plain_swar8_supported(radius)) {
+    if (variant == LTL_VARIANT_PLAIN && !plain_swar8_supported(radius) && plain_generic_vbuf_bytes(n, pitch) > 0) {
         c->vbuf_bytes = plain_generic_vbuf_bytes(n, pitch);
         e = cudaMalloc(&c->vbuf, c->vbuf_bytes);
         if (e != cudaSuccess) {
@@ -209,6 +210,7 @@ extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin
         const int want = (int)tuning_lookup("plain", radius, n, "depth", n >= 256 ? 2 : 1);
         if (want > 1 && plain_tb_supported(radius, want) && H >= want * radius) depth = want;
         c->band_rows = (int)tuning_lookup("plain", radius, n, "band_rows", plain_swar8_band_rows(n, device));
+        c->plain_wrap = plain_wrap_supported(n);
     }
     if (variant == LTL_VARIANT_PACKED) c->packed_band_rows = (int)tuning_lookup("packed", radius, n, "band_rows", 0);
     if (variant == LTL_VARIANT_PLAIN) e = plain_prepare(radius);
@@ -407,17 +409,20 @@ static cudaError_t enqueue_pass(ltl_ctx* c, int gens) {
             Frame& a = cur_frame(c);
             Frame& b = nxt_frame(c);
             if (gens > 1) {
-                e = launch_plain_tb(a, b, c->rule, c->band_rows, gens, c->stream);
+                e = launch_plain_tb(a, b, c->rule, c->band_rows, gens, c->plain_wrap, c->stream);
                 step_kernels = 1;
             } else if (plain_swar8_supported(c->rule.radius)) {
-                e = launch_plain_swar8(a, b, c->rule, c->band_rows, c->stream);
+                e = launch_plain_swar8(a, b, c->rule, c->band_rows, c->plain_wrap, c->stream);
                 step_kernels = 1;
             } else {
                 e = launch_plain_generic(a, b, c->rule, c->vbuf, c->stream);
                 step_kernels = 2;
             }
             if (c->timing && e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
-            if (e == cudaSuccess) e = launch_halo_fill(b, c->stream);
+            // the SWAR kernels with plain_wrap read inner cells only: no halo to refresh
+            const bool wrapped = c->plain_wrap && plain_swar8_supported(c->rule.radius);
+            if (wrapped) halo_kernels = 0;
+            else if (e == cudaSuccess) e = launch_halo_fill(b, c->stream);
             break;
         }
         case LTL_VARIANT_PACKED: {
@@ -579,11 +584,12 @@ extern "C" int ltl_set_param(ltl_ctx* c, const char* name, long long value) {
         return LTL_EINVAL;
     }
     if (std::strcmp(name, "band_rows") == 0) {
-        if (value < 16 || value > 4096) {
-            ltl_set_error("ltl_set_param: band_rows must be in [16, 4096]");
+        if (value != 0 && (value < 16 || value > 4096)) {
+            ltl_set_error("ltl_set_param: band_rows must be 0 (built-in choice) or in [16, 4096]");
             return LTL_EINVAL;
         }
-        if (c->variant == LTL_VARIANT_PLAIN) c->band_rows = (int)value;
+        if (c->variant == LTL_VARIANT_PLAIN)
+            c->band_rows = value ? (int)value : plain_swar8_band_rows(c->n, c->device);
         else if (c->variant == LTL_VARIANT_PACKED) c->packed_band_rows = (int)value;
         else {
             ltl_set_error("ltl_set_param: band_rows applies to the plain and packed variants");

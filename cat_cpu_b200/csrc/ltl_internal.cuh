@@ -49,37 +49,41 @@ struct Rule {
 // B <= 127: alive cell survives iff slo <= B <= shi (slo = smin+1, shi = smax+1,
 // since k = B - 1), dead cell is born iff blo <= B <= bhi.  Empty intervals are
 // encoded lo = 128, hi = 0; lo is clamped to [0,128], hi to [0,127].  Each value
-// is broadcast to the four byte lanes; `hi*` carry the 0x80 marker bit already.
+// is broadcast to the four byte lanes, lo as 0x80 - lo (so that B + (0x80 - lo)
+// has bit 7 set iff B >= lo, without a carry into the next lane) and hi with
+// the 0x80 marker bit (0x80 + hi - B has bit 7 set iff B <= hi).  `d*` hold the
+// XOR of the dead and live values, for a one-operation select by the centre.
 struct RuleSwar8 {
-    uint32_t lo0, lo1, hiH0, hiH1;  // 0 = dead-cell (birth) interval, 1 = live-cell (survival)
+    uint32_t nlo0, hiH0;  // dead cell (birth interval)
+    uint32_t dnlo, dhiH;  // XOR of the dead- and live-cell (survival) values
 };
 
-inline void clamp_interval8(int lo, int hi, uint32_t& lo_out, uint32_t& hi_out) {
+inline void clamp_interval8(int lo, int hi, uint32_t& nlo_out, uint32_t& hi_out) {
     if (lo < 0) lo = 0;
     if (hi > 127) hi = 127;
     if (hi < lo || lo > 127) {
         lo = 128;
         hi = 0;
     }
-    lo_out = (uint32_t)lo * 0x01010101u;
+    nlo_out = (uint32_t)(0x80 - lo) * 0x01010101u;
     hi_out = ((uint32_t)hi | 0x80u) * 0x01010101u;
 }
 
 inline RuleSwar8 make_rule_swar8(const Rule& r) {
-    RuleSwar8 q;
-    clamp_interval8(r.bmin, r.bmax, q.lo0, q.hiH0);
-    clamp_interval8(r.smin + 1, r.smax + 1, q.lo1, q.hiH1);
-    return q;
+    uint32_t nlo0, hi0, nlo1, hi1;
+    clamp_interval8(r.bmin, r.bmax, nlo0, hi0);
+    clamp_interval8(r.smin + 1, r.smax + 1, nlo1, hi1);
+    return RuleSwar8{nlo0, hi0, nlo0 ^ nlo1, hi0 ^ hi1};
 }
 
 // Per byte lane: 1 if the lane's cell is alive in the next generation.
 // B: four box counts (centre included, each <= 127); s: four centre cells (0/1).
 __device__ __forceinline__ uint32_t rule_swar8(uint32_t B, uint32_t s, const RuleSwar8& q) {
-    uint32_t m = s * 0xFFu;                                  // 0x00 / 0xFF per lane
-    uint32_t lo = q.lo0 ^ (m & (q.lo0 ^ q.lo1));
-    uint32_t hiH = q.hiH0 ^ (m & (q.hiH0 ^ q.hiH1));
-    uint32_t ge = (B | 0x80808080u) - lo;                    // bit 7 set iff B >= lo
-    uint32_t le = hiH - B;                                   // bit 7 set iff hi >= B
+    const uint32_t m = s * 0xFFu;                     // 0x00 / 0xFF per lane
+    const uint32_t nlo = q.nlo0 ^ (m & q.dnlo);
+    const uint32_t hiH = q.hiH0 ^ (m & q.dhiH);
+    const uint32_t ge = B + nlo;                      // bit 7 set iff B >= lo
+    const uint32_t le = hiH - B;                      // bit 7 set iff hi >= B
     return ((ge & le) >> 7) & 0x01010101u;
 }
 

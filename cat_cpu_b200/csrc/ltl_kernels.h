@@ -18,7 +18,10 @@ bool plain_swar8_supported(int radius);
 // captured in CUDA graphs without configuration calls.
 cudaError_t plain_prepare(int radius);
 cudaError_t packed_prepare(int radius);
-cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows,
+// wrap: read every cell from its inner position (torus wrap inside the kernel),
+// so the frame halo is neither read nor needed; requires plain_wrap_supported(n).
+bool plain_wrap_supported(int n);
+cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows, bool wrap,
                                cudaStream_t s);
 int plain_swar8_band_rows(int n, int device);
 // Temporally blocked SWAR step: `depth` (2 or 3, depth * R <= 16) generations per
@@ -26,7 +29,7 @@ int plain_swar8_band_rows(int n, int device);
 bool plain_tb_supported(int radius, int depth);
 cudaError_t plain_tb_prepare(int radius);
 cudaError_t launch_plain_tb(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows, int depth,
-                            cudaStream_t s);
+                            bool wrap, cudaStream_t s);
 
 // K1 generic path (any R): vertical sliding sums into `vbuf` (uint16, n rows x
 // pitch entries), then a prefix-sum horizontal pass with the rule fused.

@@ -163,7 +163,8 @@ int ltl_batch_info(const ltl_batch* b, long long* cells, long long* device_bytes
 
 /* Shape parameters (what cat_cpu_b200/autotune.py sweeps; the autotuned table
  * tuning/ltl_tuning.txt next to the library sets them at ltl_create):
- *   "band_rows"  rows per work item of the plain and packed step kernels;
+ *   "band_rows"  rows per work item of the plain and packed step kernels
+ *                (0: the built-in choice);
  *   "depth"      generations per pass of the plain variant: 1, or 2..3 with
  *                depth * R <= 16 and R <= 5 (temporal blocking: one read and
  *                one write of the grid per pass).  ltl_step accepts any step

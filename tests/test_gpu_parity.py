@@ -146,6 +146,31 @@ def test_plain_temporal_depths_vs_oracle():
                     s.close()
 
 
+def test_packed_band_rows_and_strip_edges_vs_oracle():
+    """Bit-packed step with the built-in band choice (0) and explicit bands, on
+    sides whose word count is a multiple of 32 (the last strip ends at the last
+    inner word, whose right neighbour is the halo word) and sides that leave a
+    partial last word or a lone halo lane in the last strip."""
+    rng = np.random.default_rng(31)
+    for n in (1024, 1000, 1056, 2048 + 32, 97):
+        for band in (0, 16, 37, 4096):
+            r = int(rng.choice([1, 3, 5, 8, 13]))
+            N = (2 * r + 1) ** 2
+            lo = int(rng.integers(0, N // 3))
+            rule = (lo, lo + int(rng.integers(1, N // 2)), int(rng.integers(0, N // 3)), int(rng.integers(N // 3, N)))
+            g = (rng.random((n, n)) < rng.uniform(0.25, 0.6)).astype(np.uint8)
+            s = make("packed", n, r, rule)
+            try:
+                s.set_param("band_rows", band)
+                s.setState(g)
+                s.doSteps(3)
+                want = O.run(g, r, rule, 3)
+                got = s.getCurrentState()
+                assert np.array_equal(got, want), f"n={n} R={r} band={band}: " + describe_mismatch(got, want)
+            finally:
+                s.close()
+
+
 def test_plain_default_depth_and_limits():
     s = make("plain", 1024, 5, O.BOSCO_R5)
     try:
