@@ -601,6 +601,19 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
     }
     for (int r = r0; r < r1; ++r) {
         int* Pr = P[r & 1];
+        // issue this row's global loads first (the next row's entering and
+        // leaving window rows, the first output chunk's centre cells), so that
+        // their latency hides behind the scan
+        const bool slide = r + 1 < r1 && need;
+        uint32_t xa[K], xb[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            xa[k] = slide ? ldw(r + R + 1, k) : 0u;
+            xb[k] = slide ? ldw(r - R, k) : 0u;
+        }
+        const int q0 = 4 * t;
+        const bool out0 = q0 < T && j0 + q0 < n;
+        const uint32_t sw0 = out0 ? __ldg((const uint32_t*)(X + (size_t)(H + r) * pitch + H + j0 + q0)) : 0u;
         // this thread's values and their local sum
         int v[4 * K];
 #pragma unroll
@@ -631,10 +644,10 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
         if (t == kWideThreads - 1) Pr[L] = run;
         __syncthreads();
         // outputs: 4 consecutive cells per thread per pass
-        for (int q = 4 * t; q < T; q += 4 * kWideThreads) {
+        for (int q = q0; q < T; q += 4 * kWideThreads) {
             const int j = j0 + q;
             if (j >= n) break;
-            const uint32_t sw = __ldg((const uint32_t*)(X + (size_t)(H + r) * pitch + H + j));
+            const uint32_t sw = q == q0 ? sw0 : __ldg((const uint32_t*)(X + (size_t)(H + r) * pitch + H + j));
             const int base = j - c0;
             uint32_t ow = 0;
 #pragma unroll
@@ -650,12 +663,11 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
                 for (int u = 0; u < n - j; ++u) yr[u] = (uint8_t)((ow >> (8 * u)) & 0xffu);
             }
         }
-        if (r + 1 < r1 && need) {
+        if (slide) {
 #pragma unroll
             for (int k = 0; k < K; ++k) {
-                const uint32_t a = ldw(r + R + 1, k), b = ldw(r - R, k);
-                V[2 * k] += __byte_perm(a, 0, 0x4140) - __byte_perm(b, 0, 0x4140);
-                V[2 * k + 1] += __byte_perm(a, 0, 0x4342) - __byte_perm(b, 0, 0x4342);
+                V[2 * k] += __byte_perm(xa[k], 0, 0x4140) - __byte_perm(xb[k], 0, 0x4140);
+                V[2 * k + 1] += __byte_perm(xa[k], 0, 0x4342) - __byte_perm(xb[k], 0, 0x4342);
             }
         }
     }
@@ -669,19 +681,21 @@ cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule&
     if (cur.H < ((R + 3) & ~3) || (cur.H & 3) || (cur.pitch & 3)) return cudaErrorInvalidValue;
     // T: outputs per tile, so that [j0 - R, j0 + T + R] (plus the rounding of c0)
     // fits the window columns; bands long enough to amortise the 2R+1-row start
-    const int band = std::max(64, std::min(512, 4 * (2 * R + 1)));
-    const dim3 block(kWideThreads);
-    if (1024 - 2 * R - 3 >= 256) {
-        const int T = (1024 - 2 * R - 3) & ~3;
-        k_plain_wide<1><<<dim3((n + T - 1) / T, (n + band - 1) / band), block, 0, s>>>(
-            cur.base, nxt.base, n, cur.H, cur.pitch, band, T, rule);
-    } else if (2048 - 2 * R - 3 >= 256) {
-        const int T = (2048 - 2 * R - 3) & ~3;
-        k_plain_wide<2><<<dim3((n + T - 1) / T, (n + band - 1) / band), block, 0, s>>>(
-            cur.base, nxt.base, n, cur.H, cur.pitch, band, T, rule);
-    } else {
-        return cudaErrorInvalidValue;  // R > 893
-    }
+    // (and short enough that tiles x bands keep about 6 CTAs per SM busy)
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int K = (1024 - 2 * R - 3 >= 256) ? 1 : 2;
+    if (2048 - 2 * R - 3 < 256) return cudaErrorInvalidValue;  // R > 893
+    const int T = (1024 * K - 2 * R - 3) & ~3;
+    const int tiles = (n + T - 1) / T;
+    const int want_bands = std::max(1, (6 * sms + tiles - 1) / tiles);
+    const int band = std::max(32, std::min({512, 4 * (2 * R + 1), (n + want_bands - 1) / want_bands}));
+    const dim3 grid(tiles, (n + band - 1) / band), block(kWideThreads);
+    if (K == 1)
+        k_plain_wide<1><<<grid, block, 0, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch, band, T, rule);
+    else
+        k_plain_wide<2><<<grid, block, 0, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch, band, T, rule);
     return cudaGetLastError();
 }
 
