@@ -623,9 +623,12 @@ static uint32_t* nxt_arena(ltl_batch* b) { return b->arena[b->cur_is_a ? 1 : 0];
 
 static cudaError_t refresh_streamed_halo(ltl_batch* b, uint32_t* arena, cudaStream_t s) {
     if (b->n_streamed_all == 0) return cudaSuccess;
-    dim3 g1(8, (unsigned)b->n_streamed_all);
-    k_batch_halo_cols<<<g1, 128, 0, s>>>(arena, b->d_grids, b->d_streamed_all);
-    k_batch_halo_rows<<<g1, 128, 0, s>>>(arena, b->d_grids, b->d_streamed_all);
+    // one block row per grid; launches of at most 65535 grids (the grid-y limit)
+    for (int first = 0; first < b->n_streamed_all; first += 65535) {
+        dim3 g1(8, (unsigned)std::min(65535, b->n_streamed_all - first));
+        k_batch_halo_cols<<<g1, 128, 0, s>>>(arena, b->d_grids, b->d_streamed_all + first);
+        k_batch_halo_rows<<<g1, 128, 0, s>>>(arena, b->d_grids, b->d_streamed_all + first);
+    }
     return cudaGetLastError();
 }
 

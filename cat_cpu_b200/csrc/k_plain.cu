@@ -632,10 +632,15 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
         }
         if (lane == 31) wsum[wid] = incl;
         __syncthreads();
-        int run = incl - sum;
+        // exclusive prefix of the 8 warp totals, scanned by each warp's first lanes
+        int wt = lane < kWideThreads / 32 ? wsum[lane] : 0;
 #pragma unroll
-        for (int w = 0; w < kWideThreads / 32; ++w)
-            if (w < wid) run += wsum[w];
+        for (int o = 1; o < kWideThreads / 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, wt, o);
+            if (lane >= o) wt += y;
+        }
+        const int wpre = __shfl_sync(0xffffffffu, wt, (wid + 31) & 31);  // inclusive total of warps < wid
+        int run = incl - sum + (wid > 0 ? wpre : 0);
 #pragma unroll
         for (int i = 0; i < 4 * K; ++i) {
             Pr[4 * K * t + i] = run;
@@ -654,7 +659,12 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
             for (int u = 0; u < 4; ++u) {
                 const int B = Pr[base + u + R + 1] - Pr[base + u - R];
                 const int sv = (sw >> (8 * u)) & 1;
-                ow |= (uint32_t)rule_scalar(B - sv, sv, rule.smin, rule.smax, rule.bmin, rule.bmax) << (8 * u);
+                // k in [lo, hi]  <=>  (unsigned)(k - lo) <= (unsigned)(hi - lo); an empty
+                // interval (hi < lo) has a negative width that no k passes as unsigned
+                const int lo = sv ? rule.smin : rule.bmin;
+                const int wdt = sv ? rule.smax - rule.smin : rule.bmax - rule.bmin;
+                const uint32_t in = wdt >= 0 && (uint32_t)(B - sv - lo) <= (uint32_t)wdt;
+                ow |= in << (8 * u);
             }
             uint8_t* yr = Y + (size_t)(H + r) * pitch + H + j;
             if (j + 4 <= n) {
