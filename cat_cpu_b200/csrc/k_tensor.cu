@@ -121,28 +121,30 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
-// 16 consecutive TMEM columns of this thread's lane (32-bit each).  The
-// registers are defined only after tmem_wait16 on the same array: the wait
-// takes them as read-write operands so that the compiler cannot move a use of
-// them above it.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-        : "r"(taddr));
+// 16 consecutive TMEM columns of this thread's lane, packed in pairs
+// (.pack::16b): register k holds the low 16 bits of column 2k in its low half
+// and those of column 2k + 1 in its high half.  Every accumulator read here
+// fits 16 bits: row sums are <= 2R + 1 and box counts <= (2R + 1)^2 < 2^16 for
+// R <= 32.  The registers are defined only after tmem_wait8 on the same array:
+// the wait takes them as read-write operands so that the compiler cannot move
+// a use of them above it.
+__device__ __forceinline__ void tmem_ld16p(uint32_t taddr, uint32_t (&v)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.pack::16b.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
 }
 
 // Waits for every tcgen05.ld this thread issued.
-__device__ __forceinline__ void tmem_wait16(uint32_t (&v)[16]) {
+__device__ __forceinline__ void tmem_wait8(uint32_t (&v)[8]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;"
-                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
-                   "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
-                   "+r"(v[15])
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7])
                  :
                  : "memory");
 }
+
+// Bytes 0 and 2 of a and of b: the low bytes of the four 16-bit values of two
+// packed registers, in column order.
+__device__ __forceinline__ uint32_t low_bytes4(uint32_t a, uint32_t b) { return __byte_perm(a, b, 0x6420); }
 
 // Walks this warp's 16-column chunks of a TMEM accumulator row, loading chunk
 // c + 1 while f(values, column) processes chunk c.  The chunks are the halves
@@ -155,21 +157,21 @@ __device__ __forceinline__ void tmem_walk16(uint32_t trow, int grp, int groups, 
     const int nc = 2 * blocks < max_chunks ? 2 * blocks : max_chunks;
     auto col = [&](int c) { return 32 * (grp + groups * (c >> 1)) + 16 * (c & 1); };
     if (nc == 0) return;
-    uint32_t a[16], b[16];
-    tmem_ld16(trow + col(0), a);
-    tmem_wait16(a);
+    uint32_t a[8], b[8];
+    tmem_ld16p(trow + col(0), a);
+    tmem_wait8(a);
 #pragma unroll
     for (int c = 0; c < max_chunks; ++c) {
         if (c < nc) {
             const bool more = c + 1 < nc;
             if ((c & 1) == 0) {
-                if (more) tmem_ld16(trow + col(c + 1), b);
+                if (more) tmem_ld16p(trow + col(c + 1), b);
                 f(a, col(c));
-                if (more) tmem_wait16(b);
+                if (more) tmem_wait8(b);
             } else {
-                if (more) tmem_ld16(trow + col(c + 1), a);
+                if (more) tmem_ld16p(trow + col(c + 1), a);
                 f(b, col(c));
-                if (more) tmem_wait16(a);
+                if (more) tmem_wait8(a);
             }
         }
     }
@@ -270,12 +272,6 @@ __host__ __device__ inline SmemLayout smem_layout(int Tc, int K1c) {
     o += 16;
     L.total = o;
     return L;
-}
-
-__device__ __forceinline__ uint32_t pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-    uint32_t lo = __byte_perm(a, b, 0x0040);
-    uint32_t hi = __byte_perm(c, d, 0x0040);
-    return __byte_perm(lo, hi, 0x5410);
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -432,12 +428,12 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             tc_fence_after();
             uint8_t* hsb = hs + (j & 1) * 128 * Tc;
             tmem_walk16<kMaxChunks>(tmem + kHCol + lane_off, grp, kEpiGroups, Tc,
-                                    [&](const uint32_t (&v)[16], int col) {
+                                    [&](const uint32_t (&v)[8], int col) {
                                         uint4 w;
-                                        w.x = pack4(v[0], v[1], v[2], v[3]);
-                                        w.y = pack4(v[4], v[5], v[6], v[7]);
-                                        w.z = pack4(v[8], v[9], v[10], v[11]);
-                                        w.w = pack4(v[12], v[13], v[14], v[15]);
+                                        w.x = low_bytes4(v[0], v[1]);
+                                        w.y = low_bytes4(v[2], v[3]);
+                                        w.z = low_bytes4(v[4], v[5]);
+                                        w.w = low_bytes4(v[6], v[7]);
                                         *(uint4*)(hsb + ((col >> 4) * 128 + row) * 16) = w;
                                     });
             fence_proxy_async();
@@ -467,7 +463,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             const int xr = row + R;
             const uint8_t* xrow = xs + st * kXBytes + (xr & 127) * 128;
             uint8_t* orow = p.out + (size_t)(p.H + gi) * (size_t)p.pitch + p.H + c0;
-            tmem_walk16<kMaxChunks>(tmem + kCCol + lane_off, grp, kEpiGroups, Tc, [&](const uint32_t (&v)[16], int col) {
+            tmem_walk16<kMaxChunks>(tmem + kCCol + lane_off, grp, kEpiGroups, Tc, [&](const uint32_t (&v)[8], int col) {
                 if (!row_ok) return;
                 const int xc = PADC + col;  // X column of these 16 cells
                 const int atom = xc >> 7, ch = (xc & 127) >> 4;
@@ -476,14 +472,14 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
                 uint32_t o[4];
 #pragma unroll
                 for (int qq = 0; qq < 4; ++qq) {
-                    const uint32_t* b = &v[4 * qq];
+                    const uint32_t* b = &v[2 * qq];  // cells 4qq .. 4qq+3 as two 16-bit pairs
                     if (small) {
-                        o[qq] = rule_swar8(pack4(b[0], b[1], b[2], b[3]), sw[qq], p.q);
+                        o[qq] = rule_swar8(low_bytes4(b[0], b[1]), sw[qq], p.q);
                     } else {
                         uint32_t r = 0;
 #pragma unroll
                         for (int e = 0; e < 4; ++e) {
-                            const int B = (int)b[e];
+                            const int B = (int)((b[e >> 1] >> (16 * (e & 1))) & 0xffffu);
                             const int sv = (sw[qq] >> (8 * e)) & 1;
                             const int lo = sv ? p.slo : p.blo, hi = sv ? p.shi : p.bhi;
                             r |= (uint32_t)((B >= lo) & (B <= hi)) << (8 * e);
