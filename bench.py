@@ -298,6 +298,47 @@ def radius_sweep(C, torch, args):
         print(json.dumps(out), flush=True)
 
 
+def strips_run(C, torch, args, world, rank, local):
+    """The 16384^2 R=5 grid split into `world` row strips (one per rank, plain
+    variant), halos exchanged every args.strips generations (NCCL between ranks;
+    with one rank the strip exchanges with itself).  Strong scaling: the total
+    work is fixed.  Times `steps` generations after `warmup` with CUDA events on
+    the rank's stream, max over ranks; checks the gathered grid at generation
+    100 against the reference's grid."""
+    from cat_cpu_b200 import strips as S
+    k = args.strips
+    dev = torch.device("cuda", local)
+    make = lambda rows, n: S.GpuStepper(rows, n, RADIUS, RULE, device=local)  # noqa: E731
+    if world > 1:
+        st = S.DistStrips(N, RADIUS, k, make, dev)
+        mine = [st.s]
+    else:
+        st = S.LocalStrips(N, RADIUS, 1, k, make, device=dev)
+        mine = st.strips
+    start = C.start_grid(N, SEED, DENSITY, 1)
+    try:
+        st.set_state(start)
+        st.step(100)
+        got = st.get_state().cpu().numpy()
+        bit_exact = hashlib.sha256(got.tobytes()).hexdigest() == golden_step100()
+        st.set_state(start)
+        st.step(max(args.warmup, 3) * k)
+        torch.cuda.synchronize()
+        barrier(world)
+        stream = st.stream  # the strips' own stream: every kernel and copy of theirs runs on it
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        gens = max(k, args.steps - args.steps % k)
+        a.record(stream)
+        st.step(gens)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(a.elapsed_time(b), world)
+    finally:
+        for s in mine:
+            s.st.close()
+    return dict(ms=ms, generations=gens, bit_exact=bit_exact, halo_rows=st.h)
+
+
 def batched_run(C, torch, steps, warmup_steps):
     """The batched workload (4096 grids, sides log-uniform in [64, 2048], R in 1..8,
     scaled interval rule, 256 steps per ltl_batch_step call)."""
@@ -431,6 +472,9 @@ def main():
     ap.add_argument("--sweep", action="store_true",
                     help="radius sweep at 32768^2 (one JSON line per radius) instead of the headline run")
     ap.add_argument("--sweep-steps", type=int, default=100)
+    ap.add_argument("--strips", type=int, default=0, metavar="K",
+                    help="one 16384^2 grid split into row strips across the ranks (strong scaling), "
+                         "halo exchange every K generations, instead of the per-rank replicas")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
     args = ap.parse_args()
@@ -447,6 +491,23 @@ def main():
 
     if args.sweep:
         radius_sweep(C, torch, args)
+        return
+    if args.strips > 0:
+        r = strips_run(C, torch, args, world, rank, local)
+        if rank == 0:
+            print(json.dumps({
+                "metric": METRIC, "value": round(N * N * r["generations"] / (r["ms"] * 1e-3) / 1e9, 3),
+                "unit": "GCUPS", "n_gpus": world, "steps": r["generations"], "warmup": args.warmup,
+                "ms_per_step": round(r["ms"] / r["generations"], 5), "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "u8", "data": "synthetic: reference generator start grid (seed 1)",
+                "config": {"workload": WORKLOAD, "variant": "plain, row strips", "n": N, "radius": RADIUS,
+                           "parallelism": f"row strips x{world}, {r['halo_rows']}-row halo exchange every "
+                                          f"{args.strips} generations",
+                           "l2": "not flushed (continuous run)"},
+                "bit_exact_step100": r["bit_exact"]}))
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     start = C.start_grid(N, SEED, DENSITY, 1)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")

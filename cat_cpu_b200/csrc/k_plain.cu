@@ -21,10 +21,10 @@ namespace ltl {
 // Top/bottom bands copy 16-byte chunks whose columns are inner (same column in
 // the source row); everything else goes byte by byte.
 // ---------------------------------------------------------------------------
-__global__ void k_halo_rows(uint8_t* __restrict__ g, int n, int H, size_t pitch) {
+__global__ void k_halo_rows(uint8_t* __restrict__ g, int n, int rows, int H, size_t pitch) {
     const int band = blockIdx.y;                       // 0 .. 2H-1
-    const int r = band < H ? band : n + band;          // frame row
-    const int src_r = H + wrap_mod(r - H, n);
+    const int r = band < H ? band : rows + band;       // frame row
+    const int src_r = H + wrap_mod(r - H, rows);
     const int W = n + 2 * H;
     const int nchunks = (W + 15) / 16;
     uint8_t* dst_row = g + (size_t)r * pitch;
@@ -39,10 +39,10 @@ __global__ void k_halo_rows(uint8_t* __restrict__ g, int n, int H, size_t pitch)
     }
 }
 
-__global__ void k_halo_cols(uint8_t* __restrict__ g, int n, int H, size_t pitch) {
+__global__ void k_halo_cols(uint8_t* __restrict__ g, int n, int rows, int H, size_t pitch) {
     // inner rows only; 2H halo bytes per row
     const int per_row = 2 * H;
-    const long long total = (long long)n * per_row;
+    const long long total = (long long)rows * per_row;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         int i = (int)(t / per_row);
@@ -57,10 +57,10 @@ cudaError_t launch_halo_fill(const Frame& f, cudaStream_t s) {
     const int W = f.n + 2 * f.H;
     const int nchunks = (W + 15) / 16;
     dim3 g1((unsigned)std::min((nchunks + 127) / 128, 64), (unsigned)(2 * f.H));
-    k_halo_rows<<<g1, 128, 0, s>>>(f.base, f.n, f.H, f.pitch);
-    long long total = (long long)f.n * 2 * f.H;
+    k_halo_rows<<<g1, 128, 0, s>>>(f.base, f.n, f.nrows(), f.H, f.pitch);
+    long long total = (long long)f.nrows() * 2 * f.H;
     int blocks = (int)std::min<long long>((total + 255) / 256, 4096);
-    k_halo_cols<<<blocks, 256, 0, s>>>(f.base, f.n, f.H, f.pitch);
+    k_halo_cols<<<blocks, 256, 0, s>>>(f.base, f.n, f.nrows(), f.H, f.pitch);
     return cudaGetLastError();
 }
 
@@ -178,7 +178,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 template <int R>
 __global__ void __launch_bounds__(kPlainWarps * 32)
-k_plain_swar8(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n, int H, size_t pitch,
+k_plain_swar8(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n, int rows, int H, size_t pitch,
               int band_rows, int n_strips, int n_items, RuleSwar8 q, int wrap) {
     static_assert(2 * R + 2 + kAhead <= kRingRows, "ring too small");
     extern __shared__ uint4 ring_all[];
@@ -192,15 +192,15 @@ k_plain_swar8(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n,
         const int strip = item % n_strips;
         const int band = item / n_strips;
         const int r0 = band * band_rows;
-        const int r1 = min(r0 + band_rows, n);
+        const int r1 = min(r0 + band_rows, rows);
         const int x = strip * kStripOut - 16 + 16 * lane;      // inner column of this lane's chunk
         const bool loads = x < n + 16;                          // chunks past that feed no output
         const bool outputs = lane >= 1 && lane <= 30 && x < n;
         const uint8_t* col = cur + (size_t)H + (loads ? (wrap ? wrap1(x, n) : x) : 0);
-        const int rlast = min(r1 - 1 + R, n - 1 + R);           // last row any window of the band needs
+        const int rlast = min(r1 - 1 + R, rows - 1 + R);        // last row any window of the band needs
         auto slot = [&](int r) { return ring + (r & (kRingRows - 1)) * 32; };
         auto issue = [&](int r) {
-            if (loads && r <= rlast) cp_async16(slot(r), col + (size_t)(H + (wrap ? wrap1(r, n) : r)) * pitch);
+            if (loads && r <= rlast) cp_async16(slot(r), col + (size_t)(H + (wrap ? wrap1(r, rows) : r)) * pitch);
             cp_async_commit();
         };
         // rows r0-R .. r0+R start the window; kAhead more go in flight behind them
@@ -262,9 +262,9 @@ int plain_swar8_band_rows(int n, int device) {
 template <int R>
 static cudaError_t launch_swar8_r(const Frame& cur, const Frame& nxt, const RuleSwar8& q, int band_rows, int wrap,
                                   cudaStream_t s) {
-    const int n = cur.n;
+    const int n = cur.n, rows = cur.nrows();
     const int strips = (n + kStripOut - 1) / kStripOut;
-    const int bands = (n + band_rows - 1) / band_rows;
+    const int bands = (rows + band_rows - 1) / band_rows;
     const int items = strips * bands;
     const int smem = kPlainWarps * kRingRows * 32 * (int)sizeof(uint4);
     int dev = 0, sms = 148, per_sm = 0;
@@ -273,7 +273,7 @@ static cudaError_t launch_swar8_r(const Frame& cur, const Frame& nxt, const Rule
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_plain_swar8<R>, kPlainWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
     int ctas = std::min((items + kPlainWarps - 1) / kPlainWarps, sms * per_sm);
-    k_plain_swar8<R><<<ctas, kPlainWarps * 32, smem, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch, band_rows,
+    k_plain_swar8<R><<<ctas, kPlainWarps * 32, smem, s>>>(cur.base, nxt.base, n, rows, cur.H, cur.pitch, band_rows,
                                                          strips, items, q, wrap);
     return cudaGetLastError();
 }
@@ -295,11 +295,11 @@ cudaError_t plain_prepare(int radius) {
     }
 }
 
-bool plain_wrap_supported(int n) { return n >= 64 && n % 16 == 0; }
+bool plain_wrap_supported(int n, int rows) { return n >= 64 && n % 16 == 0 && rows >= 16; }
 
 cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows, bool wrap,
                                cudaStream_t s) {
-    if (wrap && !plain_wrap_supported(cur.n)) return cudaErrorInvalidValue;
+    if (wrap && !plain_wrap_supported(cur.n, cur.nrows())) return cudaErrorInvalidValue;
     RuleSwar8 q = make_rule_swar8(rule);
     const int w = wrap ? 1 : 0;
     switch (rule.radius) {
@@ -369,7 +369,7 @@ __device__ __forceinline__ uint4 swar8_row(const uint32_t (&V)[4], uint4 c, cons
 
 template <int R, int D>
 __global__ void __launch_bounds__(kPlainWarps * 32)
-k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n, int H, size_t pitch,
+k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int n, int rows, int H, size_t pitch,
                  int band_rows, int n_strips, int n_items, RuleSwar8 q, int wrap) {
     constexpr int kAh = tb_ahead<R>();
     constexpr int kRS = 2 * R + 2;  // rows per inner-stage ring
@@ -389,7 +389,7 @@ k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int
         const int strip = item % n_strips;
         const int band = item / n_strips;
         const int r0 = band * band_rows;
-        const int r1 = min(r0 + band_rows, n);
+        const int r1 = min(r0 + band_rows, rows);
         const int x = strip * kStripOut - 16 + 16 * lane;
         const bool loads = x < n + 16;  // (D*R <= 16: columns >= n + 16 feed no output)
         const bool outputs = lane >= 1 && lane <= 30 && x < n;
@@ -398,13 +398,13 @@ k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int
         const int yfirst = r0 - (D - 1) * R;        // first and last stage-1 rows
         const int ylast = r1 - 1 + (D - 1) * R;
         for (int r = yfirst - R; r <= yfirst + R + kAh; ++r) {
-            if (loads && r <= rlast) cp_async16(slot0(r), col + (size_t)(H + (wrap ? wrap1(r, n) : r)) * pitch);
+            if (loads && r <= rlast) cp_async16(slot0(r), col + (size_t)(H + (wrap ? wrap1(r, rows) : r)) * pitch);
             cp_async_commit();
         }
         // next input row to request (y + R + 1 + kAh at iteration y, never
         // negative), and the output row of stage D once it produces (y - (D-1)R)
         int r_next = yfirst + R + 1 + kAh;
-        const uint8_t* src_next = col + (size_t)(H + (wrap ? wrap1(r_next, n) : r_next)) * pitch;
+        const uint8_t* src_next = col + (size_t)(H + (wrap ? wrap1(r_next, rows) : r_next)) * pitch;
         uint8_t* dst = nxt + (size_t)(H + r0) * pitch + H + x;
         cp_async_wait<kAh>();
         uint32_t V[D][4];
@@ -466,7 +466,7 @@ k_plain_swar8_tb(const uint8_t* __restrict__ cur, uint8_t* __restrict__ nxt, int
                 cp_async_commit();
                 ++r_next;
                 src_next += pitch;
-                if (wrap && r_next == n) src_next -= (size_t)n * pitch;  // the next row is inner row 0
+                if (wrap && r_next == rows) src_next -= (size_t)rows * pitch;  // the next row is inner row 0
                 cp_async_wait<kAh>();  // input row y + R + 1 has landed
                 v_slide(V[0], *slot0(y + R + 1), *slot0(y - R));
             }
@@ -488,9 +488,9 @@ bool plain_tb_supported(int radius, int depth) {
 template <int R, int D>
 static cudaError_t launch_tb_rd(const Frame& cur, const Frame& nxt, const RuleSwar8& q, int band_rows, int wrap,
                                 cudaStream_t s) {
-    const int n = cur.n;
+    const int n = cur.n, rows = cur.nrows();
     const int strips = (n + kStripOut - 1) / kStripOut;
-    const int bands = (n + band_rows - 1) / band_rows;
+    const int bands = (rows + band_rows - 1) / band_rows;
     const int items = strips * bands;
     constexpr int smem = tb_smem_bytes<R, D>();
     int dev = 0, sms = 148, per_sm = 0;
@@ -499,7 +499,7 @@ static cudaError_t launch_tb_rd(const Frame& cur, const Frame& nxt, const RuleSw
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_plain_swar8_tb<R, D>, kPlainWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
     int ctas = std::min((items + kPlainWarps - 1) / kPlainWarps, sms * per_sm);
-    k_plain_swar8_tb<R, D><<<ctas, kPlainWarps * 32, smem, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch,
+    k_plain_swar8_tb<R, D><<<ctas, kPlainWarps * 32, smem, s>>>(cur.base, nxt.base, n, rows, cur.H, cur.pitch,
                                                                band_rows, strips, items, q, wrap);
     return cudaGetLastError();
 }
@@ -539,7 +539,7 @@ cudaError_t plain_tb_prepare(int radius) {
 cudaError_t launch_plain_tb(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows, int depth,
                             bool wrap, cudaStream_t s) {
     if (!plain_tb_supported(rule.radius, depth) || cur.H < depth * rule.radius) return cudaErrorInvalidValue;
-    if (wrap && !plain_wrap_supported(cur.n)) return cudaErrorInvalidValue;
+    if (wrap && !plain_wrap_supported(cur.n, cur.nrows())) return cudaErrorInvalidValue;
     RuleSwar8 q = make_rule_swar8(rule);
     const int w = wrap ? 1 : 0;
     switch (rule.radius) {
@@ -570,8 +570,8 @@ constexpr int kWideThreads = 256;
 
 template <int K>
 __global__ void __launch_bounds__(kWideThreads)
-k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int H, size_t pitch, int band_rows,
-             int T, Rule rule) {
+k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int rows, int H, size_t pitch,
+             int band_rows, int T, Rule rule) {
     constexpr int L = 1024 * K;  // window columns per CTA
     __shared__ int P[2][L + 1];
     __shared__ int wsum[kWideThreads / 32];
@@ -579,7 +579,7 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
     const int R = rule.radius;
     const int j0 = blockIdx.x * T;
     const int r0 = blockIdx.y * band_rows;
-    const int r1 = min(r0 + band_rows, n);
+    const int r1 = min(r0 + band_rows, rows);
     const int c0 = (j0 - R) & ~3;                  // floor to a multiple of 4 (two's complement)
     const int cstart = c0 + 4 * K * t;             // inner column of this thread's first window column
     const bool need = cstart <= n - 1 + R;         // later columns feed no output (and may lie past the row)
@@ -687,7 +687,7 @@ size_t plain_generic_vbuf_bytes(int, size_t) { return 0; }  // the fused kernel 
 
 cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, uint16_t* /*vbuf*/,
                                  cudaStream_t s) {
-    const int n = cur.n, R = rule.radius;
+    const int n = cur.n, rows = cur.nrows(), R = rule.radius;
     if (cur.H < ((R + 3) & ~3) || (cur.H & 3) || (cur.pitch & 3)) return cudaErrorInvalidValue;
     // T: outputs per tile, so that [j0 - R, j0 + T + R] (plus the rounding of c0)
     // fits the window columns; bands long enough to amortise the 2R+1-row start
@@ -700,22 +700,22 @@ cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule&
     const int T = (1024 * K - 2 * R - 3) & ~3;
     const int tiles = (n + T - 1) / T;
     const int want_bands = std::max(1, (6 * sms + tiles - 1) / tiles);
-    const int band = std::max(32, std::min({512, 4 * (2 * R + 1), (n + want_bands - 1) / want_bands}));
-    const dim3 grid(tiles, (n + band - 1) / band), block(kWideThreads);
+    const int band = std::max(32, std::min({512, 4 * (2 * R + 1), (rows + want_bands - 1) / want_bands}));
+    const dim3 grid(tiles, (rows + band - 1) / band), block(kWideThreads);
     if (K == 1)
-        k_plain_wide<1><<<grid, block, 0, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch, band, T, rule);
+        k_plain_wide<1><<<grid, block, 0, s>>>(cur.base, nxt.base, n, rows, cur.H, cur.pitch, band, T, rule);
     else
-        k_plain_wide<2><<<grid, block, 0, s>>>(cur.base, nxt.base, n, cur.H, cur.pitch, band, T, rule);
+        k_plain_wide<2><<<grid, block, 0, s>>>(cur.base, nxt.base, n, rows, cur.H, cur.pitch, band, T, rule);
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
 // K6: population and comparison over inner cells.
 // ---------------------------------------------------------------------------
-__global__ void k_population(const uint8_t* __restrict__ g, int n, int H, size_t pitch,
+__global__ void k_population(const uint8_t* __restrict__ g, int n, int rows, int H, size_t pitch,
                              unsigned long long* out) {
     unsigned long long acc = 0;
-    const long long total = (long long)n * n;
+    const long long total = (long long)rows * n;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         int i = (int)(t / n), j = (int)(t % n);
@@ -726,10 +726,10 @@ __global__ void k_population(const uint8_t* __restrict__ g, int n, int H, size_t
     if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
 }
 
-__global__ void k_compare(const uint8_t* __restrict__ g, int n, int H, size_t pitch,
+__global__ void k_compare(const uint8_t* __restrict__ g, int n, int rows, int H, size_t pitch,
                           const uint8_t* __restrict__ other, size_t opitch, unsigned long long* out) {
     unsigned long long cnt = 0, first = ~0ull;
-    const long long total = (long long)n * n;
+    const long long total = (long long)rows * n;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         int i = (int)(t / n), j = (int)(t % n);
@@ -753,9 +753,9 @@ __global__ void k_compare(const uint8_t* __restrict__ g, int n, int H, size_t pi
 cudaError_t launch_population(const Frame& f, unsigned long long* scratch, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
-    long long total = (long long)f.n * f.n;
+    long long total = (long long)f.nrows() * f.n;
     int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
-    k_population<<<blocks, 256, 0, s>>>(f.base, f.n, f.H, f.pitch, scratch);
+    k_population<<<blocks, 256, 0, s>>>(f.base, f.n, f.nrows(), f.H, f.pitch, scratch);
     return cudaGetLastError();
 }
 
@@ -764,18 +764,18 @@ cudaError_t launch_compare(const Frame& f, const uint8_t* other, size_t other_pi
     cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(scratch + 1, 0xff, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
-    long long total = (long long)f.n * f.n;
+    long long total = (long long)f.nrows() * f.n;
     int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
-    k_compare<<<blocks, 256, 0, s>>>(f.base, f.n, f.H, f.pitch, other, other_pitch, scratch);
+    k_compare<<<blocks, 256, 0, s>>>(f.base, f.n, f.nrows(), f.H, f.pitch, other, other_pitch, scratch);
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
 // Dense n x n <-> frame inner copies (device to device).
 // ---------------------------------------------------------------------------
-__global__ void k_copy_in(uint8_t* __restrict__ g, int n, int H, size_t pitch, const uint8_t* __restrict__ src,
-                          size_t sp) {
-    const long long total = (long long)n * n;
+__global__ void k_copy_in(uint8_t* __restrict__ g, int n, int rows, int H, size_t pitch,
+                          const uint8_t* __restrict__ src, size_t sp) {
+    const long long total = (long long)rows * n;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         int i = (int)(t / n), j = (int)(t % n);
@@ -783,9 +783,9 @@ __global__ void k_copy_in(uint8_t* __restrict__ g, int n, int H, size_t pitch, c
     }
 }
 
-__global__ void k_copy_out(const uint8_t* __restrict__ g, int n, int H, size_t pitch, uint8_t* __restrict__ dst,
-                           size_t dp) {
-    const long long total = (long long)n * n;
+__global__ void k_copy_out(const uint8_t* __restrict__ g, int n, int rows, int H, size_t pitch,
+                           uint8_t* __restrict__ dst, size_t dp) {
+    const long long total = (long long)rows * n;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         int i = (int)(t / n), j = (int)(t % n);
@@ -794,16 +794,16 @@ __global__ void k_copy_out(const uint8_t* __restrict__ g, int n, int H, size_t p
 }
 
 cudaError_t launch_copy_in(const Frame& f, const uint8_t* src, size_t src_pitch, cudaStream_t s) {
-    long long total = (long long)f.n * f.n;
+    long long total = (long long)f.nrows() * f.n;
     int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
-    k_copy_in<<<blocks, 256, 0, s>>>(f.base, f.n, f.H, f.pitch, src, src_pitch);
+    k_copy_in<<<blocks, 256, 0, s>>>(f.base, f.n, f.nrows(), f.H, f.pitch, src, src_pitch);
     return cudaGetLastError();
 }
 
 cudaError_t launch_copy_out(const Frame& f, uint8_t* dst, size_t dst_pitch, cudaStream_t s) {
-    long long total = (long long)f.n * f.n;
+    long long total = (long long)f.nrows() * f.n;
     int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
-    k_copy_out<<<blocks, 256, 0, s>>>(f.base, f.n, f.H, f.pitch, dst, dst_pitch);
+    k_copy_out<<<blocks, 256, 0, s>>>(f.base, f.n, f.nrows(), f.H, f.pitch, dst, dst_pitch);
     return cudaGetLastError();
 }
 

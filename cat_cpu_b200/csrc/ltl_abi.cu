@@ -39,7 +39,8 @@ void ltl_set_error(const char* fmt, ...) {
 
 struct ltl_ctx {
     int device = 0;
-    int n = 0;
+    int n = 0;       // columns (the side of a square torus)
+    int rows = 0;    // rows (== n except for ltl_create_rect)
     Rule rule{};
     int variant = LTL_VARIANT_PLAIN;
     int depth = 1;
@@ -119,22 +120,28 @@ static void drop_graphs(ltl_ctx* c) {
     }
 }
 
-extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin, int smax, int bmin, int bmax,
-                          int variant) {
+// rows x n torus (rows == n unless the plain-only rectangular form is asked for)
+static int create_impl(ltl_ctx** out, int device, int rows, int n, int radius, int smin, int smax, int bmin,
+                       int bmax, int variant) {
     if (!out) {
         ltl_set_error("ltl_create: out is NULL");
         return LTL_EINVAL;
     }
     *out = nullptr;
-    if (n < 1 || radius < 1 || n < radius) {
-        ltl_set_error("ltl_create: need n >= 1, radius >= 1 and n >= radius (n=%d, radius=%d)", n, radius);
+    if (n < 1 || radius < 1 || n < radius || rows < radius) {
+        ltl_set_error("ltl_create: need n >= 1, radius >= 1 and n, rows >= radius (n=%d, rows=%d, radius=%d)", n,
+                      rows, radius);
         return LTL_EINVAL;
+    }
+    if (rows != n && variant != LTL_VARIANT_PLAIN) {
+        ltl_set_error("ltl_create_rect: rectangular grids are served by the plain variant only");
+        return LTL_EUNSUPPORTED;
     }
     if (radius > 2047) {
         ltl_set_error("ltl_create: radius %d > 2047 is outside the exact range of every variant", radius);
         return LTL_EUNSUPPORTED;
     }
-    if ((long long)n * n > (1ll << 40)) {
+    if ((long long)rows * n > (1ll << 40)) {
         ltl_set_error("ltl_create: n=%d too large", n);
         return LTL_EINVAL;
     }
@@ -165,6 +172,7 @@ extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin
     }
     c->device = device;
     c->n = n;
+    c->rows = rows;
     c->rule = Rule{radius, smin, smax, bmin, bmax};
     c->variant = variant;
     cudaError_t e = cudaSetDevice(device);
@@ -180,8 +188,8 @@ extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin
     int H = halo_for(radius, 1);
     if (variant == LTL_VARIANT_TENSOR) H = std::max(H, tensor_plan_halo_needed(radius));
     size_t pitch = pitch_for(n, H);
-    size_t rows = (size_t)n + 2 * H + 1;  // +1 spare row: vector loads may run past the last frame row
-    size_t one = round_up(rows * pitch, 4096);
+    size_t frows = (size_t)rows + 2 * H + 1;  // +1 spare row: vector loads may run past the last frame row
+    size_t one = round_up(frows * pitch, 4096);
     c->frames_bytes = 2 * one;
     e = cudaMalloc(&c->frames, c->frames_bytes);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->frames, 0, c->frames_bytes, c->stream);
@@ -192,8 +200,8 @@ extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin
         release(c);
         return e == cudaErrorMemoryAllocation ? LTL_ENOMEM : LTL_ECUDA;
     }
-    c->fa = Frame{c->frames, n, H, pitch};
-    c->fb = Frame{c->frames + one, n, H, pitch};
+    c->fa = Frame{c->frames, n, H, pitch, rows};
+    c->fb = Frame{c->frames + one, n, H, pitch, rows};
 
     if (variant == LTL_VARIANT_PLAIN && !plain_swar8_supported(radius) && plain_generic_vbuf_bytes(n, pitch) > 0) {
         c->vbuf_bytes = plain_generic_vbuf_bytes(n, pitch);
@@ -210,7 +218,7 @@ extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin
         const int want = (int)tuning_lookup("plain", radius, n, "depth", n >= 256 ? 2 : 1);
         if (want > 1 && plain_tb_supported(radius, want) && H >= want * radius) depth = want;
         c->band_rows = (int)tuning_lookup("plain", radius, n, "band_rows", plain_swar8_band_rows(n, device));
-        c->plain_wrap = plain_wrap_supported(n);
+        c->plain_wrap = plain_wrap_supported(n, rows);
     }
     if (variant == LTL_VARIANT_PACKED) c->packed_band_rows = (int)tuning_lookup("packed", radius, n, "band_rows", 0);
     if (variant == LTL_VARIANT_PLAIN) e = plain_prepare(radius);
@@ -263,6 +271,16 @@ extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin
     return LTL_OK;
 }
 
+extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin, int smax, int bmin, int bmax,
+                          int variant) {
+    return create_impl(out, device, n, n, radius, smin, smax, bmin, bmax, variant);
+}
+
+extern "C" int ltl_create_rect(ltl_ctx** out, int device, int rows, int cols, int radius, int smin, int smax,
+                               int bmin, int bmax) {
+    return create_impl(out, device, rows, cols, radius, smin, smax, bmin, bmax, LTL_VARIANT_PLAIN);
+}
+
 extern "C" int ltl_destroy(ltl_ctx* c) {
     if (!c) return LTL_OK;
     cudaSetDevice(c->device);
@@ -288,6 +306,7 @@ extern "C" int ltl_get_info(const ltl_ctx* c, ltl_info* info) {
     }
     info->variant = c->variant;
     info->n = c->n;
+    info->rows = c->rows;
     info->radius = c->rule.radius;
     info->smin = c->rule.smin;
     info->smax = c->rule.smax;
@@ -324,8 +343,8 @@ static int after_upload(ltl_ctx* c) {
     return LTL_OK;
 }
 
-__global__ void k_binarize(uint8_t* g, int n, int H, size_t pitch) {
-    const long long total = (long long)n * n;
+__global__ void k_binarize(uint8_t* g, int n, int rows, int H, size_t pitch) {
+    const long long total = (long long)rows * n;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         int i = (int)(t / n), j = (int)(t % n);
@@ -342,11 +361,11 @@ extern "C" int ltl_upload(ltl_ctx* c, const uint8_t* inner, size_t pitch) {
     }
     LTL_CUDA(cudaSetDevice(c->device));
     Frame& f = cur_frame(c);
-    LTL_CUDA(cudaMemcpy2DAsync(f.inner(0, 0), f.pitch, inner, pitch, c->n, c->n, cudaMemcpyHostToDevice,
+    LTL_CUDA(cudaMemcpy2DAsync(f.inner(0, 0), f.pitch, inner, pitch, c->n, c->rows, cudaMemcpyHostToDevice,
                                c->stream));
-    long long total = (long long)c->n * c->n;
-    k_binarize<<<(int)std::min<long long>((total + 255) / 256, 148 * 32), 256, 0, c->stream>>>(f.base, c->n, f.H,
-                                                                                                f.pitch);
+    long long total = (long long)c->rows * c->n;
+    k_binarize<<<(int)std::min<long long>((total + 255) / 256, 148 * 32), 256, 0, c->stream>>>(
+        f.base, c->n, c->rows, f.H, f.pitch);
     LTL_CUDA(cudaGetLastError());
     if (int r = after_upload(c)) return r;
     LTL_CUDA(cudaStreamSynchronize(c->stream));
@@ -373,7 +392,7 @@ extern "C" int ltl_download(ltl_ctx* c, uint8_t* inner, size_t pitch) {
     LTL_CUDA(cudaSetDevice(c->device));
     if (int r = sync_from_packed(c)) return r;
     Frame& f = cur_frame(c);
-    LTL_CUDA(cudaMemcpy2DAsync(inner, pitch, f.inner(0, 0), f.pitch, c->n, c->n, cudaMemcpyDeviceToHost,
+    LTL_CUDA(cudaMemcpy2DAsync(inner, pitch, f.inner(0, 0), f.pitch, c->n, c->rows, cudaMemcpyDeviceToHost,
                                c->stream));
     LTL_CUDA(cudaStreamSynchronize(c->stream));
     return LTL_OK;
@@ -389,6 +408,40 @@ extern "C" int ltl_download_device(ltl_ctx* c, uint8_t* dev_inner, size_t pitch)
     if (int r = sync_from_packed(c)) return r;
     LTL_CUDA(launch_copy_out(cur_frame(c), dev_inner, pitch, c->stream));
     return LTL_OK;
+}
+
+// Row-range transfers (device buffers): rows [row0, row0 + nrows) of the
+// current grid, `pitch` bytes apart in the caller's buffer.
+static int check_rows(ltl_ctx* c, const char* who, int row0, int nrows, const void* dev, size_t pitch) {
+    if (!dev || nrows < 0 || row0 < 0 || row0 + nrows > c->rows || pitch < (size_t)c->n) {
+        ltl_set_error("%s: bad rows [%d, %d) of %d, buffer or pitch", who, row0, row0 + nrows, c->rows);
+        return LTL_EINVAL;
+    }
+    return LTL_OK;
+}
+
+extern "C" int ltl_download_rows_device(ltl_ctx* c, int row0, int nrows, uint8_t* dev, size_t pitch) {
+    if (int r = check_ctx(c)) return r;
+    if (int r = check_rows(c, "ltl_download_rows_device", row0, nrows, dev, pitch)) return r;
+    if (nrows == 0) return LTL_OK;
+    LTL_CUDA(cudaSetDevice(c->device));
+    if (int r = sync_from_packed(c)) return r;
+    Frame& f = cur_frame(c);
+    LTL_CUDA(cudaMemcpy2DAsync(dev, pitch, f.inner(row0, 0), f.pitch, c->n, nrows, cudaMemcpyDeviceToDevice,
+                               c->stream));
+    return LTL_OK;
+}
+
+extern "C" int ltl_upload_rows_device(ltl_ctx* c, int row0, int nrows, const uint8_t* dev, size_t pitch) {
+    if (int r = check_ctx(c)) return r;
+    if (int r = check_rows(c, "ltl_upload_rows_device", row0, nrows, dev, pitch)) return r;
+    if (nrows == 0) return LTL_OK;
+    LTL_CUDA(cudaSetDevice(c->device));
+    if (int r = sync_from_packed(c)) return r;  // the other rows of a packed grid must survive
+    Frame& f = cur_frame(c);
+    LTL_CUDA(cudaMemcpy2DAsync(f.inner(row0, 0), f.pitch, dev, pitch, c->n, nrows, cudaMemcpyDeviceToDevice,
+                               c->stream));
+    return after_upload(c);
 }
 
 // One pass = `gens` generations (c->depth, or fewer for the remainder of a

@@ -21,9 +21,11 @@ constexpr int kWarp = 32;
 
 struct Frame {
     uint8_t* base;   // frame origin (row 0, column 0)
-    int n;           // inner side
+    int n;           // inner columns (and rows, unless `rows` is set)
     int H;           // halo width (cells)
     size_t pitch;    // bytes per frame row
+    int rows = 0;    // inner rows of a rectangular torus (0: square, n rows)
+    __host__ __device__ int nrows() const { return rows ? rows : n; }
     __host__ __device__ uint8_t* inner(int i, int j) const { return base + (size_t)(H + i) * pitch + H + j; }
     __host__ __device__ const uint8_t* cinner(int i, int j) const {
         return base + (size_t)(H + i) * pitch + H + j;

@@ -20,7 +20,7 @@ cudaError_t plain_prepare(int radius);
 cudaError_t packed_prepare(int radius);
 // wrap: read every cell from its inner position (torus wrap inside the kernel),
 // so the frame halo is neither read nor needed; requires plain_wrap_supported(n).
-bool plain_wrap_supported(int n);
+bool plain_wrap_supported(int n, int rows);
 cudaError_t launch_plain_swar8(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows, bool wrap,
                                cudaStream_t s);
 int plain_swar8_band_rows(int n, int device);

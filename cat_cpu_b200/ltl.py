@@ -32,7 +32,8 @@ ABI_SYMBOLS = [
     "ltl_compare_device", "ltl_benchmark_seed", "ltl_generate_state", "ltl_pack_device", "ltl_unpack_device",
     "ltl_batch_create", "ltl_batch_destroy", "ltl_batch_set_stream", "ltl_batch_upload", "ltl_batch_download",
     "ltl_batch_upload_all", "ltl_batch_download_all", "ltl_batch_step", "ltl_batch_synchronize",
-    "ltl_batch_info", "ltl_batch_set_param", "ltl_set_param", "ltl_set_timing", "ltl_get_timing", "ltl_step_noalloc", "ltl_last_error", "ltl_version",
+    "ltl_batch_info", "ltl_batch_set_param", "ltl_set_param", "ltl_set_timing", "ltl_get_timing", "ltl_step_noalloc", "ltl_create_rect", "ltl_download_rows_device", "ltl_upload_rows_device",
+    "ltl_last_error", "ltl_version",
 ]
 
 
@@ -46,7 +47,7 @@ class Info(ctypes.Structure):
     _fields_ = [("variant", ctypes.c_int), ("n", ctypes.c_int), ("radius", ctypes.c_int),
                 ("smin", ctypes.c_int), ("smax", ctypes.c_int), ("bmin", ctypes.c_int), ("bmax", ctypes.c_int),
                 ("halo", ctypes.c_int), ("pitch", ctypes.c_longlong), ("temporal_depth", ctypes.c_int),
-                ("operand_bits", ctypes.c_int), ("device_bytes", ctypes.c_longlong)]
+                ("operand_bits", ctypes.c_int), ("device_bytes", ctypes.c_longlong), ("rows", ctypes.c_int)]
 
 
 class GridDesc(ctypes.Structure):
@@ -100,6 +101,9 @@ def lib():
     L.ltl_get_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                                  ctypes.POINTER(ctypes.c_longlong)]
     L.ltl_step_noalloc.argtypes = [vp, sz, vp, sz, i, i, i, i, i, i, i, vp]
+    L.ltl_create_rect.argtypes = [ctypes.POINTER(vp), i, i, i, i, i, i, i, i]
+    L.ltl_download_rows_device.argtypes = [vp, i, i, vp, sz]
+    L.ltl_upload_rows_device.argtypes = [vp, i, i, vp, sz]
     L.ltl_last_error.restype = ctypes.c_char_p
     L.ltl_version.restype = ctypes.c_char_p
     _lib = L
@@ -135,15 +139,21 @@ def start_grid(n, user_seed, density, threads=1):
 
 class CUDASolver:
     """One n x n torus on a GPU.  Method names follow CASolver (CASolver.h:7-28);
-    radius and rule (reference centre-excluded convention) are run-time values."""
+    radius and rule (reference centre-excluded convention) are run-time values.
+    rows: a rows x n torus instead (plain variant only; ltl_create_rect)."""
 
-    def __init__(self, n, radius, rule, variant=VARIANT_AUTO, device=0, threads=1):
+    def __init__(self, n, radius, rule, variant=VARIANT_AUTO, device=0, threads=1, rows=None):
         smin, smax, bmin, bmax = rule
         h = ctypes.c_void_p()
-        check(lib().ltl_create(ctypes.byref(h), int(device), int(n), int(radius), int(smin), int(smax), int(bmin),
-                               int(bmax), int(variant)))
+        if rows is None:
+            check(lib().ltl_create(ctypes.byref(h), int(device), int(n), int(radius), int(smin), int(smax),
+                                   int(bmin), int(bmax), int(variant)))
+        else:
+            check(lib().ltl_create_rect(ctypes.byref(h), int(device), int(rows), int(n), int(radius), int(smin),
+                                        int(smax), int(bmin), int(bmax)))
         self._h = h
         self.n, self.radius, self.rule, self.device, self.threads = n, radius, tuple(rule), device, threads
+        self.rows = n if rows is None else int(rows)
         self.info = self.get_info()
         self.variant = self.info.variant
 
@@ -178,7 +188,7 @@ class CUDASolver:
 
     def setState(self, grid):
         g = np.ascontiguousarray(grid, dtype=np.uint8)
-        assert g.shape == (self.n, self.n)
+        assert g.shape == (self.rows, self.n)
         check(lib().ltl_upload(self._h, _ptr(g), self.n))
 
     def doStep(self):
@@ -191,8 +201,8 @@ class CUDASolver:
         check(lib().ltl_synchronize(self._h))
 
     def getCurrentState(self):
-        """CASolver::getCurrentState (CASolver.cpp:9-13): inner n x n cells, uint8."""
-        out = np.empty((self.n, self.n), dtype=np.uint8)
+        """CASolver::getCurrentState (CASolver.cpp:9-13): inner n x n (rows x n) cells, uint8."""
+        out = np.empty((self.rows, self.n), dtype=np.uint8)
         check(lib().ltl_download(self._h, _ptr(out), self.n))
         return out
 
@@ -229,6 +239,12 @@ class CUDASolver:
 
     def download_device(self, dev_ptr, pitch):
         check(lib().ltl_download_device(self._h, ctypes.c_void_p(dev_ptr), int(pitch)))
+
+    def download_rows_device(self, row0, nrows, dev_ptr, pitch):
+        check(lib().ltl_download_rows_device(self._h, int(row0), int(nrows), ctypes.c_void_p(dev_ptr), int(pitch)))
+
+    def upload_rows_device(self, row0, nrows, dev_ptr, pitch):
+        check(lib().ltl_upload_rows_device(self._h, int(row0), int(nrows), ctypes.c_void_p(dev_ptr), int(pitch)))
 
     def compare_device(self, dev_ptr, pitch):
         mm, first = ctypes.c_uint64(), ctypes.c_int64()

@@ -52,6 +52,7 @@ typedef struct {
     int temporal_depth;   /* generations advanced per kernel pass */
     int operand_bits;     /* tensor path: 8 (u8 kind::i8) or 16 (f16 kind::f16); 0 otherwise */
     long long device_bytes; /* device memory held by the context */
+    int rows;             /* rows of the torus (== n except for ltl_create_rect) */
 } ltl_info;
 
 /* Create a solver for one n x n torus on `device` (CUDA ordinal).
@@ -61,6 +62,15 @@ typedef struct {
  * reference's torus halo is only defined there, HostSolver.tpp:93-140). */
 int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin, int smax, int bmin, int bmax,
                int variant);
+
+/* A plain-variant solver for a rows x cols torus (rows may differ from cols).
+ * The building block of one grid split into row strips across GPUs: a strip of
+ * m rows plus R*k halo rows above and below, stepped as a torus of its own for
+ * k generations, leaves its m inner rows exact (the false vertical wrap only
+ * reaches R*k rows in).  No counterpart in the reference, whose grids are
+ * square and live in one process (CADataDomain.tpp:4-98). */
+int ltl_create_rect(ltl_ctx** out, int device, int rows, int cols, int radius, int smin, int smax, int bmin,
+                    int bmax);
 
 /* Release device memory and graphs.  (The reference never frees its domains.) */
 int ltl_destroy(ltl_ctx* ctx);
@@ -209,6 +219,12 @@ int ltl_get_timing(ltl_ctx* ctx, double* step_kernel_ms, long long* step_kernel_
  * without ordering) race and corrupt each other's results. */
 int ltl_step_noalloc(const uint8_t* dev_in, size_t in_pitch, uint8_t* dev_out, size_t out_pitch, int n, int radius,
                      int smin, int smax, int bmin, int bmax, int steps, void* stream);
+
+/* Rows [row0, row0 + nrows) of the current grid to or from device memory
+ * (`pitch` bytes between rows, cells 0/1), stream-ordered on the context's
+ * stream: the halo exchange of row strips.  No reference counterpart. */
+int ltl_download_rows_device(ltl_ctx* ctx, int row0, int nrows, uint8_t* dev, size_t pitch);
+int ltl_upload_rows_device(ltl_ctx* ctx, int row0, int nrows, const uint8_t* dev, size_t pitch);
 
 /* Message for the calling thread's last failed call ("" if none). */
 const char* ltl_last_error(void);
