@@ -64,8 +64,7 @@ extern "C" int ltl_step_noalloc(const uint8_t* dev_in, size_t in_pitch, uint8_t*
     const size_t pitch = pitch_for(n, H);
     const size_t frame = round_up(((size_t)n + 2 * H + 1) * pitch, 256);
     const bool generic = !plain_swar8_supported(radius);
-    const size_t vbytes = generic ? round_up(plain_generic_vbuf_bytes(n, pitch), 256) : 0;
-    const size_t need = 2 * frame + vbytes;
+    const size_t need = 2 * frame;
     if (need > kNoAllocScratchBytes) {
         ltl_set_error("ltl_step_noalloc: n=%d, radius=%d needs %zu bytes of scratch; the fixed scratch holds %zu "
                       "(use ltl_create for larger grids)",
@@ -99,7 +98,6 @@ extern "C" int ltl_step_noalloc(const uint8_t* dev_in, size_t in_pitch, uint8_t*
     uint8_t* scratch = (uint8_t*)base;
     Frame fa{scratch, n, H, pitch};
     Frame fb{scratch + frame, n, H, pitch};
-    uint16_t* vbuf = generic ? (uint16_t*)(scratch + 2 * frame) : nullptr;
     const Rule rule{radius, smin, smax, bmin, bmax};
     int band_rows = 0;
     if (!generic) band_rows = (int)tuning_lookup("plain", radius, n, "band_rows", plain_swar8_band_rows(n, device));
@@ -110,7 +108,7 @@ extern "C" int ltl_step_noalloc(const uint8_t* dev_in, size_t in_pitch, uint8_t*
     Frame* cur = &fa;
     Frame* nxt = &fb;
     for (int i = 0; i < steps && e == cudaSuccess; ++i) {
-        e = generic ? launch_plain_generic(*cur, *nxt, rule, vbuf, s)
+        e = generic ? launch_plain_generic(*cur, *nxt, rule, s)
                     : launch_plain_swar8(*cur, *nxt, rule, band_rows, false, s);
         if (e == cudaSuccess) e = launch_halo_fill(*nxt, s);
         Frame* t = cur;

@@ -683,10 +683,7 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
     }
 }
 
-size_t plain_generic_vbuf_bytes(int, size_t) { return 0; }  // the fused kernel needs no column-sum buffer
-
-cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, uint16_t* /*vbuf*/,
-                                 cudaStream_t s) {
+cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, cudaStream_t s) {
     const int n = cur.n, rows = cur.nrows(), R = rule.radius;
     if (cur.H < ((R + 3) & ~3) || (cur.H & 3) || (cur.pitch & 3)) return cudaErrorInvalidValue;
     // T: outputs per tile, so that [j0 - R, j0 + T + R] (plus the rounding of c0)

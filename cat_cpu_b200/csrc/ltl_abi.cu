@@ -48,8 +48,6 @@ struct ltl_ctx {
     bool cur_is_a = true;
     uint8_t* frames = nullptr;
     size_t frames_bytes = 0;
-    uint16_t* vbuf = nullptr;
-    size_t vbuf_bytes = 0;
     unsigned long long* scratch = nullptr;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
@@ -106,7 +104,6 @@ static void release(ltl_ctx* c) {
         if (g) cudaGraphExecDestroy(g);
     if (c->tplan) tensor_plan_destroy(c->tplan);
     if (c->frames) cudaFree(c->frames);
-    if (c->vbuf) cudaFree(c->vbuf);
     if (c->pwords) cudaFree(c->pwords);
     if (c->scratch) cudaFree(c->scratch);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -203,15 +200,6 @@ static int create_impl(ltl_ctx** out, int device, int rows, int n, int radius, i
     c->fa = Frame{c->frames, n, H, pitch, rows};
     c->fb = Frame{c->frames + one, n, H, pitch, rows};
 
-    if (variant == LTL_VARIANT_PLAIN && !plain_swar8_supported(radius) && plain_generic_vbuf_bytes(n, pitch) > 0) {
-        c->vbuf_bytes = plain_generic_vbuf_bytes(n, pitch);
-        e = cudaMalloc(&c->vbuf, c->vbuf_bytes);
-        if (e != cudaSuccess) {
-            ltl_set_error("ltl_create: V buffer allocation failed: %s", cudaGetErrorString(e));
-            release(c);
-            return LTL_ENOMEM;
-        }
-    }
     if (variant == LTL_VARIANT_PLAIN && plain_swar8_supported(radius)) {
         // generations per pass: the tuning table's value, else 2 where the
         // temporally blocked kernel applies (grids below 256 gain nothing)
@@ -316,7 +304,7 @@ extern "C" int ltl_get_info(const ltl_ctx* c, ltl_info* info) {
     info->pitch = (long long)c->fa.pitch;
     info->temporal_depth = c->depth;
     info->operand_bits = c->tplan ? tensor_plan_operand_bits(c->tplan) : 0;
-    info->device_bytes = (long long)(c->frames_bytes + c->vbuf_bytes + c->pwords_bytes);
+    info->device_bytes = (long long)(c->frames_bytes + c->pwords_bytes);
     return LTL_OK;
 }
 
@@ -468,7 +456,7 @@ static cudaError_t enqueue_pass(ltl_ctx* c, int gens) {
                 e = launch_plain_swar8(a, b, c->rule, c->band_rows, c->plain_wrap, c->stream);
                 step_kernels = 1;
             } else {
-                e = launch_plain_generic(a, b, c->rule, c->vbuf, c->stream);
+                e = launch_plain_generic(a, b, c->rule, c->stream);
                 step_kernels = 2;
             }
             if (c->timing && e == cudaSuccess) e = cudaEventRecord(e1, c->stream);

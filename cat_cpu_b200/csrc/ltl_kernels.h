@@ -31,11 +31,10 @@ cudaError_t plain_tb_prepare(int radius);
 cudaError_t launch_plain_tb(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows, int depth,
                             bool wrap, cudaStream_t s);
 
-// K1 generic path (any R): vertical sliding sums into `vbuf` (uint16, n rows x
-// pitch entries), then a prefix-sum horizontal pass with the rule fused.
-cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, uint16_t* vbuf,
-                                 cudaStream_t s);
-size_t plain_generic_vbuf_bytes(int n, size_t pitch);
+// K1 generic path (any R): one fused kernel (vertical window sums in registers,
+// a prefix scan per row in shared memory, the rule); needs a halo of at least
+// R rounded up to 4.
+cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, cudaStream_t s);
 
 // K6: population and comparison over the inner n x n cells.  `scratch` holds
 // two uint64 (count, first index) in device memory.
