@@ -108,7 +108,7 @@ extern "C" int ltl_step_noalloc(const uint8_t* dev_in, size_t in_pitch, uint8_t*
     Frame* cur = &fa;
     Frame* nxt = &fb;
     for (int i = 0; i < steps && e == cudaSuccess; ++i) {
-        e = generic ? launch_plain_generic(*cur, *nxt, rule, s)
+        e = generic ? launch_plain_generic(*cur, *nxt, rule, 0, s)
                     : launch_plain_swar8(*cur, *nxt, rule, band_rows, false, s);
         if (e == cudaSuccess) e = launch_halo_fill(*nxt, s);
         Frame* t = cur;

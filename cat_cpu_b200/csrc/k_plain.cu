@@ -1,6 +1,6 @@
 // k_plain.cu -- CUDA-core kernels of libltl_b200:
 //   K5 torus halo fill, K1 plain LtL step (SWAR fast path for R <= 5 and a
-//   generic two-pass path for any R), K6 population / comparison, and the
+//   fused prefix-sum path for larger R), K6 population / comparison, and the
 //   dense <-> frame copies used by upload/download.
 //
 // Semantics restated from the reference (kezada94/CAT_cpu):
@@ -553,157 +553,425 @@ cudaError_t launch_plain_tb(const Frame& cur, const Frame& nxt, const Rule& rule
 }
 
 // ---------------------------------------------------------------------------
-// K1 generic path (any R >= 1): one fused kernel, work per cell independent of R.
+// K1 generic path (any R up to 2038; serves R > 5): one fused kernel, work per
+// cell independent of R.
 //
-// A CTA of 256 threads owns a tile of T output columns [j0, j0 + T) and a band
-// of rows.  Its window columns are [c0, c0 + 1024K), c0 = j0 - R rounded down
-// to a multiple of 4; thread t owns the 4K consecutive columns starting at
-// c0 + 4Kt and keeps their vertical window sums V (2R+1 rows) in registers as
-// 16-bit SWAR lanes, sliding them down one row at a time (V += X(r+R+1) -
-// X(r-R)).  For every row the CTA scans V into prefix sums P in shared memory
-// (local sums, a warp scan, the warp totals), and each output reads
-//   B(j) = P[j - c0 + R + 1] - P[j - c0 - R],   k = B - centre,
-// then applies the interval rule.  P is double-buffered, so two barriers per
-// row suffice.  This replaces a two-kernel version that wrote V to HBM.
+// A CTA of NT threads owns a tile of T output columns [j0, j0 + T) and a band
+// of rows.  Its window columns are [c0, c0 + NT CPT), c0 = j0 - R rounded down
+// to a multiple of CPT; thread t owns the CPT consecutive columns starting at
+// c0 + CPT t and slides their vertical window sums V (2R+1 rows) down the band
+// in registers, as 16-bit lanes (two columns per word):
+//   V(r+1) = V(r) + X(r+R+1) - X(r-R).
+// For every row the CTA turns V into prefix sums P over the window columns in
+// shared memory (a local scan, a warp scan, the warp totals), and each output
+// reads two of them:
+//   B(j) = P[j - c0 + R + 1] - P[j - c0 - R],   k = B - centre.
+// Row pairs (R <= 90): one 32-bit word carries the vertical sums of two rows
+// for one column, row r in the low 16 bits and row r+1 in the high 16 bits.
+// Integer adds of such words keep the two lanes apart up to a carry out of the
+// low lane, and the window difference of the prefix sums is again a pair of
+// box counts B(r) + 65536 B(r+1) as long as B(r) < 65536.  R <= 90 keeps every
+// box count below 2^15 (181^2 = 32761), so one scan, one subtraction and a
+// 16-bit lane interval test serve two rows.  Above R = 90 each word carries
+// one row and the interval test runs on 32-bit lanes.
+//
+// Interval test on a lane holding B (centre included): with nlo = M - lo and
+// hiM = M + hi (M = 2^15 or 2^31, lo/hi clamped to [0, N+1] and [-1, N]),
+// B + nlo has the lane's top bit set iff B >= lo and hiM - B has it set iff
+// B <= hi; neither overflows the lane.  lo and hi depend on the centre s
+// (s ? [smin+1, smax+1] : [bmin, bmax]); one multiply-add of the lane-packed
+// centres selects them for both lanes at once.
 // ---------------------------------------------------------------------------
-constexpr int kWideThreads = 256;
+constexpr int kWidePairMaxRadius = 90;  // (2R+1)^2 < 2^15
+// threads per CTA: 128 for row pairs (R <= 90: the window overhead 2R/(128 CPT)
+// stays small and a CTA's barrier waits for fewer warps), 256 above, where the
+// wider window keeps the overlap of neighbouring tiles down
+constexpr int wide_threads(bool pair) { return pair ? 128 : 256; }
 
-template <int K>
-__global__ void __launch_bounds__(kWideThreads)
-k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int rows, int H, size_t pitch,
-             int band_rows, int T, Rule rule) {
-    constexpr int L = 1024 * K;  // window columns per CTA
-    __shared__ int P[2][L + 1];
-    __shared__ int wsum[kWideThreads / 32];
-    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    const int R = rule.radius;
-    const int j0 = blockIdx.x * T;
-    const int r0 = blockIdx.y * band_rows;
-    const int r1 = min(r0 + band_rows, rows);
-    const int c0 = (j0 - R) & ~3;                  // floor to a multiple of 4 (two's complement)
-    const int cstart = c0 + 4 * K * t;             // inner column of this thread's first window column
-    const bool need = cstart <= n - 1 + R;         // later columns feed no output (and may lie past the row)
-    const uint8_t* col = X + (size_t)H + cstart;   // 4-byte aligned: H, pitch and cstart are multiples of 4
-    auto ldw = [&](int r, int k) { return __ldg((const uint32_t*)(col + (size_t)(H + r) * pitch) + k); };
+struct RuleScan {
+    int radius;
+    uint32_t nlo0, hih0;  // dead centre, replicated to both 16-bit lanes in row-pair mode
+    int32_t dnlo, dhih;   // change for a live centre
+};
 
-    uint32_t V[2 * K];  // V[2k]: columns 4k, 4k+1; V[2k+1]: columns 4k+2, 4k+3 (16-bit lanes)
-#pragma unroll
-    for (int k = 0; k < 2 * K; ++k) V[k] = 0u;
-    if (need) {
-        for (int dy = -R; dy <= R; ++dy) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const uint32_t x = ldw(r0 + dy, k);
-                V[2 * k] += __byte_perm(x, 0, 0x4140);
-                V[2 * k + 1] += __byte_perm(x, 0, 0x4342);
-            }
-        }
-    }
-    for (int r = r0; r < r1; ++r) {
-        int* Pr = P[r & 1];
-        // issue this row's global loads first (the next row's entering and
-        // leaving window rows, the first output chunk's centre cells), so that
-        // their latency hides behind the scan
-        const bool slide = r + 1 < r1 && need;
-        uint32_t xa[K], xb[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            xa[k] = slide ? ldw(r + R + 1, k) : 0u;
-            xb[k] = slide ? ldw(r - R, k) : 0u;
-        }
-        const int q0 = 4 * t;
-        const bool out0 = q0 < T && j0 + q0 < n;
-        const uint32_t sw0 = out0 ? __ldg((const uint32_t*)(X + (size_t)(H + r) * pitch + H + j0 + q0)) : 0u;
-        // this thread's values and their local sum
-        int v[4 * K];
-#pragma unroll
-        for (int k = 0; k < 2 * K; ++k) {
-            v[2 * k] = (int)(V[k] & 0xffffu);
-            v[2 * k + 1] = (int)(V[k] >> 16);
-        }
-        int sum = 0;
-#pragma unroll
-        for (int i = 0; i < 4 * K; ++i) sum += v[i];
-        int incl = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (lane == 31) wsum[wid] = incl;
-        __syncthreads();
-        // exclusive prefix of the 8 warp totals, scanned by each warp's first lanes
-        int wt = lane < kWideThreads / 32 ? wsum[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < kWideThreads / 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, wt, o);
-            if (lane >= o) wt += y;
-        }
-        const int wpre = __shfl_sync(0xffffffffu, wt, (wid + 31) & 31);  // inclusive total of warps < wid
-        int run = incl - sum + (wid > 0 ? wpre : 0);
-#pragma unroll
-        for (int i = 0; i < 4 * K; ++i) {
-            Pr[4 * K * t + i] = run;
-            run += v[i];
-        }
-        if (t == kWideThreads - 1) Pr[L] = run;
-        __syncthreads();
-        // outputs: 4 consecutive cells per thread per pass
-        for (int q = q0; q < T; q += 4 * kWideThreads) {
-            const int j = j0 + q;
-            if (j >= n) break;
-            const uint32_t sw = q == q0 ? sw0 : __ldg((const uint32_t*)(X + (size_t)(H + r) * pitch + H + j));
-            const int base = j - c0;
-            uint32_t ow = 0;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int B = Pr[base + u + R + 1] - Pr[base + u - R];
-                const int sv = (sw >> (8 * u)) & 1;
-                // k in [lo, hi]  <=>  (unsigned)(k - lo) <= (unsigned)(hi - lo); an empty
-                // interval (hi < lo) has a negative width that no k passes as unsigned
-                const int lo = sv ? rule.smin : rule.bmin;
-                const int wdt = sv ? rule.smax - rule.smin : rule.bmax - rule.bmin;
-                const uint32_t in = wdt >= 0 && (uint32_t)(B - sv - lo) <= (uint32_t)wdt;
-                ow |= in << (8 * u);
-            }
-            uint8_t* yr = Y + (size_t)(H + r) * pitch + H + j;
-            if (j + 4 <= n) {
-                *(uint32_t*)yr = ow;
-            } else {
-                for (int u = 0; u < n - j; ++u) yr[u] = (uint8_t)((ow >> (8 * u)) & 0xffu);
-            }
-        }
-        if (slide) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                V[2 * k] += __byte_perm(xa[k], 0, 0x4140) - __byte_perm(xb[k], 0, 0x4140);
-                V[2 * k + 1] += __byte_perm(xa[k], 0, 0x4342) - __byte_perm(xb[k], 0, 0x4342);
-            }
-        }
+static RuleScan make_rule_scan(const Rule& r, bool pair) {
+    const long long N = (2ll * r.radius + 1) * (2ll * r.radius + 1);
+    auto clampll = [](long long v, long long a, long long b) { return v < a ? a : (v > b ? b : v); };
+    const long long lo0 = clampll(r.bmin, 0, N + 1), hi0 = clampll(r.bmax, -1, N);
+    const long long lo1 = clampll((long long)r.smin + 1, 0, N + 1), hi1 = clampll((long long)r.smax + 1, -1, N);
+    const long long M = pair ? 0x8000ll : 0x80000000ll;
+    RuleScan q;
+    q.radius = r.radius;
+    q.nlo0 = (uint32_t)(pair ? (M - lo0) * 0x10001ll : M - lo0);
+    q.hih0 = (uint32_t)(pair ? (M + hi0) * 0x10001ll : M + hi0);
+    q.dnlo = (int32_t)(lo0 - lo1);
+    q.dhih = (int32_t)(hi1 - hi0);
+    return q;
+}
+
+// PTX prmt in its default mode: result byte i is source byte sel[4i+2:4i] of
+// {b, a}; when bit 4i+3 of sel is set the byte is replaced by copies of that
+// source byte's top bit (zero for a 0/1 cell).
+template <uint32_t SEL>
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "n"(SEL));
+    return d;
+}
+
+// CPT bytes of one frame row at an address aligned to CPT.
+template <int CPT>
+__device__ __forceinline__ void ld_cells(const uint8_t* p, uint32_t (&w)[CPT / 4]) {
+    if constexpr (CPT == 8) {
+        const uint2 v = __ldg((const uint2*)p);
+        w[0] = v.x; w[1] = v.y;
+    } else {
+        const uint4 v = __ldg((const uint4*)p);
+        w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
     }
 }
 
-cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, cudaStream_t s) {
-    const int n = cur.n, rows = cur.nrows(), R = rule.radius;
-    if (cur.H < ((R + 3) & ~3) || (cur.H & 3) || (cur.pitch & 3)) return cudaErrorInvalidValue;
-    // T: outputs per tile, so that [j0 - R, j0 + T + R] (plus the rounding of c0)
-    // fits the window columns; bands long enough to amortise the 2R+1-row start
-    // (and short enough that tiles x bands keep about 6 CTAs per SM busy)
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int K = (1024 - 2 * R - 3 >= 256) ? 1 : 2;
-    if (2048 - 2 * R - 3 < 256) return cudaErrorInvalidValue;  // R > 893
-    const int T = (1024 * K - 2 * R - 3) & ~3;
-    const int tiles = (n + T - 1) / T;
-    const int want_bands = std::max(1, (6 * sms + tiles - 1) / tiles);
-    const int band = std::max(32, std::min({512, 4 * (2 * R + 1), (rows + want_bands - 1) / want_bands}));
-    const dim3 grid(tiles, (rows + band - 1) / band), block(kWideThreads);
-    if (K == 1)
-        k_plain_wide<1><<<grid, block, 0, s>>>(cur.base, nxt.base, n, rows, cur.H, cur.pitch, band, T, rule);
-    else
-        k_plain_wide<2><<<grid, block, 0, s>>>(cur.base, nxt.base, n, rows, cur.H, cur.pitch, band, T, rule);
+// V += X(entering) - X(leaving) for 4 columns held as two words of 16-bit lanes.
+// The byte difference is taken with a +1 bias so that no lane borrows.
+__device__ __forceinline__ void slide4(uint32_t& v01, uint32_t& v23, uint32_t xin, uint32_t xout) {
+    const uint32_t d = xin + 0x01010101u - xout;  // bytes in [0, 2]
+    v01 = v01 + prmt<0x4140>(d, 0u) - 0x00010001u;
+    v23 = v23 + prmt<0x4342>(d, 0u) - 0x00010001u;
+}
+
+// Inclusive warp-scan step: v += v of lane (lane - O), for lanes >= O (the
+// shuffle's own in-range predicate guards the add).
+template <int O>
+__device__ __forceinline__ uint32_t scan_up(uint32_t v) {
+    asm("{\n\t.reg .pred p;\n\t.reg .b32 y;\n\t"
+        "shfl.sync.up.b32 y|p, %0, %1, 0, -1;\n\t"
+        "@p add.u32 %0, %0, y;\n\t}"
+        : "+r"(v)
+        : "n"(O));
+    return v;
+}
+
+// v[u] = p[A + u], u = 0..3, for a 16-byte aligned p.
+template <int A>
+__device__ __forceinline__ void lds4(const uint32_t* p, uint32_t (&v)[4]) {
+    const uint4 a = *(const uint4*)p;
+    if constexpr (A == 0) {
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    } else {
+        const uint4 b = *(const uint4*)(p + 4);
+        const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = w[A + u];
+    }
+}
+
+// PAIR: two rows per iteration in 16-bit lanes (R <= 90); CPT: window columns
+// per thread (8 or 16); RM = R mod 4 fixes the alignment of the two prefix
+// reads of every output group.
+template <bool PAIR, int CPT, int RM>
+__global__ void __launch_bounds__(wide_threads(PAIR))
+k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int rows, int H, size_t pitch,
+             int band_rows, int T, RuleScan q) {
+    constexpr int kWideThreads = wide_threads(PAIR);
+    constexpr int L = kWideThreads * CPT;  // window columns per CTA
+    constexpr int NW = CPT / 4;            // words of cells per thread and row; output groups per thread
+    constexpr int EA = (RM + 1) & 3;       // (j - c0 + R + 1) mod 4
+    constexpr int SA = (4 - RM) & 3;       // (j - c0 - R) mod 4
+    constexpr int STEP = PAIR ? 2 : 1;     // rows per iteration
+    constexpr int PS = L + 4;              // words per P buffer
+    __shared__ __align__(16) uint32_t P[2 * PS];
+    __shared__ uint32_t wsum[2][kWideThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    const int R = q.radius;
+    const uint32_t nlo0 = q.nlo0, hih0 = q.hih0, dnlo = (uint32_t)q.dnlo, dhih = (uint32_t)q.dhih;
+    const int j0 = blockIdx.x * T;
+    const int r0 = blockIdx.y * band_rows;
+    const int r1 = min(r0 + band_rows, rows);
+    const int c0 = (j0 - R) & ~(CPT - 1);  // floor to a multiple of CPT (two's complement)
+    const int cstart = c0 + CPT * t;       // inner column of this thread's first window column
+    // later columns feed no output (and may lie past the row's halo)
+    const bool need = cstart <= n - 1 + R;
+    const ptrdiff_t pp = (ptrdiff_t)pitch;
+    // frame row 0 at this thread's window columns; aligned to CPT (H, pitch, c0
+    // are multiples of 16, 64 and CPT)
+    const uint8_t* colp = X + (ptrdiff_t)H + cstart;
+
+    // vertical window sums of row r0, 16-bit lanes: V[2k] columns 4k, 4k+1, V[2k+1] columns 4k+2, 4k+3
+    uint32_t V[2 * NW];
+#pragma unroll
+    for (int k = 0; k < 2 * NW; ++k) V[k] = 0u;
+    if (need) {
+        const uint8_t* p = colp + (ptrdiff_t)(H + r0 - R) * pp;
+        if constexpr (PAIR) {
+            uint32_t acc[NW];  // byte lanes: 2R+1 <= 181
+#pragma unroll
+            for (int k = 0; k < NW; ++k) acc[k] = 0u;
+#pragma unroll 16
+            for (int dy = -R; dy <= R; ++dy, p += pp) {
+                uint32_t x[NW];
+                ld_cells<CPT>(p, x);
+#pragma unroll
+                for (int k = 0; k < NW; ++k) acc[k] += x[k];
+            }
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                V[2 * k] = prmt<0x4140>(acc[k], 0u);
+                V[2 * k + 1] = prmt<0x4342>(acc[k], 0u);
+            }
+        } else {
+#pragma unroll 8
+            for (int dy = -R; dy <= R; ++dy, p += pp) {
+                uint32_t x[NW];
+                ld_cells<CPT>(p, x);
+#pragma unroll
+                for (int k = 0; k < NW; ++k) {
+                    V[2 * k] += prmt<0x4140>(x[k], 0u);
+                    V[2 * k + 1] += prmt<0x4342>(x[k], 0u);
+                }
+            }
+        }
+    }
+
+    // this thread's output groups: columns j0 + 4t + 4 NT g, g < NW (T < NT CPT)
+    bool has[NW], full[NW];
+#pragma unroll
+    for (int g = 0; g < NW; ++g) {
+        const int qq = 4 * t + 4 * kWideThreads * g;
+        has[g] = qq < T && j0 + qq < n;
+        full[g] = j0 + qq + 4 <= n;
+    }
+    const int dj = j0 - c0;  // in [R, R + CPT - 1], a multiple of 4
+    const uint32_t* pe_sm = P + 4 * t + dj + R + 1 - EA;  // 16-byte aligned
+    const uint32_t* ps_sm = P + 4 * t + dj - R - SA;
+    uint32_t* pw_sm = P + CPT * t;
+
+    // Per iteration (rows r, r+1 for pairs): the rows entering and leaving the
+    // window on the way to rows r+1 ([0]) and r+2 ([1], pairs only), and the
+    // centre cells of the output groups.  Two sets, the current one and the one
+    // being loaded for the next iteration, swap roles every iteration.
+    uint32_t inA[STEP][NW], outA[STEP][NW], cenA[NW][STEP];
+    uint32_t inB[STEP][NW], outB[STEP][NW], cenB[NW][STEP];
+    const uint8_t* xc = X + (ptrdiff_t)H * pp + H + j0 + 4 * t;  // centre row 0, group 0
+    auto load_rows = [&](int r, const uint8_t* pin, const uint8_t* pout, uint32_t(&in)[STEP][NW],
+                         uint32_t(&out)[STEP][NW]) {
+#pragma unroll
+        for (int h = 0; h < STEP; ++h) {
+            if (need && r + 1 + h < r1) {
+                ld_cells<CPT>(pin + h * pp, in[h]);
+                ld_cells<CPT>(pout + h * pp, out[h]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < NW; ++k) in[h][k] = out[h][k] = 0u;
+            }
+        }
+    };
+    auto load_centre = [&](int r, const uint8_t* pc, uint32_t(&c)[NW][STEP]) {
+#pragma unroll
+        for (int g = 0; g < NW; ++g)
+#pragma unroll
+            for (int h = 0; h < STEP; ++h)
+                c[g][h] = (r < r1 && has[g]) ? __ldg((const uint32_t*)(pc + h * pp + 4 * kWideThreads * g)) : 0u;
+    };
+    load_rows(r0, colp + (ptrdiff_t)(H + r0 + R + 1) * pp, colp + (ptrdiff_t)(H + r0 - R) * pp, inA, outA);
+    load_centre(r0, xc + (ptrdiff_t)r0 * pp, cenA);
+    const ptrdiff_t sp = STEP * pp;
+    const uint8_t* pin = colp + (ptrdiff_t)(H + r0 + STEP + R + 1) * pp;  // next iteration's rows
+    const uint8_t* pout = colp + (ptrdiff_t)(H + r0 + STEP - R) * pp;
+    const uint8_t* pc = xc + (ptrdiff_t)(r0 + STEP) * pp;
+    uint8_t* py = Y + (ptrdiff_t)(H + r0) * pp + H + j0 + 4 * t;
+
+    auto iteration = [&](const int b, int r, uint32_t(&in)[STEP][NW], uint32_t(&out)[STEP][NW],
+                         uint32_t(&cen)[NW][STEP], uint32_t(&nin)[STEP][NW], uint32_t(&nout)[STEP][NW],
+                         uint32_t(&ncen)[NW][STEP]) {
+        load_rows(r + STEP, pin, pout, nin, nout);
+        load_centre(r + STEP, pc, ncen);
+        pin += sp;
+        pout += sp;
+        pc += sp;
+        // one word per window column
+        uint32_t W[CPT];
+        uint32_t V1[2 * NW];
+        if constexpr (PAIR) {
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                V1[2 * k] = V[2 * k];
+                V1[2 * k + 1] = V[2 * k + 1];
+                slide4(V1[2 * k], V1[2 * k + 1], in[0][k], out[0][k]);  // row r+1
+                W[4 * k + 0] = prmt<0x5410>(V[2 * k], V1[2 * k]);
+                W[4 * k + 1] = prmt<0x7632>(V[2 * k], V1[2 * k]);
+                W[4 * k + 2] = prmt<0x5410>(V[2 * k + 1], V1[2 * k + 1]);
+                W[4 * k + 3] = prmt<0x7632>(V[2 * k + 1], V1[2 * k + 1]);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                W[4 * k + 0] = prmt<0x4410>(V[2 * k], 0u);
+                W[4 * k + 1] = prmt<0x4432>(V[2 * k], 0u);
+                W[4 * k + 2] = prmt<0x4410>(V[2 * k + 1], 0u);
+                W[4 * k + 3] = prmt<0x4432>(V[2 * k + 1], 0u);
+            }
+        }
+        // prefix sums over the window: local, warp, then the warp totals
+#pragma unroll
+        for (int i = 1; i < CPT; ++i) W[i] += W[i - 1];
+        const uint32_t tot = W[CPT - 1];
+        uint32_t incl = tot;
+        incl = scan_up<1>(incl);
+        incl = scan_up<2>(incl);
+        incl = scan_up<4>(incl);
+        incl = scan_up<8>(incl);
+        incl = scan_up<16>(incl);
+        if (lane == 31) wsum[b][wid] = incl;
+        __syncthreads();
+        uint32_t wt = wsum[b][lane & (kWideThreads / 32 - 1)];
+        wt = scan_up<1>(wt);
+        wt = scan_up<2>(wt);
+        wt = scan_up<4>(wt);
+        const uint32_t wpre = __shfl_sync(0xffffffffu, wt, (wid + 31) & 31);  // total of warps < wid
+        const uint32_t off = incl - tot + (wid > 0 ? wpre : 0u);
+#pragma unroll
+        for (int k = 0; k < NW; ++k) {
+            uint4 w;
+            w.x = off + (k > 0 ? W[4 * k - 1] : 0u);
+            w.y = off + W[4 * k];
+            w.z = off + W[4 * k + 1];
+            w.w = off + W[4 * k + 2];
+            *(uint4*)(pw_sm + b * PS + 4 * k) = w;
+        }
+        if (t == kWideThreads - 1) P[b * PS + L] = off + tot;
+        __syncthreads();
+
+        // outputs: 4 consecutive columns (of row r, and of row r+1 for pairs) per group
+        const bool second = r + 1 < r1;
+#pragma unroll
+        for (int g = 0; g < NW; ++g) {
+            if (!has[g]) break;
+            uint32_t pe[4], ps[4];
+            lds4<EA>(pe_sm + b * PS + 4 * kWideThreads * g, pe);
+            lds4<SA>(ps_sm + b * PS + 4 * kWideThreads * g, ps);
+            uint8_t* yr = py + 4 * kWideThreads * g;
+            const uint32_t cr = cen[g][0];
+            uint32_t res[4];
+            if constexpr (PAIR) {
+                const uint32_t cr1 = cen[g][STEP - 1];
+                uint32_t sw[4];
+                sw[0] = prmt<0x8480>(cr, cr1);  // centre of column u: row r in bit 0, row r+1 in bit 16
+                sw[1] = prmt<0x9591>(cr, cr1);
+                sw[2] = prmt<0xA6A2>(cr, cr1);
+                sw[3] = prmt<0xB7B3>(cr, cr1);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t ge = pe[u] - ps[u] + (sw[u] * dnlo + nlo0);
+                    const uint32_t le = (sw[u] * dhih + hih0) - pe[u] + ps[u];
+                    res[u] = ge & le & 0x80008000u;
+                }
+                const uint32_t t01 = prmt<0x7351>(res[0], res[1]);
+                const uint32_t t23 = prmt<0x7351>(res[2], res[3]);
+                const uint32_t o0 = prmt<0x5410>(t01, t23) >> 7;
+                const uint32_t o1 = prmt<0x7632>(t01, t23) >> 7;
+                if (full[g]) {
+                    *(uint32_t*)yr = o0;
+                    if (second) *(uint32_t*)(yr + pp) = o1;
+                } else {
+                    for (int u = 0; u < n - j0 - 4 * t - 4 * kWideThreads * g; ++u) {
+                        yr[u] = (uint8_t)(o0 >> (8 * u));
+                        if (second) yr[pp + u] = (uint8_t)(o1 >> (8 * u));
+                    }
+                }
+            } else {
+                uint32_t sw[4];
+                sw[0] = prmt<0x4440>(cr, 0u);
+                sw[1] = prmt<0x4441>(cr, 0u);
+                sw[2] = prmt<0x4442>(cr, 0u);
+                sw[3] = prmt<0x4443>(cr, 0u);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t ge = pe[u] - ps[u] + (sw[u] * dnlo + nlo0);
+                    const uint32_t le = (sw[u] * dhih + hih0) - pe[u] + ps[u];
+                    res[u] = ge & le & 0x80000000u;
+                }
+                const uint32_t t01 = prmt<0x7373>(res[0], res[1]);
+                const uint32_t t23 = prmt<0x7373>(res[2], res[3]);
+                const uint32_t o0 = prmt<0x5410>(t01, t23) >> 7;
+                if (full[g]) {
+                    *(uint32_t*)yr = o0;
+                } else {
+                    for (int u = 0; u < n - j0 - 4 * t - 4 * kWideThreads * g; ++u) yr[u] = (uint8_t)(o0 >> (8 * u));
+                }
+            }
+        }
+        py += sp;
+
+        // slide to the next iteration's first row
+        if constexpr (PAIR) {
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                V[2 * k] = V1[2 * k];
+                V[2 * k + 1] = V1[2 * k + 1];
+                slide4(V[2 * k], V[2 * k + 1], in[1][k], out[1][k]);  // row r+2
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < NW; ++k) slide4(V[2 * k], V[2 * k + 1], in[0][k], out[0][k]);
+        }
+    };
+
+    // two iterations per trip, so that the load sets and the P buffers alternate
+    // without copies
+    for (int r = r0;;) {
+        iteration(0, r, inA, outA, cenA, inB, outB, cenB);
+        r += STEP;
+        if (r >= r1) break;
+        iteration(1, r, inB, outB, cenB, inA, outA, cenA);
+        r += STEP;
+        if (r >= r1) break;
+    }
+}
+
+int plain_wide_cols_per_thread(int radius) { return radius <= 1018 ? 8 : 16; }
+
+bool plain_generic_supported(int radius) { return radius >= 1 && radius <= 2038; }
+
+template <bool PAIR, int CPT>
+static cudaError_t launch_wide_rm(const Frame& cur, const Frame& nxt, const RuleScan& q, int band, int T,
+                                  dim3 grid, cudaStream_t s) {
+    const dim3 block(wide_threads(PAIR));
+    const int n = cur.n, rows = cur.nrows();
+    const uint8_t* x = cur.base;
+    uint8_t* y = nxt.base;
+    switch (q.radius & 3) {
+        case 0: k_plain_wide<PAIR, CPT, 0><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
+        case 1: k_plain_wide<PAIR, CPT, 1><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
+        case 2: k_plain_wide<PAIR, CPT, 2><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
+        default: k_plain_wide<PAIR, CPT, 3><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
+    }
     return cudaGetLastError();
+}
+
+cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows,
+                                 cudaStream_t s) {
+    const int n = cur.n, rows = cur.nrows(), R = rule.radius;
+    if (!plain_generic_supported(R)) return cudaErrorInvalidValue;
+    const bool pair = R <= kWidePairMaxRadius;
+    const int cpt = plain_wide_cols_per_thread(R);
+    if (cur.H < (int)round_up((size_t)R, (size_t)cpt) || (cur.H & 15) || (cur.pitch & 63))
+        return cudaErrorInvalidValue;
+    // T: outputs per tile, so that the prefix reads of the last output group,
+    // up to P[T - 4 + (R + cpt - 1) + R + 4], stay inside P[0 .. NT cpt]
+    const int T = (wide_threads(pair) * cpt - 2 * R - cpt + 1) & ~3;
+    const int tiles = (n + T - 1) / T;
+    // bands of 64 rows unless set: many CTAs per SM over the launch, so that
+    // their 2R+1-row starts (independent loads) overlap other CTAs' scans
+    // (measured on 16384^2 and 32768^2 for R = 6..200: within a few percent of
+    // the best height everywhere)
+    int band = band_rows > 0 ? band_rows : 64;
+    band = std::max(band, (rows + 65534) / 65535);  // grid y limit
+    band = std::min(band + (band & 1), std::max(rows + (rows & 1), 2));  // even: row pairs never straddle bands
+    const dim3 grid(tiles, (rows + band - 1) / band);
+    const RuleScan q = make_rule_scan(rule, pair);
+    if (pair) return launch_wide_rm<true, 8>(cur, nxt, q, band, T, grid, s);  // R <= 90: cpt == 8
+    return cpt == 8 ? launch_wide_rm<false, 8>(cur, nxt, q, band, T, grid, s)
+                    : launch_wide_rm<false, 16>(cur, nxt, q, band, T, grid, s);
 }
 
 // ---------------------------------------------------------------------------

@@ -152,6 +152,10 @@ static int create_impl(ltl_ctx** out, int device, int rows, int n, int radius, i
         ltl_set_error("ltl_create: CUDA device %d not available (%d devices)", device, ndev);
         return LTL_ECUDA;
     }
+    if (variant == LTL_VARIANT_PLAIN && !plain_swar8_supported(radius) && !plain_generic_supported(radius)) {
+        ltl_set_error("ltl_create: plain variant needs radius <= 2038 (got %d)", radius);
+        return LTL_EUNSUPPORTED;
+    }
     if (variant == LTL_VARIANT_PACKED && !packed_supported(n, radius)) {
         ltl_set_error("ltl_create: packed variant needs radius <= 32 (got %d)", radius);
         return LTL_EUNSUPPORTED;
@@ -207,6 +211,8 @@ static int create_impl(ltl_ctx** out, int device, int rows, int n, int radius, i
         if (want > 1 && plain_tb_supported(radius, want) && H >= want * radius) depth = want;
         c->band_rows = (int)tuning_lookup("plain", radius, n, "band_rows", plain_swar8_band_rows(n, device));
         c->plain_wrap = plain_wrap_supported(n, rows);
+    } else if (variant == LTL_VARIANT_PLAIN) {
+        c->band_rows = (int)tuning_lookup("plain", radius, n, "band_rows", 0);  // 0: the launcher's choice
     }
     if (variant == LTL_VARIANT_PACKED) c->packed_band_rows = (int)tuning_lookup("packed", radius, n, "band_rows", 0);
     if (variant == LTL_VARIANT_PLAIN) e = plain_prepare(radius);
@@ -456,8 +462,8 @@ static cudaError_t enqueue_pass(ltl_ctx* c, int gens) {
                 e = launch_plain_swar8(a, b, c->rule, c->band_rows, c->plain_wrap, c->stream);
                 step_kernels = 1;
             } else {
-                e = launch_plain_generic(a, b, c->rule, c->stream);
-                step_kernels = 2;
+                e = launch_plain_generic(a, b, c->rule, c->band_rows, c->stream);
+                step_kernels = 1;
             }
             if (c->timing && e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
             // the SWAR kernels with plain_wrap read inner cells only: no halo to refresh
@@ -629,8 +635,9 @@ extern "C" int ltl_set_param(ltl_ctx* c, const char* name, long long value) {
             ltl_set_error("ltl_set_param: band_rows must be 0 (built-in choice) or in [16, 4096]");
             return LTL_EINVAL;
         }
-        if (c->variant == LTL_VARIANT_PLAIN)
+        if (c->variant == LTL_VARIANT_PLAIN && plain_swar8_supported(c->rule.radius))
             c->band_rows = value ? (int)value : plain_swar8_band_rows(c->n, c->device);
+        else if (c->variant == LTL_VARIANT_PLAIN) c->band_rows = (int)value;
         else if (c->variant == LTL_VARIANT_PACKED) c->packed_band_rows = (int)value;
         else {
             ltl_set_error("ltl_set_param: band_rows applies to the plain and packed variants");

@@ -31,10 +31,14 @@ cudaError_t plain_tb_prepare(int radius);
 cudaError_t launch_plain_tb(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows, int depth,
                             bool wrap, cudaStream_t s);
 
-// K1 generic path (any R): one fused kernel (vertical window sums in registers,
-// a prefix scan per row in shared memory, the rule); needs a halo of at least
-// R rounded up to 4.
-cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, cudaStream_t s);
+// K1 generic path (R up to 2038): one fused kernel (vertical window sums in
+// registers, a prefix scan per row, or per pair of rows, in shared memory, the
+// rule); needs a halo of at least R rounded up to plain_wide_cols_per_thread(R).
+// band_rows: rows per CTA (0: 64).
+bool plain_generic_supported(int radius);
+int plain_wide_cols_per_thread(int radius);
+cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule& rule, int band_rows,
+                                 cudaStream_t s);
 
 // K6: population and comparison over the inner n x n cells.  `scratch` holds
 // two uint64 (count, first index) in device memory.
