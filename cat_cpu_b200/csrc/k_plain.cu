@@ -673,6 +673,7 @@ __global__ void __launch_bounds__(wide_threads(PAIR))
 k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int rows, int H, size_t pitch,
              int band_rows, int T, RuleScan q) {
     constexpr int kWideThreads = wide_threads(PAIR);
+    static_assert(kWideThreads == 128 || kWideThreads == 256, "warp totals are read as one or two uint4");
     constexpr int L = kWideThreads * CPT;  // window columns per CTA
     constexpr int NW = CPT / 4;            // words of cells per thread and row; output groups per thread
     constexpr int EA = (RM + 1) & 3;       // (j - c0 + R + 1) mod 4
@@ -680,7 +681,7 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
     constexpr int STEP = PAIR ? 2 : 1;     // rows per iteration
     constexpr int PS = L + 4;              // words per P buffer
     __shared__ __align__(16) uint32_t P[2 * PS];
-    __shared__ uint32_t wsum[2][kWideThreads / 32];
+    __shared__ __align__(16) uint32_t wsum[2][kWideThreads / 32];
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
     const int R = q.radius;
     const uint32_t nlo0 = q.nlo0, hih0 = q.hih0, dnlo = (uint32_t)q.dnlo, dhih = (uint32_t)q.dhih;
@@ -823,12 +824,14 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
         incl = scan_up<16>(incl);
         if (lane == 31) wsum[b][wid] = incl;
         __syncthreads();
-        uint32_t wt = wsum[b][lane & (kWideThreads / 32 - 1)];
-        wt = scan_up<1>(wt);
-        wt = scan_up<2>(wt);
-        wt = scan_up<4>(wt);
-        const uint32_t wpre = __shfl_sync(0xffffffffu, wt, (wid + 31) & 31);  // total of warps < wid
-        const uint32_t off = incl - tot + (wid > 0 ? wpre : 0u);
+        // total of the warps before this one (4 or 8 warp totals, read as 16-byte vectors)
+        const uint4 w0 = *(const uint4*)wsum[b];
+        uint32_t wpre = (wid > 0 ? w0.x : 0u) + (wid > 1 ? w0.y : 0u) + (wid > 2 ? w0.z : 0u);
+        if constexpr (kWideThreads == 256) {
+            const uint4 w1 = *(const uint4*)(wsum[b] + 4);
+            wpre += (wid > 3 ? w0.w : 0u) + (wid > 4 ? w1.x : 0u) + (wid > 5 ? w1.y : 0u) + (wid > 6 ? w1.z : 0u);
+        }
+        const uint32_t off = incl - tot + wpre;
 #pragma unroll
         for (int k = 0; k < NW; ++k) {
             uint4 w;
