@@ -734,12 +734,20 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
     }
 
     // this thread's output groups: columns j0 + 4t + 4 NT g, g < NW (T < NT CPT)
+    // Row-pair mode keeps its output phase free of branches: a group past the
+    // tile reads P at group 0's offset minus 4t (a valid position) and stores
+    // nothing, and a group at the ragged right end of a row stores whole 4-byte
+    // words, whose bytes past column n - 1 land in the frame's right halo (which
+    // the halo fill after the step rewrites).  The 32-bit-lane mode, measured
+    // faster with branches, skips such groups and stores the ragged end bytewise.
     bool has[NW], full[NW];
+    int goff[NW];  // P offset of group g from group 0's
 #pragma unroll
     for (int g = 0; g < NW; ++g) {
         const int qq = 4 * t + 4 * kWideThreads * g;
         has[g] = qq < T && j0 + qq < n;
         full[g] = j0 + qq + 4 <= n;
+        goff[g] = (has[g] || !PAIR) ? 4 * kWideThreads * g : -4 * t;
     }
     const int dj = j0 - c0;  // in [R, R + CPT - 1], a multiple of 4
     const uint32_t* pe_sm = P + 4 * t + dj + R + 1 - EA;  // 16-byte aligned
@@ -848,10 +856,12 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
         const bool second = r + 1 < r1;
 #pragma unroll
         for (int g = 0; g < NW; ++g) {
-            if (!has[g]) break;
+            if constexpr (!PAIR) {
+                if (!has[g]) break;
+            }
             uint32_t pe[4], ps[4];
-            lds4<EA>(pe_sm + b * PS + 4 * kWideThreads * g, pe);
-            lds4<SA>(ps_sm + b * PS + 4 * kWideThreads * g, ps);
+            lds4<EA>(pe_sm + b * PS + goff[g], pe);
+            lds4<SA>(ps_sm + b * PS + goff[g], ps);
             uint8_t* yr = py + 4 * kWideThreads * g;
             const uint32_t cr = cen[g][0];
             uint32_t res[4];
@@ -872,15 +882,8 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
                 const uint32_t t23 = prmt<0x7351>(res[2], res[3]);
                 const uint32_t o0 = prmt<0x5410>(t01, t23) >> 7;
                 const uint32_t o1 = prmt<0x7632>(t01, t23) >> 7;
-                if (full[g]) {
-                    *(uint32_t*)yr = o0;
-                    if (second) *(uint32_t*)(yr + pp) = o1;
-                } else {
-                    for (int u = 0; u < n - j0 - 4 * t - 4 * kWideThreads * g; ++u) {
-                        yr[u] = (uint8_t)(o0 >> (8 * u));
-                        if (second) yr[pp + u] = (uint8_t)(o1 >> (8 * u));
-                    }
-                }
+                if (has[g]) *(uint32_t*)yr = o0;
+                if (has[g] && second) *(uint32_t*)(yr + pp) = o1;
             } else {
                 uint32_t sw[4];
                 sw[0] = prmt<0x4440>(cr, 0u);
