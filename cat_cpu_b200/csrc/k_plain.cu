@@ -583,10 +583,11 @@ cudaError_t launch_plain_tb(const Frame& cur, const Frame& nxt, const Rule& rule
 // centres selects them for both lanes at once.
 // ---------------------------------------------------------------------------
 constexpr int kWidePairMaxRadius = 90;  // (2R+1)^2 < 2^15
-// threads per CTA: 128 for row pairs (R <= 90: the window overhead 2R/(128 CPT)
-// stays small and a CTA's barrier waits for fewer warps), 256 above, where the
-// wider window keeps the overlap of neighbouring tiles down
-constexpr int wide_threads(bool pair) { return pair ? 128 : 256; }
+// threads per CTA: 128 up to R = 128 (the window overhead 2R/(128 CPT) stays
+// small and a CTA's barrier waits for fewer warps), 256 above, where the wider
+// window keeps the overlap of neighbouring tiles down
+constexpr int kWideNarrowMaxRadius = 128;
+inline int wide_threads(int radius) { return radius <= kWideNarrowMaxRadius ? 128 : 256; }
 
 struct RuleScan {
     int radius;
@@ -668,11 +669,11 @@ __device__ __forceinline__ void lds4(const uint32_t* p, uint32_t (&v)[4]) {
 // PAIR: two rows per iteration in 16-bit lanes (R <= 90); CPT: window columns
 // per thread (8 or 16); RM = R mod 4 fixes the alignment of the two prefix
 // reads of every output group.
-template <bool PAIR, int CPT, int RM>
-__global__ void __launch_bounds__(wide_threads(PAIR))
+template <bool PAIR, int CPT, int RM, int NT>
+__global__ void __launch_bounds__(NT)
 k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int rows, int H, size_t pitch,
              int band_rows, int T, RuleScan q) {
-    constexpr int kWideThreads = wide_threads(PAIR);
+    constexpr int kWideThreads = NT;
     static_assert(kWideThreads == 128 || kWideThreads == 256, "warp totals are read as one or two uint4");
     constexpr int L = kWideThreads * CPT;  // window columns per CTA
     constexpr int NW = CPT / 4;            // words of cells per thread and row; output groups per thread
@@ -938,18 +939,18 @@ int plain_wide_cols_per_thread(int radius) { return radius <= 1018 ? 8 : 16; }
 
 bool plain_generic_supported(int radius) { return radius >= 1 && radius <= 2038; }
 
-template <bool PAIR, int CPT>
+template <bool PAIR, int CPT, int NT>
 static cudaError_t launch_wide_rm(const Frame& cur, const Frame& nxt, const RuleScan& q, int band, int T,
                                   dim3 grid, cudaStream_t s) {
-    const dim3 block(wide_threads(PAIR));
+    const dim3 block(NT);
     const int n = cur.n, rows = cur.nrows();
     const uint8_t* x = cur.base;
     uint8_t* y = nxt.base;
     switch (q.radius & 3) {
-        case 0: k_plain_wide<PAIR, CPT, 0><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
-        case 1: k_plain_wide<PAIR, CPT, 1><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
-        case 2: k_plain_wide<PAIR, CPT, 2><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
-        default: k_plain_wide<PAIR, CPT, 3><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
+        case 0: k_plain_wide<PAIR, CPT, 0, NT><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
+        case 1: k_plain_wide<PAIR, CPT, 1, NT><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
+        case 2: k_plain_wide<PAIR, CPT, 2, NT><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
+        default: k_plain_wide<PAIR, CPT, 3, NT><<<grid, block, 0, s>>>(x, y, n, rows, cur.H, cur.pitch, band, T, q); break;
     }
     return cudaGetLastError();
 }
@@ -964,7 +965,8 @@ cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule&
         return cudaErrorInvalidValue;
     // T: outputs per tile, so that the prefix reads of the last output group,
     // up to P[T - 4 + (R + cpt - 1) + R + 4], stay inside P[0 .. NT cpt]
-    const int T = (wide_threads(pair) * cpt - 2 * R - cpt + 1) & ~3;
+    const int nt = wide_threads(R);
+    const int T = (nt * cpt - 2 * R - cpt + 1) & ~3;
     const int tiles = (n + T - 1) / T;
     // bands of 64 rows unless set: many CTAs per SM over the launch, so that
     // their 2R+1-row starts (independent loads) overlap other CTAs' scans
@@ -975,9 +977,11 @@ cudaError_t launch_plain_generic(const Frame& cur, const Frame& nxt, const Rule&
     band = std::min(band + (band & 1), std::max(rows + (rows & 1), 2));  // even: row pairs never straddle bands
     const dim3 grid(tiles, (rows + band - 1) / band);
     const RuleScan q = make_rule_scan(rule, pair);
-    if (pair) return launch_wide_rm<true, 8>(cur, nxt, q, band, T, grid, s);  // R <= 90: cpt == 8
-    return cpt == 8 ? launch_wide_rm<false, 8>(cur, nxt, q, band, T, grid, s)
-                    : launch_wide_rm<false, 16>(cur, nxt, q, band, T, grid, s);
+    // R <= 90: row pairs, cpt 8, 128 threads; R <= 128: 128 threads; R <= 1018: cpt 8
+    if (pair) return launch_wide_rm<true, 8, 128>(cur, nxt, q, band, T, grid, s);
+    if (nt == 128) return launch_wide_rm<false, 8, 128>(cur, nxt, q, band, T, grid, s);
+    return cpt == 8 ? launch_wide_rm<false, 8, 256>(cur, nxt, q, band, T, grid, s)
+                    : launch_wide_rm<false, 16, 256>(cur, nxt, q, band, T, grid, s);
 }
 
 // ---------------------------------------------------------------------------
