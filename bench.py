@@ -252,19 +252,22 @@ def e2e_run(C, torch, name, start, steps):
 def radius_sweep(C, torch, args):
     """The radius-sweep workloads: 32768^2, seed 2, d = 0.5, R in {1,2,4,8,16,32},
     scaled interval rule, and R in {64,128} at d = 0.3 (seed 3).  One JSON line per
-    radius with every variant's GCUPS (kernel passes timed with CUDA events on the
-    launching stream, L2 flushed before each pass).  Exactness at these sizes is
-    covered by tests/test_gpu_fullsize.py."""
+    radius with every variant's GCUPS (passes timed with CUDA events on the
+    launching stream, L2 flushed before each pass), the step kernel's own GCUPS
+    (halo launches excluded) and its HBM roofline at 2 B (uint8) or 0.25 B
+    (packed) per cell-update.  Exactness at these sizes is covered by
+    tests/test_gpu_fullsize.py."""
     from cat_cpu_b200.workloads import scaled_rule
     n = 32768
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     vcodes = {"plain": C.VARIANT_PLAIN, "packed": C.VARIANT_PACKED, "tensor": C.VARIANT_TENSOR}
+    peak, peak_kind = measured_peaks()
     for radius, seed, dens in [(1, 2, 0.5), (2, 2, 0.5), (4, 2, 0.5), (8, 2, 0.5), (16, 2, 0.5), (32, 2, 0.5),
                                (64, 3, 0.3), (128, 3, 0.3)]:
         rule = scaled_rule(radius)
         start = C.start_grid(n, seed, dens, 1)
         out = {"workload": f"{n}x{n} torus, R={radius}, scaled interval rule, seed {seed}, d={dens}",
-               "radius": radius, "unit": "GCUPS", "variants": {}}
+               "radius": radius, "unit": "GCUPS", "peak_kind": f"{peak_kind} hbm_gbs", "variants": {}}
         for name in [v for v in args.variants.split(",") if v]:
             try:
                 s = C.CUDASolver(n, radius, rule, variant=vcodes[name])
@@ -281,6 +284,7 @@ def radius_sweep(C, torch, args):
                 passes = max(1, min(args.sweep_steps, 200) // depth)
                 ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                       for _ in range(passes)]
+                s.set_timing(True)
                 with torch.cuda.stream(stream):
                     for a, b in ev:
                         flush.zero_()
@@ -289,10 +293,19 @@ def radius_sweep(C, torch, args):
                         b.record(stream)
                 stream.synchronize()
                 ms = sum(a.elapsed_time(b) for a, b in ev)
+                kernel_ms, kernel_launches, _ = s.get_timing()
+                s.set_timing(False)
                 gens = passes * depth
+                # roofline of the step kernel alone (halo launches excluded):
+                # algorithmic bytes per cell-update x cell-updates / kernel time
+                achieved = n * n * gens * BYTES_PER_UPDATE[name] / (kernel_ms * 1e-3) / 1e9
                 out["variants"][name] = {"gcups": round(n * n * gens / (ms * 1e-3) / 1e9, 2),
+                                         "kernel_gcups": round(n * n * gens / (kernel_ms * 1e-3) / 1e9, 2),
                                          "ms_per_generation": round(ms / gens, 4), "temporal_depth": depth,
-                                         "generations": gens, "population": s.population()}
+                                         "generations": gens, "population": s.population(),
+                                         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                                                      "unit": "GB/s", "frac": round(achieved / peak, 4),
+                                                      "bytes_per_update": BYTES_PER_UPDATE[name]}}
             finally:
                 s.close()
         print(json.dumps(out), flush=True)
