@@ -721,14 +721,23 @@ k_plain_wide(const uint8_t* __restrict__ X, uint8_t* __restrict__ Y, int n, int 
                 V[2 * k + 1] = prmt<0x4342>(acc[k], 0u);
             }
         } else {
+            // byte lanes over chunks of at most 255 rows, widened once per chunk
+            for (int dy0 = -R; dy0 <= R; dy0 += 255) {
+                const int cnt = min(255, R - dy0 + 1);
+                uint32_t acc[NW];
+#pragma unroll
+                for (int k = 0; k < NW; ++k) acc[k] = 0u;
 #pragma unroll 8
-            for (int dy = -R; dy <= R; ++dy, p += pp) {
-                uint32_t x[NW];
-                ld_cells<CPT>(p, x);
+                for (int i = 0; i < cnt; ++i, p += pp) {
+                    uint32_t x[NW];
+                    ld_cells<CPT>(p, x);
+#pragma unroll
+                    for (int k = 0; k < NW; ++k) acc[k] += x[k];
+                }
 #pragma unroll
                 for (int k = 0; k < NW; ++k) {
-                    V[2 * k] += prmt<0x4140>(x[k], 0u);
-                    V[2 * k + 1] += prmt<0x4342>(x[k], 0u);
+                    V[2 * k] += prmt<0x4140>(acc[k], 0u);
+                    V[2 * k + 1] += prmt<0x4342>(acc[k], 0u);
                 }
             }
         }
