@@ -4,17 +4,20 @@ The reference has no checkpoint format; this one is defined here.  A file is
 
     8 bytes   magic b"LTLCKPT1"
     4 bytes   header length L (little-endian uint32)
-    L bytes   UTF-8 JSON header: n, radius, rule (centre-excluded smin, smax,
-              bmin, bmax), generation, words_per_row, payload_sha256, and any
-              caller metadata under "meta"
-    payload   the grid in the PACK coding: n rows of words_per_row = ceil(n/64)
-              little-endian uint64, cell (i, j) = bit j % 64 of word j / 64, bits
-              past n zero (the layout of ltl_pack_device)
+    L bytes   UTF-8 JSON header: n (columns), rows, radius, rule
+              (centre-excluded smin, smax, bmin, bmax), generation,
+              words_per_row, payload_sha256, and any caller metadata under "meta"
+    payload   the grid in the PACK coding: `rows` rows of words_per_row =
+              ceil(n/64) little-endian uint64, cell (i, j) = bit j % 64 of word
+              j / 64, bits past n zero (the layout of ltl_pack_device)
 
-so a 32768^2 grid takes 128 MiB instead of 1 GiB.  On the device path the grid
+so a 32768^2 grid takes 128 MiB instead of 1 GiB.  `rows` equals n for the
+square tori of ltl_create and differs for the row strips of ltl_create_rect; a
+header without it (older files) means rows = n.  On the device path the grid
 is packed by ltl_pack_device before the download and unpacked by
 ltl_unpack_device after the upload, so only the packed bytes cross PCIe.
-`read` checks the magic, the sizes and the payload's SHA-256.
+`read` checks the magic, the sizes and the payload's SHA-256; `load` refuses a
+solver whose n, rows, radius or rule differ from the header's.
 """
 import ctypes
 import hashlib
@@ -48,17 +51,18 @@ def unpack_host(words, n):
     return b[:, :n].astype(np.uint8)
 
 
-def _header(n, radius, rule, generation, payload, meta):
-    return {"n": int(n), "radius": int(radius), "rule": [int(x) for x in rule], "generation": int(generation),
-            "words_per_row": words_per_row(n), "payload_sha256": hashlib.sha256(payload).hexdigest(),
-            "meta": meta or {}}
+def _header(n, radius, rule, generation, payload, meta, rows):
+    return {"n": int(n), "rows": int(rows), "radius": int(radius), "rule": [int(x) for x in rule],
+            "generation": int(generation), "words_per_row": words_per_row(n),
+            "payload_sha256": hashlib.sha256(payload).hexdigest(), "meta": meta or {}}
 
 
-def write(path, words, n, radius, rule, generation=0, meta=None):
+def write(path, words, n, radius, rule, generation=0, meta=None, rows=None):
+    rows = n if rows is None else int(rows)
     payload = np.ascontiguousarray(words, dtype="<u8").tobytes()
-    if len(payload) != n * words_per_row(n) * 8:
-        raise ValueError("payload size does not match n")
-    head = json.dumps(_header(n, radius, rule, generation, payload, meta), sort_keys=True).encode()
+    if len(payload) != rows * words_per_row(n) * 8:
+        raise ValueError("payload size does not match rows x n")
+    head = json.dumps(_header(n, radius, rule, generation, payload, meta, rows), sort_keys=True).encode()
     with open(path, "wb") as f:
         f.write(MAGIC)
         f.write(struct.pack("<I", len(head)))
@@ -67,8 +71,9 @@ def write(path, words, n, radius, rule, generation=0, meta=None):
 
 
 def read(path):
-    """-> (header dict, uint64 words of shape (n, words_per_row)).  Raises ValueError on
-    a bad magic, a truncated file or a checksum mismatch."""
+    """-> (header dict, uint64 words of shape (rows, words_per_row)).  Raises ValueError
+    on a bad magic, a truncated file or a checksum mismatch.  The header always
+    carries "rows" (n for files written without it)."""
     with open(path, "rb") as f:
         if f.read(8) != MAGIC:
             raise ValueError(f"{path}: not a grid checkpoint")
@@ -76,49 +81,65 @@ def read(path):
         head = json.loads(f.read(hl).decode())
         payload = f.read()
     n, wpr = head["n"], head["words_per_row"]
-    if wpr != words_per_row(n) or len(payload) != n * wpr * 8:
+    rows = head.setdefault("rows", n)
+    if wpr != words_per_row(n) or len(payload) != rows * wpr * 8:
         raise ValueError(f"{path}: truncated or inconsistent checkpoint")
     if hashlib.sha256(payload).hexdigest() != head["payload_sha256"]:
         raise ValueError(f"{path}: checksum mismatch")
-    return head, np.frombuffer(payload, dtype="<u8").reshape(n, wpr).copy()
+    return head, np.frombuffer(payload, dtype="<u8").reshape(rows, wpr).copy()
 
 
 def save(path, solver, generation=0, meta=None):
-    """Write `solver`'s current grid.  Packs on the device (ltl_pack_device) and
-    downloads the packed words only."""
+    """Write `solver`'s current grid (rows x n; rows = n unless the solver is a
+    rectangular strip).  Packs on the device (ltl_pack_device) and downloads the
+    packed words only."""
     import torch
     from . import ltl
     n = solver.n
+    rows = getattr(solver, "rows", n)
     wpr = words_per_row(n)
     dev = torch.device("cuda", solver.device)
-    cells = torch.empty((n, n), dtype=torch.uint8, device=dev)
-    words = torch.empty((n, wpr), dtype=torch.int64, device=dev)
+    cells = torch.empty((rows, n), dtype=torch.uint8, device=dev)
+    words = torch.empty((rows, wpr), dtype=torch.int64, device=dev)
     torch.cuda.synchronize(dev)
     solver.download_device(cells.data_ptr(), n)
     solver.synchronize()
-    ltl.check(ltl.lib().ltl_pack_device(ctypes.c_void_p(cells.data_ptr()), n, n, n,
+    ltl.check(ltl.lib().ltl_pack_device(ctypes.c_void_p(cells.data_ptr()), n, rows, n,
                                         ctypes.c_void_p(words.data_ptr()), wpr * 8, None))
     torch.cuda.synchronize(dev)
     host = words.cpu().numpy().view("<u8")
-    write(path, host, n, solver.radius, solver.rule, generation, meta)
+    write(path, host, n, solver.radius, solver.rule, generation, meta, rows=rows)
+
+
+def check_compatible(head, solver):
+    """Raise ValueError unless `solver` has the checkpoint's shape, radius and rule:
+    restoring a grid into a solver with another rule would step it under that rule."""
+    want = (head["n"], head["rows"], head["radius"], tuple(head["rule"]))
+    have = (solver.n, getattr(solver, "rows", solver.n), solver.radius, tuple(solver.rule))
+    for name, a, b in zip(("n", "rows", "radius", "rule"), want, have):
+        if a != b:
+            raise ValueError(f"checkpoint holds {name}={a}, solver has {name}={b}")
 
 
 def load(path, solver=None, variant=None, device=0):
-    """Restore a checkpoint into `solver` (same n), or into a new CUDASolver built
-    from the header.  Returns (solver, header)."""
+    """Restore a checkpoint into `solver` (same n, rows, radius and rule, else
+    ValueError), or into a new CUDASolver built from the header (a rectangular
+    one for a strip).  Returns (solver, header)."""
+    head, host = read(path)
+    n, rows = head["n"], head["rows"]
+    if solver is not None:
+        check_compatible(head, solver)
     import torch
     from . import ltl
-    head, host = read(path)
-    n = head["n"]
     if solver is None:
         kw = {} if variant is None else {"variant": variant}
+        if rows != n:
+            kw["rows"] = rows
         solver = ltl.CUDASolver(n, head["radius"], tuple(head["rule"]), device=device, **kw)
-    elif solver.n != n:
-        raise ValueError(f"checkpoint holds n={n}, solver has n={solver.n}")
     dev = torch.device("cuda", solver.device)
     words = torch.from_numpy(host.view(np.int64)).to(dev)
-    cells = torch.empty((n, n), dtype=torch.uint8, device=dev)
-    ltl.check(ltl.lib().ltl_unpack_device(ctypes.c_void_p(words.data_ptr()), head["words_per_row"] * 8, n, n,
+    cells = torch.empty((rows, n), dtype=torch.uint8, device=dev)
+    ltl.check(ltl.lib().ltl_unpack_device(ctypes.c_void_p(words.data_ptr()), head["words_per_row"] * 8, rows, n,
                                           ctypes.c_void_p(cells.data_ptr()), n, None))
     torch.cuda.synchronize(dev)
     solver.upload_device(cells.data_ptr(), n)

@@ -23,7 +23,9 @@
 
 namespace ltl {
 
-// 32 MiB: two halo'd grids up to n = 4000 (R <= 5), smaller n for larger R.
+// 32 MiB: two halo'd grids.  A grid needs round_up((n + 2H + 1) * pitch, 256)
+// bytes with H = halo_for(R, 1) and pitch = round_up(n + 2H + 16, 64), so the
+// limit is n <= 4048 for R <= 16 (H = 16) and smaller n for larger R.
 constexpr size_t kNoAllocScratchBytes = 32ull << 20;
 
 // The scratch.  Host code only sees a host-side stand-in for this symbol; the
@@ -101,8 +103,15 @@ extern "C" int ltl_step_noalloc(const uint8_t* dev_in, size_t in_pitch, uint8_t*
     const Rule rule{radius, smin, smax, bmin, bmax};
     int band_rows = 0;
     if (!generic) band_rows = (int)tuning_lookup("plain", radius, n, "band_rows", plain_swar8_band_rows(n, device));
-    // The frames need no clearing: every cell a kernel reads is written first
-    // (inner cells by the copy, halo cells by the halo fill).
+    // The frames are not cleared.  The inner cells are written by the copy and
+    // the halo by the halo fill before any step reads them.  The kernels also
+    // read bytes outside the halo'd grid (the wide kernel's loads past the right
+    // halo into the pitch padding, the SWAR kernel's vector loads into the spare
+    // row) and discard what they compute from them; those bytes hold whatever an
+    // earlier call with another n left there.  That is safe because every byte
+    // ever written to this array is a 0/1 cell, so the byte-lane sums that touch
+    // stale bytes cannot carry into the lanes that are kept.  A kernel that
+    // writes anything other than 0/1 cells here would break that.
     e = launch_copy_in(fa, dev_in, in_pitch, s);
     if (e == cudaSuccess) e = launch_halo_fill(fa, s);
     Frame* cur = &fa;

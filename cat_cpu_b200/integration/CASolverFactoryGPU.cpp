@@ -4,8 +4,9 @@
 // bit-packed); every other code goes to the reference's own factory
 // (src/CellularAutomata/CASolverFactory.cpp:6-121), reached here under the
 // name ltl_reference_createSolver.  In the reference tree a maintainer would
-// instead add the three `case` blocks to that switch; the
-// renamed symbol lets the test build link both without editing its sources.
+// instead add the three `case` blocks (codes 7, 8, 9, each returning a
+// CUDASolver) to that switch; the renamed symbol lets the test build link both
+// without editing the reference's sources.
 #include "CellularAutomata/CASolverFactory.h"
 #include "CUDASolver.h"
 #include "Memory/Allocators/CPUAllocator.h"

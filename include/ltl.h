@@ -213,7 +213,9 @@ int ltl_get_timing(ltl_ctx* ctx, double* step_kernel_ms, long long* step_kernel_
  * the current device.  It calls no cudaMalloc/cudaFree: the two halo'd grids it
  * needs live in a fixed 32 MiB array in device memory that every GPU loading
  * the library holds until the process exits.  Grids needing more return
- * LTL_EINVAL with a message (R <= 5: n up to 4000; larger R: smaller n).
+ * LTL_EINVAL with a message: a grid takes round_up((n + 2H + 1) * pitch, 256)
+ * bytes, H = 16 for R <= 16 (32 up to R = 32, ...), pitch = round_up(n + 2H + 16,
+ * 64), and two must fit, so n <= 4048 for R <= 16 and less for larger R.
  * The first call on a device looks up that array's address and sets the
  * kernels' shared-memory limits; make that first call before any stream
  * capture.  All calls share the one array and it keeps the last call's data:

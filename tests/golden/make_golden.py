@@ -1,7 +1,8 @@
 """Generate tests/golden/golden.json from the reference's own CPU solvers.
 
-Run in a container that has the reference sources (kezada94/CAT_cpu) at
-$LTL_REFERENCE (default /root/reference):
+Run where the reference sources (kezada94/CAT_cpu) are present, with
+$LTL_REFERENCE naming their directory (the script's built-in default is the
+directory they were mounted at when the fixtures were made):
 
     python tests/golden/make_golden.py [--jobs 8] [--only NAME_SUBSTRING]
 

@@ -51,6 +51,81 @@ def test_corrupt_file_is_rejected(tmp_path):
         ck.read(p)
 
 
+def test_rectangular_grid_roundtrip(tmp_path):
+    rows, n = 37, 130
+    rng = np.random.default_rng(5)
+    g = (rng.random((rows, n)) < 0.5).astype(np.uint8)
+    p = os.path.join(tmp_path, "strip.ckpt")
+    ck.write(p, ck.pack_host(g), n, 3, (2, 3, 3, 3), rows=rows)
+    head, words = ck.read(p)
+    assert (head["n"], head["rows"]) == (n, rows) and words.shape == (rows, 3)
+    assert np.array_equal(ck.unpack_host(words, n), g)
+    with pytest.raises(ValueError, match="rows x n"):
+        ck.write(p, ck.pack_host(g), n, 3, (2, 3, 3, 3))  # rows defaults to n: sizes disagree
+
+
+def test_header_without_rows_means_square(tmp_path):
+    import json
+    import struct
+    n = 40
+    g = np.eye(n, dtype=np.uint8)
+    p = os.path.join(tmp_path, "old.ckpt")
+    ck.write(p, ck.pack_host(g), n, 2, (1, 2, 3, 4))
+    raw = open(p, "rb").read()
+    (hl,) = struct.unpack("<I", raw[8:12])
+    head = json.loads(raw[12:12 + hl])
+    del head["rows"]
+    h2 = json.dumps(head, sort_keys=True).encode()
+    open(p, "wb").write(raw[:8] + struct.pack("<I", len(h2)) + h2 + raw[12 + hl:])
+    head, words = ck.read(p)
+    assert head["rows"] == n and np.array_equal(ck.unpack_host(words, n), g)
+
+
+class _FakeSolver:
+    def __init__(self, n, rows, radius, rule):
+        self.n, self.rows, self.radius, self.rule = n, rows, radius, rule
+
+
+@pytest.mark.parametrize("field,fake", [
+    ("n", _FakeSolver(65, 64, 5, (32, 56, 34, 45))),
+    ("rows", _FakeSolver(64, 80, 5, (32, 56, 34, 45))),
+    ("radius", _FakeSolver(64, 64, 4, (32, 56, 34, 45))),
+    ("rule", _FakeSolver(64, 64, 5, (32, 57, 34, 45))),
+])
+def test_load_refuses_incompatible_solver(tmp_path, field, fake):
+    """load() checks the header against an existing solver before touching the
+    device: a grid restored under another radius or rule would be stepped wrongly."""
+    g = np.zeros((64, 64), dtype=np.uint8)
+    p = os.path.join(tmp_path, "g.ckpt")
+    ck.write(p, ck.pack_host(g), 64, 5, (32, 56, 34, 45))
+    with pytest.raises(ValueError, match=field):
+        ck.load(p, solver=fake)
+
+
+@pytest.mark.gpu
+def test_rect_solver_save_load(tmp_path):
+    import cat_cpu_b200 as C
+    rows, n, r, rule = 90, 200, 3, (7, 14, 8, 12)
+    g0 = (np.random.default_rng(2).random((rows, n)) < 0.5).astype(np.uint8)
+    a = C.CUDASolver(n, r, rule, variant=C.VARIANT_PLAIN, rows=rows)
+    p = os.path.join(tmp_path, "strip.ckpt")
+    try:
+        a.setState(g0)
+        a.doSteps(3)
+        want = a.getCurrentState()
+        ck.save(p, a, generation=3)
+    finally:
+        a.close()
+    head, words = ck.read(p)
+    assert head["rows"] == rows and np.array_equal(ck.unpack_host(words, n), want)
+    b, head = ck.load(p)
+    try:
+        assert (b.rows, b.n) == (rows, n)
+        assert np.array_equal(b.getCurrentState(), want)
+    finally:
+        b.close()
+
+
 @pytest.mark.gpu
 def test_save_load_continue_matches_uninterrupted(tmp_path):
     import cat_cpu_b200 as C

@@ -77,6 +77,21 @@ def test_noalloc_in_place_and_stream():
     assert np.array_equal(buf.cpu().numpy(), want)
 
 
+def test_noalloc_size_limit_is_the_documented_bound():
+    """n = 4048 at R = 5 fits the two halo'd grids of the 32 MiB scratch; 4049 does not."""
+    import torch
+    import cat_cpu_b200 as C
+    L = C.lib()
+    for n, want in ((4048, 0), (4049, C.ltl.EINVAL)):
+        dev = torch.zeros((n, n), dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        rc = L.ltl_step_noalloc(ctypes.c_void_p(dev.data_ptr()), n, ctypes.c_void_p(dev.data_ptr()), n, n, 5, 32,
+                                56, 34, 45, 1, None)
+        torch.cuda.synchronize()
+        assert rc == want, (n, L.ltl_last_error())
+        del dev
+
+
 def test_noalloc_rejects_grids_beyond_its_scratch():
     import torch
     import cat_cpu_b200 as C
