@@ -1,270 +1,104 @@
 // k_tensor.cu -- K2: the LtL step as two banded 0/1 matrix products on the
-// 5th-generation tensor cores (tcgen05, kind::i8, accumulators in TMEM).
+// 5th-generation tensor cores (tcgen05, kind::i8, accumulators in TMEM), on a
+// bit-packed grid (32 cells per 32-bit word, the PACK coding).
 //
 // This is the reference's AMX formulation (kezada94/CAT_cpu,
 // src/CellularAutomata/Solvers/AMXSolver16.cpp:63-138 band tiles, :254-309 row
 // sums X*B, :322-384 column sums + rule) re-designed for sm_100a:
-//   - one CTA owns a tile of Tr x Tc output cells.  TMA brings the halo'd input
-//     tile X (128 rows x 256 bytes, two 128-byte swizzle atoms) into shared memory;
+//   - one CTA per SM walks a strided list of output tiles of Tr x Tc cells;
+//   - unpack warps read the tile's packed input words (rows and words taken
+//     modulo n: the torus wrap happens here, so no halo pass runs between
+//     generations) and spread every bit to a byte in shared memory, in the
+//     128-byte-swizzled K-major layout the MMA reads (128 rows x 256 columns);
 //   - product 1:  H = X * B_h   (row sums; M = 128 tile rows, N = 32-column
-//     chunks, K = a 64-column window; u8 x u8 -> s32 in TMEM).  B_h is the 0/1
-//     band |k - PADC - n| <= R, built once per CTA in shared memory;
+//     chunks, K = the chunk's column window; u8 x u8 -> s32 in TMEM);
 //   - H (<= 2R+1) is read back with tcgen05.ld, re-quantised to u8 and stored
 //     as the MN-major B operand of
-//   - product 2:  C = B_v * H   (column sums; M = 128, N = Tc, K = 128) with the
-//     band B_v[m][k] = [m <= k <= m + 2R], so the reference's transposed
-//     scatter between the two products (AMXSolver.cpp:321-325) disappears;
-//   - epilogue: C is the box count including the centre, the birth/survival
-//     interval rule (HostSolver.tpp:47-73, k = C - centre) is applied four
-//     cells per register, and the uint8 result goes straight to global memory.
-// Exactness: inputs are 0/1, H <= 2R+1 <= 255 fits u8, C <= (2R+1)^2 in s32.
+//   - product 2:  C = B_v * H   (column sums; M = 128, N = Tc, K = 128) with
+//     B_v[m][k] = [m <= k <= m + 2R], so the reference's transposed scatter
+//     between the two products (AMXSolver.cpp:321-325) disappears;
+//   - epilogue: C is the box count including the centre; the birth/survival
+//     interval rule (HostSolver.tpp:47-73, k = C - centre) runs on four 8-bit
+//     (R <= 5) or two 16-bit lanes per register, and the result bits are
+//     gathered straight into the output word.
 //
-// Every wait on an mbarrier is bounded (globaltimer); on timeout the kernel
-// sets a bit in an error word that the host reads (ltl_synchronize), finishes
-// waiting for its own TMA copy (also bounded), frees its TMEM and returns.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
+// Column order.  A packed word w spreads to bytes with (w >> k) & 0x01010101,
+// k = 0..7: register k holds cells k, 8+k, 16+k, 24+k.  The shared-memory tile
+// keeps that order: within each 32-column group, byte position 4k+j holds the
+// group's cell 8j+k (the permutation pi(4k+j) = 8j+k).  Product 1 contracts over
+// the positions, so B_h's rows follow pi, and its columns (the N order of H
+// and C) are chosen so that the rule's result bits land in the output word's
+// own bit order with one shift per register (sigma below).  No byte is moved
+// to undo the permutation.
+//
+// Exactness: inputs are 0/1, H <= 2R+1 <= 65 fits u8, C <= (2R+1)^2 in s32.
+//
+// Every wait on an mbarrier is bounded (globaltimer, hardware-suspended
+// tries); on timeout the kernel sets a bit in an error word that the host
+// reads (ltl_synchronize), waits (bounded) for its own MMAs, frees its TMEM and
+// returns.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
 
 #include "ltl_kernels.h"
+#include "tc_ptx.cuh"
 
 namespace ltl {
 
-// ---------------------------------------------------------------------------
-// PTX helpers (sm_100a)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ uint64_t globaltimer() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(phase)
-        : "memory");
-    return done != 0;
-}
-
-// Bounded wait for `phase` of `bar`: false after `limit_ns` of wall time.  The
-// clock is read once per 16 tries, so that a waiting warp spends few issue
-// slots per try; `sleep_ns` > 0 backs off between tries (for warps whose wait
-// is not on the critical path).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint64_t limit_ns, uint32_t sleep_ns = 0) {
-    if (mbar_try(bar, phase)) return true;
-    const uint64_t t0 = globaltimer();
-    while (true) {
-#pragma unroll 4
-        for (int i = 0; i < 16; ++i) {
-            if (mbar_try(bar, phase)) return true;
-            if (sleep_ns) __nanosleep(sleep_ns);
-        }
-        if (globaltimer() - t0 > limit_ns) return false;
-    }
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
-            "r"(smem_u32(dst)),
-        "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
-        : "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)),
-                 "r"(ncols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
-}
-
-__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
-                                       uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-// 16 consecutive TMEM columns of this thread's lane, packed in pairs
-// (.pack::16b): register k holds the low 16 bits of column 2k in its low half
-// and those of column 2k + 1 in its high half.  Every accumulator read here
-// fits 16 bits: row sums are <= 2R + 1 and box counts <= (2R + 1)^2 < 2^16 for
-// R <= 32.  The registers are defined only after tmem_wait8 on the same array:
-// the wait takes them as read-write operands so that the compiler cannot move
-// a use of them above it.
-__device__ __forceinline__ void tmem_ld16p(uint32_t taddr, uint32_t (&v)[8]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.pack::16b.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-                 : "r"(taddr));
-}
-
-// Waits for every tcgen05.ld this thread issued.
-__device__ __forceinline__ void tmem_wait8(uint32_t (&v)[8]) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;"
-                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7])
-                 :
-                 : "memory");
-}
-
-// Bytes 0 and 2 of a and of b: the low bytes of the four 16-bit values of two
-// packed registers, in column order.
-__device__ __forceinline__ uint32_t low_bytes4(uint32_t a, uint32_t b) { return __byte_perm(a, b, 0x6420); }
-
-// Walks this warp's 16-column chunks of a TMEM accumulator row, loading chunk
-// c + 1 while f(values, column) processes chunk c.  The chunks are the halves
-// of 32-column blocks grp, grp + groups, grp + 2*groups, ... below `cols`;
-// `max_chunks` bounds the unrolled loop.  Every argument is warp-uniform, as
-// tcgen05.ld requires.
-template <int max_chunks, class F>
-__device__ __forceinline__ void tmem_walk16(uint32_t trow, int grp, int groups, int cols, F&& f) {
-    const int blocks = grp * 32 < cols ? (cols / 32 - grp + groups - 1) / groups : 0;
-    const int nc = 2 * blocks < max_chunks ? 2 * blocks : max_chunks;
-    auto col = [&](int c) { return 32 * (grp + groups * (c >> 1)) + 16 * (c & 1); };
-    if (nc == 0) return;
-    uint32_t a[8], b[8];
-    tmem_ld16p(trow + col(0), a);
-    tmem_wait8(a);
-#pragma unroll
-    for (int c = 0; c < max_chunks; ++c) {
-        if (c < nc) {
-            const bool more = c + 1 < nc;
-            if ((c & 1) == 0) {
-                if (more) tmem_ld16p(trow + col(c + 1), b);
-                f(a, col(c));
-                if (more) tmem_wait8(b);
-            } else {
-                if (more) tmem_ld16p(trow + col(c + 1), a);
-                f(b, col(c));
-                if (more) tmem_wait8(a);
-            }
-        }
-    }
-}
-
-// Shared-memory matrix descriptors (tcgen05 "version 1" format).
-// K-major, 128-byte swizzle: 8-row atoms of 1024 B (SBO), LBO unused.
-__device__ __forceinline__ uint64_t desc_k_sw128(uint32_t addr) {
-    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) |
-           ((uint64_t)1u << 46) | ((uint64_t)2u << 61);
-}
-// No swizzle ("interleave"): 8 x 16-byte core matrices stored as 128 contiguous
-// bytes; `lbo` / `sbo` are the byte strides between core matrices along the
-// leading / strided dimension.
-__device__ __forceinline__ uint64_t desc_noswz(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1u << 46);
-}
-
-// Instruction descriptor: kind::i8, u8 x u8 -> s32, M = 128.
-__host__ __device__ constexpr uint32_t idesc_u8(int N, bool b_mn_major) {
-    return (2u << 4)                       // D format s32
-           | (0u << 7) | (0u << 10)        // A, B unsigned 8-bit
-           | (0u << 15)                    // A K-major
-           | ((b_mn_major ? 1u : 0u) << 16)
-           | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-}
+using namespace tc;
 
 // ---------------------------------------------------------------------------
-// Tile geometry and the persistent, warp-specialised kernel
-//
-// One CTA per SM walks a strided list of tiles.  Warp roles:
-//   warp 0    TMA producer: X tiles into a kXStages ring (x_full / x_empty);
-//   warp 1    MMA issuer, per tile j:  product 2 of tile j-1 (once H(j-1) is in
-//             shared memory and C of tile j-2 has been read), then product 1 of
-//             tile j (H's TMEM columns are free as soon as H(j-1) was read);
-//   warps 2.. epilogue: kEpiGroups groups of 4 warps (one warp per TMEM lane
-//             quarter); group g handles the 32-column blocks g, g + kEpiGroups,
-//             ... of every tile: re-quantise H(j), then rule + store C(j).
-// TMEM holds H (columns [0, Tc)) and C (columns [256, 256 + Tc)) separately, so
-// product 1 of the next tile overlaps the rule of the current one and only
-// product 2's latency is on the epilogue's critical path.  All waits are bounded.
+// Geometry
 // ---------------------------------------------------------------------------
-constexpr int kAtomBytes = 128 * 128;  // one 128-row x 128-byte swizzle atom
-constexpr int kAtoms = 2;              // X tile = 128 rows x 256 columns
-constexpr int kXBytes = kAtoms * kAtomBytes;
-constexpr int kXCols = 128 * kAtoms;
+constexpr int kAtomBytes = 128 * 128;    // one 128-row x 128-byte swizzle atom
+constexpr int kXBytes = 2 * kAtomBytes;  // X tile = 128 rows x 256 columns
 constexpr int kXStages = 4;
-constexpr int kHCol = 0;               // TMEM column of H
-constexpr int kCCol = 256;             // TMEM column of C
-constexpr int kN1 = 32;                // product-1 column chunk
-constexpr int kEpiGroups = 4;          // epilogue warp groups (column blocks round-robin)
-// The MMA warp waits for the epilogue most of the time; between its tries it
-// sleeps this long, so that it leaves issue slots to the epilogue warps that
-// share its scheduler.
-constexpr uint32_t kMmaSleepNs = 32;
-constexpr int kMaxChunks = 4;          // 16-column chunks per epilogue warp: 2 blocks of 32 (Tc <= 256)
-constexpr int kEpiWarps = 4 * kEpiGroups;
-constexpr int kThreads = 64 + 32 * kEpiWarps;  // producer + MMA + epilogue warps
+constexpr int kHCol = 0;    // TMEM column of H
+constexpr int kCCol = 256;  // TMEM column of C
+constexpr int kN1 = 32;     // product-1 column chunk = one output word
+constexpr int kGroups = 4;  // epilogue column groups
+constexpr int kEpiWarps = 4 * kGroups;
+constexpr int kUnpackWarps = 4;
+constexpr int kEpiWarp0 = 1 + kUnpackWarps;  // warp 0: MMA, 1..4: unpack, 5..20: epilogue
+constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);
+constexpr int kMaxChunks = 7;  // Tc <= 224
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any legitimate wait
 
-struct TensorParams {
-    uint8_t* out;      // destination frame base
-    int n, H;
-    long long pitch;
-    int R, PADC;       // radius, column halo of the tile (multiple of 16, >= R)
-    int Tr, Tc;        // output rows / columns per tile
-    int K1c;           // product-1 K window (multiple of 32)
+struct TcParams {
+    const uint32_t* src;  // inner word (0, 0) of the current packed frame
+    uint32_t* dst;        // inner word (0, 0) of the next packed frame
+    long long wpitch;     // words per frame row
+    int n, nw;
+    int R, PADC, glo, K1;  // column halo of a tile (16 mod 32), first window group, product-1 K
+    int Tr, Tc, nchunks;
     int tiles_x, tiles_y;
-    RuleSwar8 q;       // rule on the box count (used when (2R+1)^2 <= 127)
-    int slo, shi, blo, bhi;  // rule on the box count, scalar form
+    int fast;     // n % 32 == 0 and n >= 256: word-aligned wrap with one correction
+    int lanes16;  // rule lanes: 0 = four 8-bit lanes (R <= 5), 1 = two 16-bit lanes
+    uint32_t nlo0, dlo, hiH0, dhi;  // rule constants (lane-broadcast; d* = live minus dead, mod 2^32)
+    uint32_t rq_mask[kGroups];      // bit i: this epilogue group re-quantises chunk i
     unsigned int* err;
-    unsigned long long wait_ns;  // limit of every mbarrier wait
-    int inject_missing_commit;   // test hook: product 1 of the first tile never signals
+    unsigned long long wait_ns;
+    int inject_missing_commit;  // test hook: product 1 of the first tile never signals
 };
 
 struct SmemLayout {
     int x_off, hs_off, bh_off, bv_off, bar_off, tmem_off, total;
 };
 
-enum Bar { X_FULL = 0, X_EMPTY = kXStages, H_FULL = 2 * kXStages, HS_FULL, C_FULL, C_EMPTY, NBARS };
+enum Bar { X_FULL = 0, X_EMPTY = kXStages, H_FULL = 2 * kXStages, HS_FULL, C_FULL, C_EMPTY, DRAIN, NBARS };
 
-__host__ __device__ inline SmemLayout smem_layout(int Tc, int K1c) {
+__host__ __device__ inline SmemLayout smem_layout(int Tc, int K1) {
     SmemLayout L{};
     int o = 0;
     L.x_off = o;
-    o += kXStages * kXBytes;                // 1024-aligned stages
+    o += kXStages * kXBytes;  // 1024-aligned stages
     L.hs_off = o;
-    o += 2 * 128 * Tc;                      // H as u8, MN-major, two buffers (tile parity)
+    o += 2 * 128 * Tc;        // H as u8, MN-major, two buffers (tile parity)
     L.bh_off = o;
-    o += kN1 * K1c;                         // B_h
+    o += kN1 * K1;            // B_h
     L.bv_off = o;
-    o += 128 * 128;                         // B_v
+    o += 128 * 128;           // B_v
     o = (o + 7) & ~7;
     L.bar_off = o;
     o += NBARS * 8;
@@ -274,15 +108,43 @@ __host__ __device__ inline SmemLayout smem_layout(int Tc, int K1c) {
     return L;
 }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+// Column permutation inside a 32-column group: byte position q holds cell pi(q).
+__host__ __device__ constexpr int perm_pi(int q) { return 8 * (q & 3) + (q >> 2); }
+// Output cell (within a 32-column chunk) of accumulator column n.
+__host__ __device__ constexpr int perm_sigma(int n, int lanes16) {
+    return lanes16 ? 16 * (n & 1) + (n >> 1) : perm_pi(n);
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
-k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
+__device__ __forceinline__ int wrap_slow(int v, int n) {
+    int r = v % n;
+    return r < 0 ? r + n : r;
+}
+
+// Cells a .. a+31 (modulo n) of one packed row, bit b = cell a+b; 0 <= a < n.
+// Bits past n in the row's last word are ignored.
+__device__ __forceinline__ uint32_t fetch32(const uint32_t* __restrict__ row, int a, int n) {
+    if (n >= 32) {
+        const int w0 = a >> 5, s = a & 31;
+        // row[w0 + 1] may be the right halo word (w0 = nw - 1): its bits are masked below
+        uint32_t v = __funnelshift_r(__ldg(row + w0), __ldg(row + w0 + 1), s);
+        const int valid = n - a;
+        if (valid < 32) v = (v & ((1u << valid) - 1u)) | (__ldg(row) << valid);
+        return v;
+    }
+    const uint32_t w = __ldg(row);
+    uint32_t v = 0u;
+    int c = a;
+    for (int b = 0; b < 32; ++b) {
+        v |= ((w >> c) & 1u) << b;
+        if (++c == n) c = 0;
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_constant__ TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const SmemLayout L = smem_layout(p.Tc, p.K1c);
+    const SmemLayout L = smem_layout(p.Tc, p.K1);
     uint8_t* xs = smem + L.x_off;
     uint8_t* hs = smem + L.hs_off;
     uint8_t* bh = smem + L.bh_off;
@@ -291,7 +153,7 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
     uint32_t* tmem_slot = (uint32_t*)(smem + L.tmem_off);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int R = p.R, PADC = p.PADC, Tc = p.Tc, K1c = p.K1c;
+    const int R = p.R, Tc = p.Tc, K1 = p.K1;
     const int ntiles = p.tiles_x * p.tiles_y;
     int mine = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) ++mine;
@@ -299,22 +161,25 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
 
     if (tid == 0) {
         for (int i = 0; i < kXStages; ++i) {
-            mbar_init(&bars[X_FULL + i], 1);
+            mbar_init(&bars[X_FULL + i], kUnpackWarps);
             mbar_init(&bars[X_EMPTY + i], kEpiWarps);
         }
         mbar_init(&bars[H_FULL], 1);
         mbar_init(&bars[HS_FULL], kEpiWarps);
         mbar_init(&bars[C_FULL], 1);
         mbar_init(&bars[C_EMPTY], kEpiWarps);
+        mbar_init(&bars[DRAIN], 1);
         fence_mbar_init();
     }
     if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
-    // Band matrices (no-swizzle K-major layouts: [k / 16][row][16 bytes]).
-    // B_h[n][k] = [|k - PADC - n| <= R], n < 32, k < K1c
-    for (int idx = tid; idx < kN1 * K1c; idx += kThreads) {
-        const int k = idx / kN1, n = idx % kN1;
-        const int d = k - PADC - n;
-        bh[((k >> 4) * kN1 + n) * 16 + (k & 15)] = (d >= -R && d <= R) ? 1 : 0;
+    // B_h (K-major, no swizzle: [k / 16][n][16 bytes]), K1 x 32.  Row k is byte
+    // position k of the chunk's window (group glo + k / 32, permuted by pi), column
+    // n is accumulator column n (output cell sigma(n) of the chunk).
+    for (int idx = tid; idx < kN1 * K1; idx += kThreads) {
+        const int k = idx / kN1, nn = idx % kN1;
+        const int xc = 32 * (p.glo + (k >> 5)) + perm_pi(k & 31);  // X column relative to the chunk
+        const int d = xc - p.PADC - perm_sigma(nn, p.lanes16);
+        bh[((k >> 4) * kN1 + nn) * 16 + (k & 15)] = (d >= -R && d <= R) ? 1 : 0;
     }
     // B_v[m][k] = [m <= k <= m + 2R], m, k < 128 (16 bytes per store)
     for (int idx = tid; idx < 8 * 128; idx += kThreads) {
@@ -333,58 +198,29 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
         *(uint4*)(bv + (kc * 128 + m) * 16) = make_uint4(w[0], w[1], w[2], w[3]);
     }
     fence_proxy_async();
-    tc_fence_before();
+    fence_before();
     __syncthreads();
-    tc_fence_after();
+    fence_after();
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0) {
-        // ------------------------- TMA producer -----------------------------
-        if (lane == 0) {
-            int it = 0;
-            bool ok = true;
-            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++it) {
-                const int st = it % kXStages;
-                const uint32_t ph = (uint32_t)(it / kXStages) & 1u;
-                if (it >= kXStages) ok = mbar_wait(&bars[X_EMPTY + st], ph ^ 1u, p.wait_ns, 128);
-                if (!ok) {
-                    atomicOr(p.err, 1u);
-                    break;
-                }
-                const int ty = t / p.tiles_x, tx = t % p.tiles_x;
-                const int y = p.H + ty * p.Tr - R;
-                const int x = p.H + tx * Tc - PADC;
-                uint8_t* dst = xs + st * kXBytes;
-                mbar_expect_tx(&bars[X_FULL + st], kXBytes);
-#pragma unroll
-                for (int a = 0; a < kAtoms; ++a) tma_load_2d(dst + a * kAtomBytes, &xmap, &bars[X_FULL + st], x + 128 * a, y);
-            }
-            // never leave with a copy in flight into this CTA's shared memory
-            const int issued = it;
-            for (int j = (issued > kXStages ? issued - kXStages : 0); j < issued; ++j) {
-                if (!mbar_wait(&bars[X_FULL + j % kXStages], (uint32_t)(j / kXStages) & 1u, p.wait_ns))
-                    atomicOr(p.err, 16u);
-            }
-        }
-    } else if (warp == 1) {
         // --------------------------- MMA issuer -----------------------------
         if (lane == 0) {
             const uint32_t ba = smem_u32(bh), va = smem_u32(bv), ha0 = smem_u32(hs);
             const uint32_t id1 = idesc_u8(kN1, false);
             const uint32_t id2 = idesc_u8(Tc, true);
-            bool ok = true;
+            const int ksteps = K1 / 32;
             auto product1 = [&](int j) -> bool {
                 const int st = j % kXStages;
                 if (!mbar_wait(&bars[X_FULL + st], (uint32_t)(j / kXStages) & 1u, p.wait_ns)) return false;
-                tc_fence_after();
+                fence_after();
                 const uint32_t xa = smem_u32(xs + st * kXBytes);
-                for (int n0 = 0; n0 < Tc; n0 += kN1) {
-                    for (int s = 0; s < K1c / 32; ++s) {
-                        const int col = n0 + 32 * s;  // X column of this K step
-                        const uint32_t a_addr = xa + (col >> 7) * kAtomBytes + (col & 127);
-                        const uint64_t ad = desc_k_sw128(a_addr);
+                for (int i = 0; i < p.nchunks; ++i) {
+                    for (int s = 0; s < ksteps; ++s) {
+                        const int col = 32 * (i + p.glo + s);  // X column of this K step
+                        const uint64_t ad = desc_k_sw128(xa + (col >> 7) * kAtomBytes + (col & 127));
                         const uint64_t bd = desc_noswz(ba + s * 2 * kN1 * 16, kN1 * 16, 128);
-                        mma_i8(tmem + kHCol + n0, ad, bd, id1, s > 0 ? 1u : 0u);
+                        mma_i8(tmem + kHCol + kN1 * i, ad, bd, id1, s > 0 ? 1u : 0u);
                     }
                 }
                 if (!(p.inject_missing_commit && j == 0)) mma_commit(&bars[H_FULL]);
@@ -392,8 +228,8 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             };
             // product 2 of tile j: C = B_v * H(j), H(j) in shared-memory buffer j % 2
             auto product2 = [&](int j) -> bool {
-                if (j >= 1 && !mbar_wait(&bars[C_EMPTY], (uint32_t)(j - 1) & 1u, p.wait_ns, kMmaSleepNs)) return false;
-                tc_fence_after();
+                if (j >= 1 && !mbar_wait(&bars[C_EMPTY], (uint32_t)(j - 1) & 1u, p.wait_ns)) return false;
+                fence_after();
                 const uint32_t ha = ha0 + (j & 1) * 128 * Tc;
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
@@ -406,38 +242,123 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
             };
             // Order per tile j: product 1 of tile j+1 as soon as H(j) has been read
             // back, then product 2 of tile j once C(j-1) has been read.
-            ok = mine >= 1 ? product1(0) : true;
+            bool ok = mine >= 1 ? product1(0) : true;
             for (int j = 0; j < mine && ok; ++j) {
-                ok = mbar_wait(&bars[HS_FULL], (uint32_t)j & 1u, p.wait_ns, kMmaSleepNs);
+                ok = mbar_wait(&bars[HS_FULL], (uint32_t)j & 1u, p.wait_ns);
                 if (ok && j + 1 < mine) ok = product1(j + 1);
                 if (ok) ok = product2(j);
             }
             if (!ok) atomicOr(p.err, 2u);
+            // never leave with an MMA in flight (TMEM is freed below)
+            mma_commit(&bars[DRAIN]);
+            if (!mbar_wait(&bars[DRAIN], 0u, p.wait_ns)) atomicOr(p.err, 32u);
         }
+    } else if (warp < kEpiWarp0) {
+        // ------------------------------ unpack ------------------------------
+        // 128 threads fill a stage: 128 rows x 8 groups of 32 columns.  Thread
+        // ut always handles group g = ut % 8 of rows ut / 8 + 16 q, q = 0..7
+        // (4 rows x 8 groups per warp and round).  The words of the next tile are
+        // loaded while this one is spread and stored, so the loads' latency is
+        // spent waiting for a free stage rather than on the critical path.
+        const int ut = tid - 32;
+        const int g = ut & 7;
+        // the 8 groups (32 cells each, bit b = cell b) this thread stores for tile t
+        auto gather = [&](int t, uint32_t (&x)[8]) {
+            const int ty = t / p.tiles_x, tx = t % p.tiles_x;
+            const int rbase = ty * p.Tr - R;
+            const int cbase = tx * Tc - p.PADC;  // column of X-tile column 0 (16 mod 32)
+            if (p.fast) {
+                int wl = (cbase + 32 * g - 16) >> 5;  // word holding the group's first cell
+                if (wl < 0) wl += p.nw;
+                else if (wl >= p.nw) wl -= p.nw;
+                const int wr = wl + 1 == p.nw ? 0 : wl + 1;
+                uint32_t lo[8], hi[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    int gr = rbase + (ut >> 3) + 16 * q;
+                    if (gr < 0) gr += p.n;
+                    else if (gr >= p.n) gr -= p.n;
+                    const uint32_t* rp = p.src + (size_t)gr * (size_t)p.wpitch;
+                    lo[q] = __ldg(rp + wl);
+                    hi[q] = __ldg(rp + wr);
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q) x[q] = prmt(lo[q], hi[q], 0x5432u);  // upper half of wl, lower of wr
+            } else {
+                const int a = wrap_slow(cbase + 32 * g, p.n);
+                for (int q = 0; q < 8; ++q) {
+                    const int gr = wrap_slow(rbase + (ut >> 3) + 16 * q, p.n);
+                    x[q] = fetch32(p.src + (size_t)gr * (size_t)p.wpitch, a, p.n);
+                }
+            }
+        };
+        bool ok = true;
+        int it = 0;
+        uint32_t x[8];
+        if ((int)blockIdx.x < ntiles) gather(blockIdx.x, x);
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+            const int st = it % kXStages;
+            if (it >= kXStages) {
+                bool w = true;
+                if (lane == 0) w = mbar_wait(&bars[X_EMPTY + st], ((uint32_t)(it / kXStages) & 1u) ^ 1u, p.wait_ns);
+                ok = __shfl_sync(0xffffffffu, w, 0);
+                if (!ok) break;
+            }
+            uint8_t* xst = xs + st * kXBytes + (g >> 2) * kAtomBytes;
+            const int ch = 2 * (g & 3);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int row = (ut >> 3) + 16 * q;
+                uint32_t u[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) u[k] = (x[q] >> k) & 0x01010101u;
+                uint8_t* rowp = xst + row * 128;
+                const int sw = row & 7;
+                *(uint4*)(rowp + ((ch ^ sw) << 4)) = make_uint4(u[0], u[1], u[2], u[3]);
+                *(uint4*)(rowp + (((ch + 1) ^ sw) << 4)) = make_uint4(u[4], u[5], u[6], u[7]);
+            }
+            fence_proxy_async();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bars[X_FULL + st]);
+            if (t + (int)gridDim.x < ntiles) gather(t + gridDim.x, x);
+        }
+        if (!ok && lane == 0) atomicOr(p.err, 4u);
     } else {
         // ---------------------------- epilogue ------------------------------
-        const int q = warp & 3;                 // TMEM lane quarter of this warp
-        const int grp = (warp - 2) >> 2;        // column group
-        const int row = q * 32 + lane;          // H row / output row within the tile
+        const int ew = warp - kEpiWarp0;
+        const int q = warp & 3;          // TMEM lane quarter this warp may access
+        const int grp = ew >> 2;         // column group
+        const int m = q * 32 + lane;     // tile row (TMEM lane)
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
-        const bool small = (2 * R + 1) * (2 * R + 1) <= 127;
+        const uint32_t rq_mask = p.rq_mask[grp];
+        const int aoff = (p.PADC - 16) >> 5;  // centre groups of chunk i: i + aoff, i + aoff + 1
         bool ok = true;
+        auto wait_all = [&](uint64_t* bar, uint32_t ph) -> bool {
+            const bool w = mbar_wait(bar, ph, p.wait_ns);
+            return __all_sync(0xffffffffu, w);
+        };
         // re-quantise H(j) to u8 into shared-memory buffer j % 2 (MN-major B operand of product 2)
         auto requant = [&](int j) -> bool {
-            if (!mbar_wait(&bars[H_FULL], (uint32_t)j & 1u, p.wait_ns)) return false;
-            tc_fence_after();
+            if (!wait_all(&bars[H_FULL], (uint32_t)j & 1u)) return false;
+            fence_after();
             uint8_t* hsb = hs + (j & 1) * 128 * Tc;
-            tmem_walk16<kMaxChunks>(tmem + kHCol + lane_off, grp, kEpiGroups, Tc,
-                                    [&](const uint32_t (&v)[8], int col) {
-                                        uint4 w;
-                                        w.x = low_bytes4(v[0], v[1]);
-                                        w.y = low_bytes4(v[2], v[3]);
-                                        w.z = low_bytes4(v[4], v[5]);
-                                        w.w = low_bytes4(v[6], v[7]);
-                                        *(uint4*)(hsb + ((col >> 4) * 128 + row) * 16) = w;
-                                    });
+            for (int i = 0; i < p.nchunks; ++i) {
+                if (!((rq_mask >> i) & 1u)) continue;
+                uint32_t v[16];
+                tmem_ld32p(tmem + lane_off + kHCol + kN1 * i, v);
+                tmem_wait16(v);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    uint4 w;
+                    w.x = prmt(v[8 * h + 0], v[8 * h + 1], 0x6420u);
+                    w.y = prmt(v[8 * h + 2], v[8 * h + 3], 0x6420u);
+                    w.z = prmt(v[8 * h + 4], v[8 * h + 5], 0x6420u);
+                    w.w = prmt(v[8 * h + 6], v[8 * h + 7], 0x6420u);
+                    *(uint4*)(hsb + ((2 * i + h) * 128 + m) * 16) = w;
+                }
+            }
             fence_proxy_async();
-            tc_fence_before();
+            fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&bars[HS_FULL]);
             return true;
@@ -450,66 +371,73 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
                 break;
             }
             // rule + store C(j)
-            if (!mbar_wait(&bars[C_FULL], (uint32_t)j & 1u, p.wait_ns)) {
+            if (!wait_all(&bars[C_FULL], (uint32_t)j & 1u)) {
                 ok = false;
                 break;
             }
-            tc_fence_after();
+            fence_after();
             const int st = j % kXStages;
             const int ty = t / p.tiles_x, tx = t % p.tiles_x;
-            const int r0 = ty * p.Tr, c0 = tx * Tc;
-            const int gi = r0 + row;
-            const bool row_ok = (row < p.Tr) && (gi < p.n);
-            const int xr = row + R;
-            const uint8_t* xrow = xs + st * kXBytes + (xr & 127) * 128;
-            uint8_t* orow = p.out + (size_t)(p.H + gi) * (size_t)p.pitch + p.H + c0;
-            tmem_walk16<kMaxChunks>(tmem + kCCol + lane_off, grp, kEpiGroups, Tc, [&](const uint32_t (&v)[8], int col) {
-                if (!row_ok) return;
-                const int xc = PADC + col;  // X column of these 16 cells
-                const int atom = xc >> 7, ch = (xc & 127) >> 4;
-                const uint4 s4 = *(const uint4*)(xrow + atom * kAtomBytes + ((ch ^ (xr & 7)) << 4));
-                const uint32_t sw[4] = {s4.x, s4.y, s4.z, s4.w};  // compile-time indices only
-                uint32_t o[4];
+            const int gi = ty * p.Tr + m;
+            const bool row_ok = (m < p.Tr) && (gi < p.n);
+            const int xr = min(m + R, 127);  // X row of this output row's centre cells (rows >= Tr are not stored)
+            const uint8_t* xrow = xs + st * kXBytes + xr * 128;
+            const int sw = xr & 7;
+            uint32_t* orow = p.dst + (size_t)(row_ok ? gi : 0) * (size_t)p.wpitch;
+            const int w0 = tx * (Tc >> 5);
+            for (int i = grp; i < p.nchunks; i += kGroups) {
+                uint32_t v[16];
+                tmem_ld32p(tmem + lane_off + kCCol + kN1 * i, v);
+                // centre cells: groups ga and ga + 1 of the X row (8 words each)
+                const int ga = i + aoff, gb = ga + 1;
+                const uint4 a0 = *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3)) ^ sw) << 4));
+                const uint4 a1 = *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3) + 1) ^ sw) << 4));
+                const uint4 b0 = *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3)) ^ sw) << 4));
+                const uint4 b1 = *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3) + 1) ^ sw) << 4));
+                const uint32_t Ga[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+                const uint32_t Gb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+                tmem_wait16(v);
+                uint32_t acc = 0u;
+                if (!p.lanes16) {
+                    // accumulator column 4k+j = output cell 8j+k: four box counts per
+                    // register, bit 7 of each byte lane = the rule's result
 #pragma unroll
-                for (int qq = 0; qq < 4; ++qq) {
-                    const uint32_t* b = &v[2 * qq];  // cells 4qq .. 4qq+3 as two 16-bit pairs
-                    if (small) {
-                        o[qq] = rule_swar8(low_bytes4(b[0], b[1]), sw[qq], p.q);
-                    } else {
-                        uint32_t r = 0;
+                    for (int k = 0; k < 8; ++k) {
+                        const uint32_t B4 = prmt(v[2 * k], v[2 * k + 1], 0x6420u);
+                        const uint32_t s4 = prmt(Ga[k], Gb[k], 0x5432u);
+                        const uint32_t ge = (B4 + p.nlo0) + s4 * p.dlo;  // bit 7: B >= lo(s)
+                        const uint32_t le = (p.hiH0 + s4 * p.dhi) - B4;  // bit 7: B <= hi(s)
+                        acc |= (ge & le & 0x80808080u) >> (7 - k);
+                    }
+                } else {
+                    // accumulator column 2r+h = output cell 16h+r: two box counts per
+                    // register, bit 15 of each 16-bit lane = the rule's result
 #pragma unroll
-                        for (int e = 0; e < 4; ++e) {
-                            const int B = (int)((b[e >> 1] >> (16 * (e & 1))) & 0xffffu);
-                            const int sv = (sw[qq] >> (8 * e)) & 1;
-                            const int lo = sv ? p.slo : p.blo, hi = sv ? p.shi : p.bhi;
-                            r |= (uint32_t)((B >= lo) & (B <= hi)) << (8 * e);
-                        }
-                        o[qq] = r;
+                    for (int r = 0; r < 16; ++r) {
+                        const uint32_t hsel = (uint32_t)(r >> 3);
+                        const uint32_t s2 = prmt(Ga[r & 7], Gb[r & 7], (2u + hsel) | 0x80u | ((4u + hsel) << 8) | 0x8000u);
+                        const uint32_t ge = (v[r] + p.nlo0) + s2 * p.dlo;
+                        const uint32_t le = (p.hiH0 + s2 * p.dhi) - v[r];
+                        acc |= (ge & le & 0x80008000u) >> (15 - r);
                     }
                 }
-                const int gj = c0 + col;
-                if (gj + 16 <= p.n) {
-                    *(uint4*)(orow + col) = make_uint4(o[0], o[1], o[2], o[3]);
-                } else if (gj < p.n) {
-                    const int cnt = p.n - gj;
-#pragma unroll
-                    for (int e = 0; e < 16; ++e)
-                        if (e < cnt) orow[col + e] = (uint8_t)((o[e >> 2] >> (8 * (e & 3))) & 0xff);
-                }
-            });
-            tc_fence_before();
+                const int wi = w0 + i;
+                if (row_ok && wi < p.nw) orow[wi] = acc;
+            }
+            fence_before();
             __syncwarp();
             if (lane == 0) {
                 mbar_arrive(&bars[C_EMPTY]);
                 mbar_arrive(&bars[X_EMPTY + st]);
             }
         }
-        if (!ok) atomicOr(p.err, 8u);
+        if (!ok && lane == 0) atomicOr(p.err, 8u);
     }
-    tc_fence_before();
+    fence_before();
     __syncthreads();
     if (warp == 0) {
         __syncwarp();
+        fence_after();
         tmem_dealloc(tmem, kTmemCols);
     }
 }
@@ -518,28 +446,11 @@ k_tensor_step(const __grid_constant__ CUtensorMap xmap, TensorParams p) {
 // Host side
 // ---------------------------------------------------------------------------
 struct TensorPlan {
-    CUtensorMap map[2];  // source frame a / b
-    TensorParams prm[2]; // destination frame b / a
+    TcParams prm[2];  // source frame a -> b, b -> a
     int smem_bytes;
     int grid;
     unsigned int* err;
 };
-
-static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-    }
-    return fn;
-}
-
-static int pad_for(int R) { return (int)round_up((size_t)R, 16); }
-
-int tensor_plan_halo_needed(int radius) { return std::max(16, pad_for(radius)); }
 
 bool tensor_supported(int n, int radius, char* why, size_t why_len) {
     if (radius < 1 || radius > 32) {
@@ -553,7 +464,24 @@ bool tensor_supported(int n, int radius, char* why, size_t why_len) {
     return true;
 }
 
-TensorPlan* tensor_plan_create(const Frame& a, const Frame& b, const Rule& rule, int device, char* why,
+// Lane constants of the interval rule on the box count B (centre included):
+// a live cell survives iff smin+1 <= B <= smax+1, a dead one is born iff
+// bmin <= B <= bmax.  For a lane of `bits` bits whose top bit is the marker,
+// nlo = top - lo (B + nlo has the marker set iff B >= lo) and hiH = top + hi
+// (hiH - B has it set iff B <= hi); empty intervals become lo = top, hi = 0.
+static void lane_consts(int lo, int hi, int bits, int& nlo, int& hiH) {
+    const int top = 1 << (bits - 1);
+    if (lo < 0) lo = 0;
+    if (hi > top - 1) hi = top - 1;
+    if (hi < lo || lo > top - 1) {
+        lo = top;
+        hi = 0;
+    }
+    nlo = top - lo;
+    hiH = top + hi;
+}
+
+TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const Rule& rule, int device, char* why,
                                size_t why_len) {
     if (!tensor_supported(a.n, rule.radius, why, why_len)) return nullptr;
     int major = 0;
@@ -562,55 +490,68 @@ TensorPlan* tensor_plan_create(const Frame& a, const Frame& b, const Rule& rule,
         snprintf(why, why_len, "tcgen05 needs an sm_100 device (compute capability %d.x)", major);
         return nullptr;
     }
-    auto encode = encode_fn();
-    if (!encode) {
-        snprintf(why, why_len, "cuTensorMapEncodeTiled not available");
+    if (a.HW < 1 || b.HW < 1) {
+        snprintf(why, why_len, "packed frames need a halo word");
         return nullptr;
     }
     TensorPlan* P = new TensorPlan();
     const int R = rule.radius;
-    const int PADC = pad_for(R);
-    const int Tc = ((kXCols - 2 * PADC) / kN1) * kN1;  // 224 for R <= 16, 192 for R <= 32
+    const int PADC = R <= 16 ? 16 : 48;
+    const int Tc = 256 - 2 * PADC;  // 224 or 160
     const int Tr = 128 - 2 * R;
-    const int K1c = (int)round_up((size_t)(kN1 + PADC + R), 32);
-    if (Tc < kN1 || Tc > 16 * kEpiGroups * kMaxChunks || Tr < 1 || K1c > kN1 + 2 * PADC) {
+    const int glo = (PADC - R) / 32;
+    const int ghi = (PADC + 31 + R) / 32;
+    const int K1 = 32 * (ghi - glo + 1);
+    const int nchunks = Tc / 32;
+    const int lanes16 = (2 * R + 1) * (2 * R + 1) > 127 ? 1 : 0;
+    const int bits = lanes16 ? 16 : 8;
+    const uint32_t bcast = lanes16 ? 0x00010001u : 0x01010101u;
+    int nlo_d, hiH_d, nlo_s, hiH_s;
+    lane_consts(rule.bmin, rule.bmax, bits, nlo_d, hiH_d);
+    lane_consts(rule.smin + 1, rule.smax + 1, bits, nlo_s, hiH_s);
+    if (Tr < 1 || nchunks > kMaxChunks || (nchunks - 1) + (PADC - 16) / 32 + 1 > 7 || (nchunks - 1) + ghi > 7) {
         snprintf(why, why_len, "no tile shape for R=%d", R);
         delete P;
         return nullptr;
     }
-    const Frame* src[2] = {&a, &b};
-    const Frame* dst[2] = {&b, &a};
+    // epilogue balance: the rule of chunk i runs on group i % 4; each
+    // re-quantisation (about a quarter of a rule chunk's work) goes to the
+    // group with the least work so far
+    uint32_t rq_mask[kGroups] = {0, 0, 0, 0};
+    int load[kGroups] = {0, 0, 0, 0};
+    for (int i = 0; i < nchunks; ++i) load[i % kGroups] += 4;
+    for (int i = 0; i < nchunks; ++i) {
+        int g = 0;
+        for (int h = 1; h < kGroups; ++h)
+            if (load[h] < load[g]) g = h;
+        rq_mask[g] |= 1u << i;
+        load[g] += 1;
+    }
+    const PackedFrame* src[2] = {&a, &b};
+    const PackedFrame* dst[2] = {&b, &a};
     for (int i = 0; i < 2; ++i) {
-        const Frame& f = *src[i];
-        cuuint64_t gdim[2] = {(cuuint64_t)f.pitch, (cuuint64_t)(f.n + 2 * f.H)};
-        cuuint64_t gstride[1] = {(cuuint64_t)f.pitch};
-        cuuint32_t box[2] = {128, 128};
-        cuuint32_t estride[2] = {1, 1};
-        CUresult cr = encode(&P->map[i], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)f.base, gdim, gstride, box, estride,
-                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (cr != CUDA_SUCCESS) {
-            snprintf(why, why_len, "cuTensorMapEncodeTiled failed (%d)", (int)cr);
-            delete P;
-            return nullptr;
-        }
-        TensorParams& q = P->prm[i];
-        q.out = dst[i]->base;
-        q.n = f.n;
-        q.H = f.H;
-        q.pitch = (long long)f.pitch;
+        TcParams& q = P->prm[i];
+        q.src = src[i]->words + (size_t)src[i]->HR * src[i]->wpitch + src[i]->HW;
+        q.dst = dst[i]->words + (size_t)dst[i]->HR * dst[i]->wpitch + dst[i]->HW;
+        q.wpitch = (long long)a.wpitch;
+        q.n = a.n;
+        q.nw = a.nw;
         q.R = R;
         q.PADC = PADC;
+        q.glo = glo;
+        q.K1 = K1;
         q.Tr = Tr;
         q.Tc = Tc;
-        q.K1c = K1c;
-        q.tiles_x = (f.n + Tc - 1) / Tc;
-        q.tiles_y = (f.n + Tr - 1) / Tr;
-        q.q = make_rule_swar8(rule);
-        q.slo = rule.smin + 1;
-        q.shi = rule.smax + 1;
-        q.blo = rule.bmin;
-        q.bhi = rule.bmax;
+        q.nchunks = nchunks;
+        q.tiles_x = (a.n + Tc - 1) / Tc;
+        q.tiles_y = (a.n + Tr - 1) / Tr;
+        q.fast = (a.n % 32 == 0 && a.n >= 256) ? 1 : 0;
+        q.lanes16 = lanes16;
+        q.nlo0 = (uint32_t)nlo_d * bcast;
+        q.dlo = (uint32_t)(nlo_s - nlo_d);
+        q.hiH0 = (uint32_t)hiH_d * bcast;
+        q.dhi = (uint32_t)(hiH_s - hiH_d);
+        for (int g = 0; g < kGroups; ++g) q.rq_mask[g] = rq_mask[g];
     }
     if (cudaMalloc(&P->err, sizeof(unsigned int)) != cudaSuccess) {
         snprintf(why, why_len, "error-flag allocation failed");
@@ -623,7 +564,7 @@ TensorPlan* tensor_plan_create(const Frame& a, const Frame& b, const Rule& rule,
         q.wait_ns = kWaitLimitNs;
         q.inject_missing_commit = 0;
     }
-    P->smem_bytes = smem_layout(Tc, K1c).total + 1024;
+    P->smem_bytes = smem_layout(Tc, K1).total + 1024;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     P->grid = std::min(P->prm[0].tiles_x * P->prm[0].tiles_y, sms);
@@ -656,7 +597,7 @@ unsigned int* tensor_plan_error_flag(TensorPlan* p) { return p ? p->err : nullpt
 
 cudaError_t launch_tensor_pass(TensorPlan* p, bool src_is_a, cudaStream_t s) {
     const int i = src_is_a ? 0 : 1;
-    k_tensor_step<<<p->grid, kThreads, p->smem_bytes, s>>>(p->map[i], p->prm[i]);
+    k_tensor_step<<<p->grid, kThreads, p->smem_bytes, s>>>(p->prm[i]);
     return cudaGetLastError();
 }
 

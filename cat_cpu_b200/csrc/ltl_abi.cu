@@ -54,7 +54,7 @@ struct ltl_ctx {
     int band_rows = 64;         // plain: rows per work item
     bool plain_wrap = false;    // plain R <= 5: kernels apply the torus wrap, no halo refresh
     int packed_band_rows = 0;   // packed: rows per work item (0: heuristic)
-    // packed variant
+    // packed and tensor variants: the grid lives in packed frames between steps
     PackedFrame pa{}, pb{};
     uint32_t* pwords = nullptr;
     size_t pwords_bytes = 0;
@@ -186,8 +186,7 @@ static int create_impl(ltl_ctx** out, int device, int rows, int n, int radius, i
     c->stream = c->own_stream;
 
     int depth = 1;
-    int H = halo_for(radius, 1);
-    if (variant == LTL_VARIANT_TENSOR) H = std::max(H, tensor_plan_halo_needed(radius));
+    const int H = halo_for(radius, 1);
     size_t pitch = pitch_for(n, H);
     size_t frows = (size_t)rows + 2 * H + 1;  // +1 spare row: vector loads may run past the last frame row
     size_t one = round_up(frows * pitch, 4096);
@@ -223,11 +222,13 @@ static int create_impl(ltl_ctx** out, int device, int rows, int n, int radius, i
         release(c);
         return LTL_ECUDA;
     }
-    if (variant == LTL_VARIANT_PACKED) {
+    if (variant == LTL_VARIANT_PACKED || variant == LTL_VARIANT_TENSOR) {
+        // the packed step reads R + 1 halo rows; the tensor step wraps rows and
+        // words itself and only needs the right halo word to exist
         PackedFrame p{};
         p.n = n;
         p.nw = (n + 31) / 32;
-        p.HR = radius + 1;
+        p.HR = variant == LTL_VARIANT_PACKED ? radius + 1 : 1;
         p.HW = 1;
         p.wpitch = round_up((size_t)p.nw + 2 * p.HW + 1, 4);  // +1: edge lanes read one word past the halo
         size_t prow = (size_t)n + 2 * p.HR;
@@ -246,7 +247,7 @@ static int create_impl(ltl_ctx** out, int device, int rows, int n, int radius, i
         c->pb.words = (uint32_t*)((uint8_t*)c->pwords + pone);
     }
     if (variant == LTL_VARIANT_TENSOR) {
-        c->tplan = tensor_plan_create(c->fa, c->fb, c->rule, device, why, sizeof(why));
+        c->tplan = tensor_plan_create(c->pa, c->pb, c->rule, device, why, sizeof(why));
         if (!c->tplan) {
             ltl_set_error("ltl_create: tensor plan: %s", why);
             release(c);
@@ -316,16 +317,20 @@ extern "C" int ltl_get_info(const ltl_ctx* c, ltl_info* info) {
 
 // Make the packed frames hold the byte frame's state (packed variant keeps its
 // state packed between steps; the byte frame is refreshed on download).
+static bool keeps_packed(const ltl_ctx* c) {
+    return c->variant == LTL_VARIANT_PACKED || c->variant == LTL_VARIANT_TENSOR;
+}
+
 static int sync_to_packed(ltl_ctx* c) {
     Frame& f = cur_frame(c);
     LTL_CUDA(launch_pack_frame(f, cur_packed(c), c->stream));
-    LTL_CUDA(launch_packed_halo(cur_packed(c), c->stream));
+    if (c->variant == LTL_VARIANT_PACKED) LTL_CUDA(launch_packed_halo(cur_packed(c), c->stream));
     c->packed_valid = true;
     return LTL_OK;
 }
 
 static int sync_from_packed(ltl_ctx* c) {
-    if (c->variant != LTL_VARIANT_PACKED || !c->packed_valid) return LTL_OK;
+    if (!keeps_packed(c) || !c->packed_valid) return LTL_OK;
     LTL_CUDA(launch_unpack_frame(cur_packed(c), cur_frame(c), c->stream));
     return LTL_OK;
 }
@@ -333,7 +338,7 @@ static int sync_from_packed(ltl_ctx* c) {
 static int after_upload(ltl_ctx* c) {
     LTL_CUDA(launch_halo_fill(cur_frame(c), c->stream));
     c->packed_valid = false;
-    if (c->variant == LTL_VARIANT_PACKED) return sync_to_packed(c);
+    if (keeps_packed(c)) return sync_to_packed(c);
     return LTL_OK;
 }
 
@@ -480,10 +485,11 @@ static cudaError_t enqueue_pass(ltl_ctx* c, int gens) {
             break;
         }
         case LTL_VARIANT_TENSOR: {
+            // packed frames, torus wrap inside the kernel: no halo pass
             e = launch_tensor_pass(c->tplan, c->cur_is_a, c->stream);
             step_kernels = 1;
+            halo_kernels = 0;
             if (c->timing && e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
-            if (e == cudaSuccess) e = launch_halo_fill(nxt_frame(c), c->stream);
             break;
         }
     }
@@ -528,7 +534,7 @@ extern "C" int ltl_step(ltl_ctx* c, int steps) {
     }
     if (steps == 0) return LTL_OK;
     LTL_CUDA(cudaSetDevice(c->device));
-    if (c->variant == LTL_VARIANT_PACKED && !c->packed_valid) {
+    if (keeps_packed(c) && !c->packed_valid) {
         if (int r = sync_to_packed(c)) return r;
     }
     int passes = steps / c->depth;

@@ -74,16 +74,17 @@ cudaError_t launch_pack(const uint8_t* cells, size_t cell_pitch, int rows, int c
 cudaError_t launch_unpack(const uint64_t* words, size_t word_pitch_words, int rows, int cols, uint8_t* cells,
                           size_t cell_pitch, cudaStream_t s);
 
-// K2: tcgen05 banded-product step.
+// K2: tcgen05 banded-product step on packed frames (the tensor variant keeps
+// its grid in the packed layout of K3; the kernel wraps rows and words modulo n
+// itself, so the packed halo is never read).  The frames need HW >= 1.
 struct TensorPlan;
 bool tensor_supported(int n, int radius, char* why, size_t why_len);
-TensorPlan* tensor_plan_create(const Frame& a, const Frame& b, const Rule& rule, int device, char* why,
+TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const Rule& rule, int device, char* why,
                                size_t why_len);
 void tensor_plan_destroy(TensorPlan* p);
 int tensor_plan_depth(const TensorPlan* p);
 int tensor_plan_operand_bits(const TensorPlan* p);
-int tensor_plan_halo_needed(int radius);
-// Advance one pass (tensor_plan_depth generations) from frame `src_is_a ? a : b`.
+// Advance one pass (tensor_plan_depth generations) from packed frame `src_is_a ? a : b`.
 cudaError_t launch_tensor_pass(TensorPlan* p, bool src_is_a, cudaStream_t s);
 unsigned int* tensor_plan_error_flag(TensorPlan* p);
 // Limit of the kernel's bounded waits, and a test hook that withholds one

@@ -1,0 +1,200 @@
+"""The tile arithmetic of the tcgen05 step (k_tensor_step in
+cat_cpu_b200/csrc/k_tensor.cu), restated in numpy and checked against the
+oracle on the CPU.
+
+The kernel reads the packed grid, spreads each 32-cell group to bytes with
+(w >> k) & 0x01010101 (byte position 4k+j of a group holds cell pi(4k+j) =
+8j+k), contracts product 1 over those permuted positions with a band matrix
+B_h whose rows follow pi and whose columns follow sigma (the output cell of
+accumulator column n), sums rows with B_v in product 2, and applies the rule on
+8-bit (R <= 5) or 16-bit lanes with the centre cells taken from the same
+shared-memory tile through one byte permute per register.  The result bits are
+gathered into the output word by one shift per register.  This test runs that
+exact sequence (tile geometry, windows, torus wrap of rows and words, lane
+constants with 32-bit wraparound, byte permutes, gather) on whole small grids
+and compares every generation with the oracle, so that the index algebra is
+settled before the kernel runs on a GPU."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+M32 = np.uint64(0xFFFFFFFF)
+
+
+def pi(q):
+    return 8 * (q & 3) + (q >> 2)
+
+
+def sigma(n, lanes16):
+    return 16 * (n & 1) + (n >> 1) if lanes16 else pi(n)
+
+
+def lane_consts(lo, hi, bits):
+    top = 1 << (bits - 1)
+    lo = max(lo, 0)
+    hi = min(hi, top - 1)
+    if hi < lo or lo > top - 1:
+        lo, hi = top, 0
+    return top - lo, top + hi
+
+
+def plan(n, R, rule):
+    smin, smax, bmin, bmax = rule
+    PADC = 16 if R <= 16 else 48
+    Tc = 256 - 2 * PADC
+    Tr = 128 - 2 * R
+    glo = (PADC - R) // 32
+    ghi = (PADC + 31 + R) // 32
+    K1 = 32 * (ghi - glo + 1)
+    lanes16 = (2 * R + 1) ** 2 > 127
+    bits = 16 if lanes16 else 8
+    bc = 0x00010001 if lanes16 else 0x01010101
+    nlo_d, hih_d = lane_consts(bmin, bmax, bits)
+    nlo_s, hih_s = lane_consts(smin + 1, smax + 1, bits)
+    return dict(PADC=PADC, Tc=Tc, Tr=Tr, glo=glo, K1=K1, nchunks=Tc // 32, lanes16=lanes16,
+                nlo0=(nlo_d * bc) & 0xFFFFFFFF, dlo=(nlo_s - nlo_d) & 0xFFFFFFFF,
+                hiH0=(hih_d * bc) & 0xFFFFFFFF, dhi=(hih_s - hih_d) & 0xFFFFFFFF)
+
+
+def bh_matrix(P, R):
+    K1, glo, PADC, lanes16 = P["K1"], P["glo"], P["PADC"], P["lanes16"]
+    k = np.arange(K1)[:, None]
+    nn = np.arange(32)[None, :]
+    xc = 32 * (glo + (k >> 5)) + pi(k & 31)
+    d = xc - PADC - sigma(nn, lanes16)
+    return ((d >= -R) & (d <= R)).astype(np.int64)
+
+
+def prmt(a, b, sel):
+    """prmt.b32 default mode on uint64 arrays holding 32-bit values."""
+    src = [(a >> np.uint64(8 * i)) & np.uint64(0xFF) for i in range(4)] + \
+          [(b >> np.uint64(8 * i)) & np.uint64(0xFF) for i in range(4)]
+    out = np.zeros_like(a)
+    for i in range(4):
+        nib = (sel >> (4 * i)) & 0xF
+        byte = src[nib & 7]
+        if nib & 8:
+            byte = np.where(byte & np.uint64(0x80), np.uint64(0xFF), np.uint64(0))
+        out |= byte << np.uint64(8 * i)
+    return out
+
+
+def _word(Xc, base):
+    """Four consecutive bytes of every row of Xc as one little-endian 32-bit value."""
+    return (Xc[:, base] | (Xc[:, base + 1] << np.uint64(8)) | (Xc[:, base + 2] << np.uint64(16)) |
+            (Xc[:, base + 3] << np.uint64(24)))
+
+
+def tensor_step(grid, R, rule):
+    """One generation exactly as k_tensor_step computes it (numpy, int arithmetic)."""
+    n = grid.shape[0]
+    P = plan(n, R, rule)
+    PADC, Tc, Tr = P["PADC"], P["Tc"], P["Tr"]
+    assert Tr >= 1
+    Bh = bh_matrix(P, R)
+    m_ = np.arange(128)[:, None]
+    k_ = np.arange(128)[None, :]
+    Bv = ((k_ >= m_) & (k_ <= m_ + 2 * R)).astype(np.int64)
+    nw = (n + 31) // 32
+    out_words = np.zeros((n, nw), dtype=np.uint64)
+    tiles_x, tiles_y = -(-n // Tc), -(-n // Tr)
+    q = np.arange(32)
+    nlo0, dlo, hiH0, dhi = (np.uint64(P[k]) for k in ("nlo0", "dlo", "hiH0", "dhi"))
+    for ty in range(tiles_y):
+        for tx in range(tiles_x):
+            rbase, cbase = ty * Tr - R, tx * Tc - PADC
+            rows = (rbase + np.arange(128)) % n
+            # X tile in shared-memory byte order: position 32g + q holds cell pi(q) of group g
+            cols = np.concatenate([(cbase + 32 * g + pi(q)) % n for g in range(8)])
+            X = grid[np.ix_(rows, cols)].astype(np.int64)
+            H = np.zeros((128, Tc), dtype=np.int64)
+            for i in range(P["nchunks"]):
+                w0 = 32 * (i + P["glo"])
+                H[:, 32 * i: 32 * i + 32] = X[:, w0: w0 + P["K1"]] @ Bh
+            assert H.max() <= 2 * R + 1
+            C = Bv @ H  # box counts, centre included
+            aoff = (PADC - 16) >> 5
+            xr = np.minimum(np.arange(128) + R, 127)
+            Xc = X[xr].astype(np.uint64)  # centre rows
+            for i in range(P["nchunks"]):
+                ga, gb = i + aoff, i + aoff + 1
+                Ga = [_word(Xc, 32 * ga + 4 * k) for k in range(8)]
+                Gb = [_word(Xc, 32 * gb + 4 * k) for k in range(8)]
+                Cc = C[:, 32 * i: 32 * i + 32].astype(np.uint64)
+                # tcgen05.ld .pack::16b: register r = column 2r (low 16) | column 2r+1 (high 16)
+                v = [(Cc[:, 2 * r] & np.uint64(0xFFFF)) | ((Cc[:, 2 * r + 1] & np.uint64(0xFFFF)) << np.uint64(16))
+                     for r in range(16)]
+                acc = np.zeros(128, dtype=np.uint64)
+                if not P["lanes16"]:
+                    for k in range(8):
+                        B4 = prmt(v[2 * k], v[2 * k + 1], 0x6420)
+                        s4 = prmt(Ga[k], Gb[k], 0x5432)
+                        ge = (B4 + nlo0 + s4 * dlo) & M32
+                        le = (hiH0 + s4 * dhi - B4) & M32
+                        acc |= (ge & le & np.uint64(0x80808080)) >> np.uint64(7 - k)
+                else:
+                    for r in range(16):
+                        h = r >> 3
+                        sel = (2 + h) | 0x80 | ((4 + h) << 8) | 0x8000
+                        s2 = prmt(Ga[r & 7], Gb[r & 7], sel)
+                        ge = (v[r] + nlo0 + s2 * dlo) & M32
+                        le = (hiH0 + s2 * dhi - v[r]) & M32
+                        acc |= (ge & le & np.uint64(0x80008000)) >> np.uint64(15 - r)
+                wi = tx * (Tc // 32) + i
+                for mm in range(Tr):
+                    gi = ty * Tr + mm
+                    if gi < n and wi < nw:
+                        out_words[gi, wi] = acc[mm]
+    bits = ((out_words[:, :, None] >> np.arange(32, dtype=np.uint64)[None, None, :]) & np.uint64(1))
+    return bits.reshape(n, nw * 32)[:, :n].astype(np.uint8)
+
+
+CASES = [
+    # (n, R, rule, density, seed, steps)
+    (64, 1, O.CONWAY, 0.35, 1, 3),
+    (97, 2, O.sweep_rule(2), 0.5, 2, 2),
+    (160, 5, O.BOSCO_R5, 0.5, 3, 2),
+    (256, 5, O.BOSCO_R5, 0.5, 4, 1),
+    (41, 3, O.sweep_rule(3), 0.4, 5, 2),
+    (120, 8, O.scaled_rule(8), 0.45, 6, 2),
+    (200, 16, O.scaled_rule(16), 0.45, 7, 1),
+    (150, 17, O.scaled_rule(17), 0.45, 8, 1),
+    (100, 32, O.scaled_rule(32), 0.44, 9, 1),
+    (33, 5, O.BOSCO_R5, 0.5, 10, 2),
+    (20, 4, O.sweep_rule(4), 0.5, 11, 2),
+]
+
+
+@pytest.mark.parametrize("n,R,rule,density,seed,steps", CASES)
+def test_tile_arithmetic_matches_oracle(n, R, rule, density, seed, steps):
+    g = O.generate(n, seed, density, 1)
+    for s in range(steps):
+        want = O.step(g, R, rule)
+        got = tensor_step(g, R, rule)
+        assert np.array_equal(got, want), f"generation {s + 1}: {int((got != want).sum())} cells differ"
+        g = want
+
+
+def test_rule_lanes_every_count():
+    """Every box count and centre against the scalar rule, for rules with empty and
+    out-of-range intervals, in both lane widths (through the same constants)."""
+    for R in (1, 2, 5, 6, 12, 32):
+        N = (2 * R + 1) ** 2
+        for rule in [O.scaled_rule(R), (0, N, 0, N), (N, 0, 5, 3), (-3, 2, N + 5, N + 9), (4, 4, 4, 4)]:
+            P = plan(64, R, rule)
+            B = np.arange(N + 1, dtype=np.uint64)
+            smin, smax, bmin, bmax = rule
+            top = np.uint64(0x8000 if P["lanes16"] else 0x80)
+            mask = np.uint64(0xFFFF if P["lanes16"] else 0xFF)
+            nlo0, dlo, hiH0, dhi = (np.uint64(P[k]) for k in ("nlo0", "dlo", "hiH0", "dhi"))
+            for s in (0, 1):
+                k = B.astype(np.int64) - s
+                want = ((k >= smin) & (k <= smax)) if s else ((k >= bmin) & (k <= bmax))
+                sw = np.uint64(s)
+                # lane 0 only (the other lanes hold the same constants)
+                ge = (B + (nlo0 & mask) + sw * dlo) & M32
+                le = ((hiH0 & mask) + sw * dhi - B) & M32
+                got = (ge & le & top) != 0
+                valid = B >= s  # a live centre implies B >= 1
+                assert np.array_equal(got[valid], want[valid]), (R, rule, s)
