@@ -40,8 +40,12 @@ DENSITY = 0.5
 WORKLOAD = ("16384x16384 torus, R=5 Moore, Bosco S33-57/B34-45 (centre counted; reference S32-56/B34-45), "
             "start grid = reference generator --seed 1 -d 0.5 --threads 1")
 METRIC = "GCUPS (cell updates / s / 1e9) of generations of a 16384^2 LtL torus, R=5, bit-exact"
-BYTES_PER_UPDATE = {"plain": 2.0, "tensor": 2.0, "packed": 0.25}
-DTYPE = {"plain": "u8", "tensor": "u8 (tcgen05 kind::i8)", "packed": "b1 (32 cells per u32)"}
+# algorithmic HBM bytes per cell-update: one read and one write of the state
+# (uint8 cells for plain; bit-packed cells for packed and tensor, whose grids
+# live in the packed frame between generations)
+BYTES_PER_UPDATE = {"plain": 2.0, "tensor": 0.25, "packed": 0.25}
+DTYPE = {"plain": "u8", "tensor": "b1 state, u8 x u8 -> s32 operands (tcgen05 kind::i8)",
+         "packed": "b1 (32 cells per u32)"}
 REF_RULE_TAG = "R5_S32-56_B34-45"
 
 
@@ -76,7 +80,7 @@ def traffic_table():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks / throttle reasons sampled every 20 ms while running."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -190,11 +194,21 @@ def run_variant(C, torch, name, start, args, flush, sampler=None):
         passes = max(1, args.steps // depth)
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(passes)]
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(passes)]
+        if sampler:
+            # nvidia-smi samples every 20 ms, longer than the timed passes below
+            # (K passes of ~0.1 ms each): the sampler also covers a sustained,
+            # untimed run of the same passes (L2 flush included) right before them
+            sampler.start()
+            t_end = time.time() + 0.6
+            with torch.cuda.stream(stream):
+                while time.time() < t_end:
+                    for _ in range(20):
+                        flush.zero_()
+                        s.doSteps(depth)
+                    stream.synchronize()
         s.set_timing(True)
         barrier(args.world)
         torch.cuda.synchronize()
-        if sampler:
-            sampler.start()
         with torch.cuda.stream(stream):
             for p in range(passes):
                 flush.zero_()
@@ -249,23 +263,31 @@ def e2e_run(C, torch, name, start, steps):
         s.close()
 
 
-def radius_sweep(C, torch, args):
+SWEEP_POINTS = [(1, 2, 0.5), (2, 2, 0.5), (4, 2, 0.5), (8, 2, 0.5), (16, 2, 0.5), (32, 2, 0.5),
+                (64, 3, 0.3), (128, 3, 0.3)]
+
+
+def radius_sweep(C, torch, args, passes_per_variant, emit=None):
     """The radius-sweep workloads: 32768^2, seed 2, d = 0.5, R in {1,2,4,8,16,32},
-    scaled interval rule, and R in {64,128} at d = 0.3 (seed 3).  One JSON line per
+    scaled interval rule, and R in {64,128} at d = 0.3 (seed 3).  One record per
     radius with every variant's GCUPS (passes timed with CUDA events on the
     launching stream, L2 flushed before each pass), the step kernel's own GCUPS
-    (halo launches excluded) and its HBM roofline at 2 B (uint8) or 0.25 B
-    (packed) per cell-update.  Exactness at these sizes is covered by
-    tests/test_gpu_fullsize.py."""
+    (halo launches excluded) and its HBM roofline at the variant's algorithmic
+    bytes per cell-update.  Exactness at these sizes is covered by
+    tests/test_gpu_fullsize.py.  `emit(record)` is called per radius."""
     from cat_cpu_b200.workloads import scaled_rule
     n = 32768
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     vcodes = {"plain": C.VARIANT_PLAIN, "packed": C.VARIANT_PACKED, "tensor": C.VARIANT_TENSOR}
     peak, peak_kind = measured_peaks()
-    for radius, seed, dens in [(1, 2, 0.5), (2, 2, 0.5), (4, 2, 0.5), (8, 2, 0.5), (16, 2, 0.5), (32, 2, 0.5),
-                               (64, 3, 0.3), (128, 3, 0.3)]:
+    starts = {}
+    records = []
+    for radius, seed, dens in SWEEP_POINTS:
         rule = scaled_rule(radius)
-        start = C.start_grid(n, seed, dens, 1)
+        if (seed, dens) not in starts:
+            starts.clear()
+            starts[(seed, dens)] = C.start_grid(n, seed, dens, 1)
+        start = starts[(seed, dens)]
         out = {"workload": f"{n}x{n} torus, R={radius}, scaled interval rule, seed {seed}, d={dens}",
                "radius": radius, "unit": "GCUPS", "peak_kind": f"{peak_kind} hbm_gbs", "variants": {}}
         for name in [v for v in args.variants.split(",") if v]:
@@ -281,7 +303,7 @@ def radius_sweep(C, torch, args):
                 s.setState(start)
                 s.doSteps(3 * depth)
                 s.synchronize()
-                passes = max(1, min(args.sweep_steps, 200) // depth)
+                passes = max(1, passes_per_variant // depth)
                 ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                       for _ in range(passes)]
                 s.set_timing(True)
@@ -308,7 +330,10 @@ def radius_sweep(C, torch, args):
                                                       "bytes_per_update": BYTES_PER_UPDATE[name]}}
             finally:
                 s.close()
-        print(json.dumps(out), flush=True)
+        records.append(out)
+        if emit:
+            emit(out)
+    return records
 
 
 def strips_run(C, torch, args, world, rank, local):
@@ -489,6 +514,8 @@ def main():
                     help="one 16384^2 grid split into row strips across the ranks (strong scaling), "
                          "halo exchange every K generations, instead of the per-rank replicas")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true",
+                    help="skip the short radius sweep (32768^2, R = 1..128) that rank 0 appends to the line")
     ap.add_argument("--e2e-steps", type=int, default=None)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -503,7 +530,7 @@ def main():
     import cat_cpu_b200 as C
 
     if args.sweep:
-        radius_sweep(C, torch, args)
+        radius_sweep(C, torch, args, min(args.sweep_steps, 200), emit=lambda r: print(json.dumps(r), flush=True))
         return
     if args.strips > 0:
         r = strips_run(C, torch, args, world, rank, local)
@@ -603,6 +630,18 @@ def main():
                                                                                                 e2["steps"]),
                    "note": f"upload start grid from pinned host memory + {e2['steps']} steps + download, "
                            f"{best} variant"}
+    if rank == 0 and not args.no_sweep:
+        # the radius-sweep workloads (32768^2, R in {1,2,4,8,16,32} and {64,128}) at
+        # 4 timed generations per variant and radius; `bench.py --sweep` runs more
+        recs = radius_sweep(C, torch, args, 4)
+        line["radius_sweep"] = {
+            "workload": "32768x32768 torus, scaled interval rule; seed 2 d=0.5 for R<=32, seed 3 d=0.3 for R=64,128; "
+                        "4 generations per variant, L2 flushed before each, CUDA events",
+            "unit": "GCUPS",
+            "by_radius": {str(r["radius"]): {v: ({"gcups": d["gcups"], "kernel_gcups": d["kernel_gcups"],
+                                                  "hbm_frac": d["roofline"]["frac"]} if "gcups" in d else
+                                                 {"unsupported": d["unsupported"]})
+                                             for v, d in r["variants"].items()} for r in recs}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline_sample(os.cpu_count() or 1)
         if cb is not None:

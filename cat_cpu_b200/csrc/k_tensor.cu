@@ -51,18 +51,20 @@ using namespace tc;
 // ---------------------------------------------------------------------------
 // Geometry
 // ---------------------------------------------------------------------------
-constexpr int kAtomBytes = 128 * 128;    // one 128-row x 128-byte swizzle atom
-constexpr int kXBytes = 2 * kAtomBytes;  // X tile = 128 rows x 256 columns
-constexpr int kXStages = 4;
+constexpr int kAtomBytes = 128 * 128;  // one 128-row x 128-byte swizzle atom
+constexpr int kMaxAtoms = 4;           // X tile: 2..4 atoms = 256..512 columns
+constexpr int kMaxGroups = 4 * kMaxAtoms;  // 32-column groups per X row
+constexpr int kMaxStages = 4;
 constexpr int kHCol = 0;    // TMEM column of H
 constexpr int kCCol = 256;  // TMEM column of C
 constexpr int kN1 = 32;     // product-1 column chunk = one output word
 constexpr int kGroups = 4;  // epilogue column groups
 constexpr int kEpiWarps = 4 * kGroups;
-constexpr int kUnpackWarps = 4;
+constexpr int kUnpackWarps = 4;              // one X row per unpack thread
 constexpr int kEpiWarp0 = 1 + kUnpackWarps;  // warp 0: MMA, 1..4: unpack, 5..20: epilogue
 constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);
 constexpr int kMaxChunks = 7;  // Tc <= 224
+constexpr int kSmemLimit = 227 * 1024;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any legitimate wait
 
 struct TcParams {
@@ -72,33 +74,48 @@ struct TcParams {
     int n, nw;
     int R, PADC, glo, K1;  // column halo of a tile (16 mod 32), first window group, product-1 K
     int Tr, Tc, nchunks;
+    int half0;        // chunks of column half 0 (half 1 has nchunks - half0); each <= 4
+    int atoms;        // X tile width = 128 * atoms columns
+    int nb;           // 128-row X blocks per tile: product 2 contracts over 128 * nb rows
+    int stages;       // X ring stages
+    int nhs;          // H buffers in shared memory (1 or 2)
     int tiles_x, tiles_y;
-    int fast;     // n % 32 == 0 and n >= 256: word-aligned wrap with one correction
-    int lanes16;  // rule lanes: 0 = four 8-bit lanes (R <= 5), 1 = two 16-bit lanes
     uint32_t nlo0, dlo, hiH0, dhi;  // rule constants (lane-broadcast; d* = live minus dead, mod 2^32)
     uint32_t rq_mask[kGroups];      // bit i: this epilogue group re-quantises chunk i
     unsigned int* err;
     unsigned long long wait_ns;
-    int inject_missing_commit;  // test hook: product 1 of the first tile never signals
+    int inject_missing_commit;  // test hook: product 1 of the first unit never signals
 };
 
 struct SmemLayout {
     int x_off, hs_off, bh_off, bv_off, bar_off, tmem_off, total;
 };
 
-enum Bar { X_FULL = 0, X_EMPTY = kXStages, H_FULL = 2 * kXStages, HS_FULL, C_FULL, C_EMPTY, DRAIN, NBARS };
+enum Bar {
+    X_FULL = 0,
+    X_EMPTY = kMaxStages,
+    H_FULL = 2 * kMaxStages,  // [2]: per TMEM column half
+    HS_FULL = H_FULL + 2,     // [2]
+    HS_EMPTY = HS_FULL + 2,   // [2]: per shared-memory H buffer
+    C_FULL = HS_EMPTY + 2,    // [2]
+    C_EMPTY = C_FULL + 2,     // [2]
+    DRAIN = C_EMPTY + 2,
+    NBARS
+};
 
-__host__ __device__ inline SmemLayout smem_layout(int Tc, int K1) {
+constexpr int kHalfCols = 128;  // TMEM columns of one half's H or C (4 chunks)
+
+__host__ __device__ inline SmemLayout smem_layout(int stages, int atoms, int nhs, int K1, int nb) {
     SmemLayout L{};
     int o = 0;
     L.x_off = o;
-    o += kXStages * kXBytes;  // 1024-aligned stages
+    o += stages * atoms * kAtomBytes;  // 1024-aligned stages
     L.hs_off = o;
-    o += 2 * 128 * Tc;        // H as u8, MN-major, two buffers (tile parity)
+    o += nhs * 128 * kHalfCols;        // one half's H as u8, MN-major, one or two buffers
     L.bh_off = o;
-    o += kN1 * K1;            // B_h
+    o += kN1 * K1;                     // B_h
     L.bv_off = o;
-    o += 128 * 128;           // B_v
+    o += 128 * 128 * nb;               // B_v, 128 x (128 nb)
     o = (o + 7) & ~7;
     L.bar_off = o;
     o += NBARS * 8;
@@ -141,10 +158,22 @@ __device__ __forceinline__ uint32_t fetch32(const uint32_t* __restrict__ row, in
     return v;
 }
 
+// The work is a stream of units u = ((tile j * nb + row block b) * 2 + column
+// half h).  Per X block (j, b) the unpack warps fill one stage; per unit the MMA
+// warp runs product 1 for the half's chunks into TMEM half h of H, the epilogue
+// re-quantises it to shared memory, and product 2 adds B_v[:, 128b ..] * H to
+// TMEM half h of C.  After a tile's last block the epilogue applies the rule to
+// C half h.  The two halves use separate TMEM columns (H: [0, 256), C: [256,
+// 512)), so the tensor core works on one half while the epilogue reads the other.
+//
+// LANES16: rule lanes (four 8-bit, or two 16-bit); CENTRE_SMEM: centre cells
+// from the X tile (single-block tiles) or from the packed input word; FAST:
+// n % 32 == 0 and large enough that rows and words wrap with one correction.
+template <bool LANES16, bool CENTRE_SMEM, bool FAST>
 __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_constant__ TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const SmemLayout L = smem_layout(p.Tc, p.K1);
+    const SmemLayout L = smem_layout(p.stages, p.atoms, p.nhs, p.K1, p.nb);
     uint8_t* xs = smem + L.x_off;
     uint8_t* hs = smem + L.hs_off;
     uint8_t* bh = smem + L.bh_off;
@@ -153,21 +182,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
     uint32_t* tmem_slot = (uint32_t*)(smem + L.tmem_off);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int R = p.R, Tc = p.Tc, K1 = p.K1;
+    const int R = p.R, Tc = p.Tc, K1 = p.K1, nb = p.nb, S = p.stages, nhs = p.nhs;
+    const int xbytes = p.atoms * kAtomBytes;
     const int ntiles = p.tiles_x * p.tiles_y;
     int mine = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) ++mine;
+    const int units = mine * nb * 2;
     constexpr uint32_t kTmemCols = 512;
 
     if (tid == 0) {
-        for (int i = 0; i < kXStages; ++i) {
+        for (int i = 0; i < S; ++i) {
             mbar_init(&bars[X_FULL + i], kUnpackWarps);
-            mbar_init(&bars[X_EMPTY + i], kEpiWarps);
+            mbar_init(&bars[X_EMPTY + i], CENTRE_SMEM ? kEpiWarps : 1);
         }
-        mbar_init(&bars[H_FULL], 1);
-        mbar_init(&bars[HS_FULL], kEpiWarps);
-        mbar_init(&bars[C_FULL], 1);
-        mbar_init(&bars[C_EMPTY], kEpiWarps);
+        for (int h = 0; h < 2; ++h) {
+            mbar_init(&bars[H_FULL + h], 1);
+            mbar_init(&bars[HS_FULL + h], kEpiWarps);
+            mbar_init(&bars[HS_EMPTY + h], 1);
+            mbar_init(&bars[C_FULL + h], 1);
+            mbar_init(&bars[C_EMPTY + h], kEpiWarps);
+        }
         mbar_init(&bars[DRAIN], 1);
         fence_mbar_init();
     }
@@ -178,11 +212,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
     for (int idx = tid; idx < kN1 * K1; idx += kThreads) {
         const int k = idx / kN1, nn = idx % kN1;
         const int xc = 32 * (p.glo + (k >> 5)) + perm_pi(k & 31);  // X column relative to the chunk
-        const int d = xc - p.PADC - perm_sigma(nn, p.lanes16);
+        const int d = xc - p.PADC - perm_sigma(nn, LANES16);
         bh[((k >> 4) * kN1 + nn) * 16 + (k & 15)] = (d >= -R && d <= R) ? 1 : 0;
     }
-    // B_v[m][k] = [m <= k <= m + 2R], m, k < 128 (16 bytes per store)
-    for (int idx = tid; idx < 8 * 128; idx += kThreads) {
+    // B_v[m][k] = [m <= k <= m + 2R], m < 128, k < 128 nb (K-major, no swizzle, 16 bytes per store)
+    for (int idx = tid; idx < 8 * nb * 128; idx += kThreads) {
         const int kc = idx / 128, m = idx % 128;
         uint32_t w[4];
 #pragma unroll
@@ -202,51 +236,62 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tmem_slot;
+    const int half0 = p.half0, nch = p.nchunks;
 
     if (warp == 0) {
         // --------------------------- MMA issuer -----------------------------
         if (lane == 0) {
             const uint32_t ba = smem_u32(bh), va = smem_u32(bv), ha0 = smem_u32(hs);
             const uint32_t id1 = idesc_u8(kN1, false);
-            const uint32_t id2 = idesc_u8(Tc, true);
+            const uint32_t id2a = idesc_u8(32 * half0, true), id2b = idesc_u8(32 * (nch - half0), true);
             const int ksteps = K1 / 32;
-            auto product1 = [&](int j) -> bool {
-                const int st = j % kXStages;
-                if (!mbar_wait(&bars[X_FULL + st], (uint32_t)(j / kXStages) & 1u, p.wait_ns)) return false;
+            auto product1 = [&](int u) -> bool {
+                const int h = u & 1, xi = u >> 1;  // X block index (j * nb + b)
+                const int st = xi % S;
+                if (!mbar_wait(&bars[X_FULL + st], (uint32_t)(xi / S) & 1u, p.wait_ns)) return false;
                 fence_after();
-                const uint32_t xa = smem_u32(xs + st * kXBytes);
-                for (int i = 0; i < p.nchunks; ++i) {
+                const uint32_t xa = smem_u32(xs + st * xbytes);
+                const int c0 = h ? half0 : 0, c1 = h ? nch : half0;
+                for (int i = c0; i < c1; ++i) {
                     for (int s = 0; s < ksteps; ++s) {
                         const int col = 32 * (i + p.glo + s);  // X column of this K step
                         const uint64_t ad = desc_k_sw128(xa + (col >> 7) * kAtomBytes + (col & 127));
                         const uint64_t bd = desc_noswz(ba + s * 2 * kN1 * 16, kN1 * 16, 128);
-                        mma_i8(tmem + kHCol + kN1 * i, ad, bd, id1, s > 0 ? 1u : 0u);
+                        mma_i8(tmem + kHCol + kHalfCols * h + kN1 * (i - c0), ad, bd, id1, s > 0 ? 1u : 0u);
                     }
                 }
-                if (!(p.inject_missing_commit && j == 0)) mma_commit(&bars[H_FULL]);
+                if (!(p.inject_missing_commit && u == 0)) mma_commit(&bars[H_FULL + h]);
+                // the centre cells come from global memory: the stage is free once both halves read it
+                if (!CENTRE_SMEM && h == 1) mma_commit(&bars[X_EMPTY + st]);
                 return true;
             };
-            // product 2 of tile j: C = B_v * H(j), H(j) in shared-memory buffer j % 2
-            auto product2 = [&](int j) -> bool {
-                if (j >= 1 && !mbar_wait(&bars[C_EMPTY], (uint32_t)(j - 1) & 1u, p.wait_ns)) return false;
+            // product 2 of unit u: C[h] (+)= B_v[:, 128b ..] * H(u), H(u) in buffer u % nhs
+            auto product2 = [&](int u) -> bool {
+                const int h = u & 1, xi = u >> 1, b = xi % nb, j = xi / nb;
+                if (b == 0 && j >= 1 && !mbar_wait(&bars[C_EMPTY + h], (uint32_t)(j - 1) & 1u, p.wait_ns))
+                    return false;
                 fence_after();
-                const uint32_t ha = ha0 + (j & 1) * 128 * Tc;
+                const uint32_t ha = ha0 + (u % nhs) * 128 * kHalfCols;
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
-                    const uint64_t ad = desc_noswz(va + s * 2 * 128 * 16, 128 * 16, 128);
+                    const uint64_t ad = desc_noswz(va + (4 * b + s) * 2 * 128 * 16, 128 * 16, 128);
                     const uint64_t bd = desc_noswz(ha + s * 32 * 16, 128, 128 * 16);
-                    mma_i8(tmem + kCCol, ad, bd, id2, s > 0 ? 1u : 0u);
+                    mma_i8(tmem + kCCol + kHalfCols * h, ad, bd, h ? id2b : id2a, (b > 0 || s > 0) ? 1u : 0u);
                 }
-                mma_commit(&bars[C_FULL]);
+                mma_commit(&bars[HS_EMPTY + (u % nhs)]);
+                if (b == nb - 1) mma_commit(&bars[C_FULL + h]);
                 return true;
             };
-            // Order per tile j: product 1 of tile j+1 as soon as H(j) has been read
-            // back, then product 2 of tile j once C(j-1) has been read.
-            bool ok = mine >= 1 ? product1(0) : true;
-            for (int j = 0; j < mine && ok; ++j) {
-                ok = mbar_wait(&bars[HS_FULL], (uint32_t)j & 1u, p.wait_ns);
-                if (ok && j + 1 < mine) ok = product1(j + 1);
-                if (ok) ok = product2(j);
+            // Per unit u, once H(u) has been read back: product 2 of unit u (the
+            // epilogue waits for it next), then product 1 of unit u+2 into the
+            // TMEM half that H(u) has just left.
+            bool ok = true;
+            if (units >= 1) ok = product1(0);
+            if (ok && units >= 2) ok = product1(1);
+            for (int u = 0; u < units && ok; ++u) {
+                ok = mbar_wait(&bars[HS_FULL + (u & 1)], (uint32_t)(u >> 1) & 1u, p.wait_ns);
+                if (ok) ok = product2(u);
+                if (ok && u + 2 < units) ok = product1(u + 2);
             }
             if (!ok) atomicOr(p.err, 2u);
             // never leave with an MMA in flight (TMEM is freed below)
@@ -255,72 +300,72 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         }
     } else if (warp < kEpiWarp0) {
         // ------------------------------ unpack ------------------------------
-        // 128 threads fill a stage: 128 rows x 8 groups of 32 columns.  Thread
-        // ut always handles group g = ut % 8 of rows ut / 8 + 16 q, q = 0..7
-        // (4 rows x 8 groups per warp and round).  The words of the next tile are
-        // loaded while this one is spread and stored, so the loads' latency is
-        // spent waiting for a free stage rather than on the critical path.
-        const int ut = tid - 32;
-        const int g = ut & 7;
-        // the 8 groups (32 cells each, bit b = cell b) this thread stores for tile t
-        auto gather = [&](int t, uint32_t (&x)[8]) {
+        // Thread `row` (0..127) fills X row `row` of every stage: the 4*atoms
+        // groups of 32 columns of one packed row.  The words of the next X block
+        // are loaded right after this one is stored, so their latency is spent
+        // waiting for a free stage rather than on the critical path.
+        const int row = tid - 32;
+        const int ng = 4 * p.atoms;
+        const int sw = row & 7;
+        const int blocks = mine * nb;
+        uint32_t w[kMaxGroups + 1];
+        // FAST: the ng + 1 words that hold X row `row` of block xi (group g = upper
+        // half of word g, lower half of word g + 1); otherwise the ng groups
+        auto gather = [&](int xi) {
+            const int t = blockIdx.x + (xi / nb) * gridDim.x;
             const int ty = t / p.tiles_x, tx = t % p.tiles_x;
-            const int rbase = ty * p.Tr - R;
+            const int gr0 = ty * p.Tr - R + 128 * (xi % nb) + row;
             const int cbase = tx * Tc - p.PADC;  // column of X-tile column 0 (16 mod 32)
-            if (p.fast) {
-                int wl = (cbase + 32 * g - 16) >> 5;  // word holding the group's first cell
-                if (wl < 0) wl += p.nw;
-                else if (wl >= p.nw) wl -= p.nw;
-                const int wr = wl + 1 == p.nw ? 0 : wl + 1;
-                uint32_t lo[8], hi[8];
+            if (FAST) {
+                int gr = gr0;
+                if (gr < 0) gr += p.n;
+                else if (gr >= p.n) gr -= p.n;
+                const uint32_t* rp = p.src + (size_t)gr * (size_t)p.wpitch;
+                const int wl0 = (cbase - 16) >> 5;  // word holding X column 0
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    int gr = rbase + (ut >> 3) + 16 * q;
-                    if (gr < 0) gr += p.n;
-                    else if (gr >= p.n) gr -= p.n;
-                    const uint32_t* rp = p.src + (size_t)gr * (size_t)p.wpitch;
-                    lo[q] = __ldg(rp + wl);
-                    hi[q] = __ldg(rp + wr);
+                for (int k = 0; k <= kMaxGroups; ++k) {
+                    if (k <= ng) {
+                        int wi = wl0 + k;
+                        if (wi < 0) wi += p.nw;
+                        else if (wi >= p.nw) wi -= p.nw;
+                        w[k] = __ldg(rp + wi);
+                    }
                 }
-#pragma unroll
-                for (int q = 0; q < 8; ++q) x[q] = prmt(lo[q], hi[q], 0x5432u);  // upper half of wl, lower of wr
             } else {
-                const int a = wrap_slow(cbase + 32 * g, p.n);
-                for (int q = 0; q < 8; ++q) {
-                    const int gr = wrap_slow(rbase + (ut >> 3) + 16 * q, p.n);
-                    x[q] = fetch32(p.src + (size_t)gr * (size_t)p.wpitch, a, p.n);
-                }
+                const uint32_t* rp = p.src + (size_t)wrap_slow(gr0, p.n) * (size_t)p.wpitch;
+#pragma unroll
+                for (int k = 0; k < kMaxGroups; ++k)
+                    if (k < ng) w[k] = fetch32(rp, wrap_slow(cbase + 32 * k, p.n), p.n);
             }
         };
         bool ok = true;
-        int it = 0;
-        uint32_t x[8];
-        if ((int)blockIdx.x < ntiles) gather(blockIdx.x, x);
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
-            const int st = it % kXStages;
-            if (it >= kXStages) {
-                bool w = true;
-                if (lane == 0) w = mbar_wait(&bars[X_EMPTY + st], ((uint32_t)(it / kXStages) & 1u) ^ 1u, p.wait_ns);
-                ok = __shfl_sync(0xffffffffu, w, 0);
+        if (blocks > 0) gather(0);
+        for (int xi = 0; xi < blocks; ++xi) {
+            const int st = xi % S;
+            if (xi >= S) {
+                bool wt = true;
+                if (lane == 0) wt = mbar_wait(&bars[X_EMPTY + st], ((uint32_t)(xi / S) & 1u) ^ 1u, p.wait_ns);
+                ok = __shfl_sync(0xffffffffu, wt, 0);
                 if (!ok) break;
             }
-            uint8_t* xst = xs + st * kXBytes + (g >> 2) * kAtomBytes;
-            const int ch = 2 * (g & 3);
+            uint8_t* xrow = xs + st * xbytes + row * 128;
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int row = (ut >> 3) + 16 * q;
-                uint32_t u[8];
+            for (int g = 0; g < kMaxGroups; ++g) {
+                if (g < ng) {
+                    const uint32_t x = FAST ? prmt(w[g], w[g + 1], 0x5432u) : w[g];
+                    uint32_t v[8];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) u[k] = (x[q] >> k) & 0x01010101u;
-                uint8_t* rowp = xst + row * 128;
-                const int sw = row & 7;
-                *(uint4*)(rowp + ((ch ^ sw) << 4)) = make_uint4(u[0], u[1], u[2], u[3]);
-                *(uint4*)(rowp + (((ch + 1) ^ sw) << 4)) = make_uint4(u[4], u[5], u[6], u[7]);
+                    for (int k = 0; k < 8; ++k) v[k] = (x >> k) & 0x01010101u;
+                    uint8_t* ap = xrow + (g >> 2) * kAtomBytes;
+                    const int ch = 2 * (g & 3);
+                    *(uint4*)(ap + ((ch ^ sw) << 4)) = make_uint4(v[0], v[1], v[2], v[3]);
+                    *(uint4*)(ap + (((ch + 1) ^ sw) << 4)) = make_uint4(v[4], v[5], v[6], v[7]);
+                }
             }
             fence_proxy_async();
             __syncwarp();
             if (lane == 0) mbar_arrive(&bars[X_FULL + st]);
-            if (t + (int)gridDim.x < ntiles) gather(t + gridDim.x, x);
+            if (xi + 1 < blocks) gather(xi + 1);
         }
         if (!ok && lane == 0) atomicOr(p.err, 4u);
     } else {
@@ -332,104 +377,127 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
         const uint32_t rq_mask = p.rq_mask[grp];
         const int aoff = (p.PADC - 16) >> 5;  // centre groups of chunk i: i + aoff, i + aoff + 1
+        const uint32_t nlo0 = p.nlo0, dlo = p.dlo, hiH0 = p.hiH0, dhi = p.dhi;
         bool ok = true;
         auto wait_all = [&](uint64_t* bar, uint32_t ph) -> bool {
-            const bool w = mbar_wait(bar, ph, p.wait_ns);
-            return __all_sync(0xffffffffu, w);
+            const bool wt = mbar_wait(bar, ph, p.wait_ns);
+            return __all_sync(0xffffffffu, wt);
         };
-        // re-quantise H(j) to u8 into shared-memory buffer j % 2 (MN-major B operand of product 2)
-        auto requant = [&](int j) -> bool {
-            if (!wait_all(&bars[H_FULL], (uint32_t)j & 1u)) return false;
+        // re-quantise H(u) to u8 into shared-memory buffer u % nhs (MN-major B operand of product 2)
+        auto requant = [&](int u) -> bool {
+            const int h = u & 1;
+            if (!wait_all(&bars[H_FULL + h], (uint32_t)(u >> 1) & 1u)) return false;
+            const int k = u / nhs;
+            if (k >= 1 && !wait_all(&bars[HS_EMPTY + (u % nhs)], (uint32_t)(k - 1) & 1u)) return false;
             fence_after();
-            uint8_t* hsb = hs + (j & 1) * 128 * Tc;
-            for (int i = 0; i < p.nchunks; ++i) {
+            uint8_t* hsb = hs + (u % nhs) * 128 * kHalfCols;
+            const int c0 = h ? half0 : 0, c1 = h ? nch : half0;
+            for (int i = c0; i < c1; ++i) {
                 if (!((rq_mask >> i) & 1u)) continue;
                 uint32_t v[16];
-                tmem_ld32p(tmem + lane_off + kHCol + kN1 * i, v);
+                tmem_ld32p(tmem + lane_off + kHCol + kHalfCols * h + kN1 * (i - c0), v);
                 tmem_wait16(v);
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    uint4 w;
-                    w.x = prmt(v[8 * h + 0], v[8 * h + 1], 0x6420u);
-                    w.y = prmt(v[8 * h + 2], v[8 * h + 3], 0x6420u);
-                    w.z = prmt(v[8 * h + 4], v[8 * h + 5], 0x6420u);
-                    w.w = prmt(v[8 * h + 6], v[8 * h + 7], 0x6420u);
-                    *(uint4*)(hsb + ((2 * i + h) * 128 + m) * 16) = w;
+                for (int hh = 0; hh < 2; ++hh) {
+                    uint4 wv;
+                    wv.x = prmt(v[8 * hh + 0], v[8 * hh + 1], 0x6420u);
+                    wv.y = prmt(v[8 * hh + 2], v[8 * hh + 3], 0x6420u);
+                    wv.z = prmt(v[8 * hh + 4], v[8 * hh + 5], 0x6420u);
+                    wv.w = prmt(v[8 * hh + 6], v[8 * hh + 7], 0x6420u);
+                    *(uint4*)(hsb + ((2 * (i - c0) + hh) * 128 + m) * 16) = wv;
                 }
             }
             fence_proxy_async();
             fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bars[HS_FULL]);
+            if (lane == 0) mbar_arrive(&bars[HS_FULL + h]);
             return true;
         };
-        if (mine >= 1) ok = requant(0);
-        int t = blockIdx.x;
-        for (int j = 0; j < mine && ok; ++j, t += gridDim.x) {
-            if (j + 1 < mine && !requant(j + 1)) {
-                ok = false;
-                break;
-            }
-            // rule + store C(j)
-            if (!wait_all(&bars[C_FULL], (uint32_t)j & 1u)) {
-                ok = false;
-                break;
-            }
+        // rule + store of column half h of C(j)
+        auto rule = [&](int j, int h) -> bool {
+            if (!wait_all(&bars[C_FULL + h], (uint32_t)j & 1u)) return false;
             fence_after();
-            const int st = j % kXStages;
+            const int t = blockIdx.x + j * gridDim.x;
+            const int st = j % S;  // (CENTRE_SMEM: one X block per tile)
             const int ty = t / p.tiles_x, tx = t % p.tiles_x;
             const int gi = ty * p.Tr + m;
             const bool row_ok = (m < p.Tr) && (gi < p.n);
             const int xr = min(m + R, 127);  // X row of this output row's centre cells (rows >= Tr are not stored)
-            const uint8_t* xrow = xs + st * kXBytes + xr * 128;
+            const uint8_t* xrow = xs + st * xbytes + xr * 128;
             const int sw = xr & 7;
             uint32_t* orow = p.dst + (size_t)(row_ok ? gi : 0) * (size_t)p.wpitch;
+            const uint32_t* crow = p.src + (size_t)(row_ok ? gi : 0) * (size_t)p.wpitch;
             const int w0 = tx * (Tc >> 5);
-            for (int i = grp; i < p.nchunks; i += kGroups) {
+            const int c0 = h ? half0 : 0, c1 = h ? nch : half0;
+            for (int i = c0 + grp; i < c1; i += kGroups) {
                 uint32_t v[16];
-                tmem_ld32p(tmem + lane_off + kCCol + kN1 * i, v);
-                // centre cells: groups ga and ga + 1 of the X row (8 words each)
-                const int ga = i + aoff, gb = ga + 1;
-                const uint4 a0 = *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3)) ^ sw) << 4));
-                const uint4 a1 = *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3) + 1) ^ sw) << 4));
-                const uint4 b0 = *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3)) ^ sw) << 4));
-                const uint4 b1 = *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3) + 1) ^ sw) << 4));
-                const uint32_t Ga[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-                const uint32_t Gb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+                tmem_ld32p(tmem + lane_off + kCCol + kHalfCols * h + kN1 * (i - c0), v);
+                const int wi = w0 + i;
+                const bool store = row_ok && wi < p.nw;
+                uint32_t Ga[8], Gb[8];
+                uint32_t cw = 0u;
+                if (CENTRE_SMEM) {
+                    // centre cells: groups ga and ga + 1 of the X row (8 words each)
+                    const int ga = i + aoff, gb = ga + 1;
+                    const uint4 a0 = *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3)) ^ sw) << 4));
+                    const uint4 a1 =
+                        *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3) + 1) ^ sw) << 4));
+                    const uint4 b0 = *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3)) ^ sw) << 4));
+                    const uint4 b1 =
+                        *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3) + 1) ^ sw) << 4));
+                    Ga[0] = a0.x; Ga[1] = a0.y; Ga[2] = a0.z; Ga[3] = a0.w;
+                    Ga[4] = a1.x; Ga[5] = a1.y; Ga[6] = a1.z; Ga[7] = a1.w;
+                    Gb[0] = b0.x; Gb[1] = b0.y; Gb[2] = b0.z; Gb[3] = b0.w;
+                    Gb[4] = b1.x; Gb[5] = b1.y; Gb[6] = b1.z; Gb[7] = b1.w;
+                } else {
+                    // the output word's own cells in the current grid (word-aligned)
+                    cw = store ? __ldg(crow + wi) : 0u;
+                }
                 tmem_wait16(v);
                 uint32_t acc = 0u;
-                if (!p.lanes16) {
+                if (!LANES16) {
                     // accumulator column 4k+j = output cell 8j+k: four box counts per
                     // register, bit 7 of each byte lane = the rule's result
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
                         const uint32_t B4 = prmt(v[2 * k], v[2 * k + 1], 0x6420u);
-                        const uint32_t s4 = prmt(Ga[k], Gb[k], 0x5432u);
-                        const uint32_t ge = (B4 + p.nlo0) + s4 * p.dlo;  // bit 7: B >= lo(s)
-                        const uint32_t le = (p.hiH0 + s4 * p.dhi) - B4;  // bit 7: B <= hi(s)
+                        const uint32_t s4 = CENTRE_SMEM ? prmt(Ga[k], Gb[k], 0x5432u) : (cw >> k) & 0x01010101u;
+                        const uint32_t ge = (B4 + nlo0) + s4 * dlo;  // bit 7: B >= lo(s)
+                        const uint32_t le = (hiH0 + s4 * dhi) - B4;  // bit 7: B <= hi(s)
                         acc |= (ge & le & 0x80808080u) >> (7 - k);
                     }
                 } else {
-                    // accumulator column 2r+h = output cell 16h+r: two box counts per
+                    // accumulator column 2r+e = output cell 16e+r: two box counts per
                     // register, bit 15 of each 16-bit lane = the rule's result
 #pragma unroll
                     for (int r = 0; r < 16; ++r) {
                         const uint32_t hsel = (uint32_t)(r >> 3);
-                        const uint32_t s2 = prmt(Ga[r & 7], Gb[r & 7], (2u + hsel) | 0x80u | ((4u + hsel) << 8) | 0x8000u);
-                        const uint32_t ge = (v[r] + p.nlo0) + s2 * p.dlo;
-                        const uint32_t le = (p.hiH0 + s2 * p.dhi) - v[r];
+                        const uint32_t s2 = CENTRE_SMEM ? prmt(Ga[r & 7], Gb[r & 7],
+                                                               (2u + hsel) | 0x80u | ((4u + hsel) << 8) | 0x8000u)
+                                                        : (cw >> r) & 0x00010001u;
+                        const uint32_t ge = (v[r] + nlo0) + s2 * dlo;
+                        const uint32_t le = (hiH0 + s2 * dhi) - v[r];
                         acc |= (ge & le & 0x80008000u) >> (15 - r);
                     }
                 }
-                const int wi = w0 + i;
-                if (row_ok && wi < p.nw) orow[wi] = acc;
+                if (store) orow[wi] = acc;
             }
             fence_before();
             __syncwarp();
             if (lane == 0) {
-                mbar_arrive(&bars[C_EMPTY]);
-                mbar_arrive(&bars[X_EMPTY + st]);
+                mbar_arrive(&bars[C_EMPTY + h]);
+                if (CENTRE_SMEM && h == 1) mbar_arrive(&bars[X_EMPTY + st]);
             }
+            return true;
+        };
+        if (units >= 1) ok = requant(0);
+        for (int u = 0; u < units && ok; ++u) {
+            if (u + 1 < units && !requant(u + 1)) {
+                ok = false;
+                break;
+            }
+            const int xi = u >> 1;
+            if (xi % nb == nb - 1 && !rule(xi / nb, u & 1)) ok = false;
         }
         if (!ok && lane == 0) atomicOr(p.err, 8u);
     }
@@ -445,16 +513,32 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
+using TcKernel = void (*)(TcParams);
+
 struct TensorPlan {
     TcParams prm[2];  // source frame a -> b, b -> a
+    TcKernel kernel;
     int smem_bytes;
     int grid;
     unsigned int* err;
 };
 
+template <bool L16, bool CS>
+static TcKernel pick_fast(bool fast) {
+    return fast ? k_tensor_step<L16, CS, true> : k_tensor_step<L16, CS, false>;
+}
+static TcKernel pick_kernel(bool lanes16, bool centre_smem, bool fast) {
+    if (lanes16) return centre_smem ? pick_fast<true, true>(fast) : pick_fast<true, false>(fast);
+    return centre_smem ? pick_fast<false, true>(fast) : pick_fast<false, false>(fast);
+}
+
+// Largest radius of the tensor step: box counts (2R+1)^2 must fit the 16-bit
+// rule lanes (< 2^15) and row sums 2R+1 the u8 operand of product 2.
+constexpr int kTensorMaxRadius = 90;
+
 bool tensor_supported(int n, int radius, char* why, size_t why_len) {
-    if (radius < 1 || radius > 32) {
-        snprintf(why, why_len, "tensor variant supports 1 <= R <= 32 (got %d)", radius);
+    if (radius < 1 || radius > kTensorMaxRadius) {
+        snprintf(why, why_len, "tensor variant supports 1 <= R <= %d (got %d)", kTensorMaxRadius, radius);
         return false;
     }
     if (n < radius) {
@@ -481,6 +565,57 @@ static void lane_consts(int lo, int hi, int bits, int& nlo, int& hiH) {
     hiH = top + hi;
 }
 
+// Tile geometry for radius R (also restated in tests/test_tensor_tiles.py):
+//   PADC = 16 + 32a >= R columns of halo on each side of the Tc output columns
+//          (16 mod 32, so that every X group straddles two packed words by halves);
+//   the X tile is 2..4 swizzle atoms wide, chosen to minimise X columns per output
+//          column, with Tc <= 224 so that H and C fit 512 TMEM columns;
+//   nb = 1 row block for R <= 32 (Tr = 128 - 2R output rows per tile), else
+//          enough 128-row blocks for Tr = 128 rows plus 2R halo rows;
+//   K1 = the product-1 window of one 32-column chunk, whole 32-column groups.
+struct TensorGeometry {
+    int PADC, atoms, Tc, Tr, nb, glo, ghi, K1, nchunks, half0, lanes16, stages, nhs;
+};
+
+static bool tensor_geometry(int R, TensorGeometry& G) {
+    G.PADC = R <= 16 ? 16 : 16 + 32 * ((R - 16 + 31) / 32);
+    G.nb = R <= 32 ? 1 : (128 + 2 * R + 127) / 128;
+    G.Tr = G.nb == 1 ? 128 - 2 * R : std::min(128, 128 * G.nb - 2 * R);
+    G.atoms = 0;
+    double best = 1e30;
+    for (int a = 2; a <= kMaxAtoms; ++a) {
+        const int tc = std::min(32 * kMaxChunks, ((128 * a - 2 * G.PADC) / 32) * 32);
+        if (tc < 32) continue;
+        const double cost = 128.0 * a / tc;
+        if (cost < best - 1e-9) {
+            best = cost;
+            G.atoms = a;
+            G.Tc = tc;
+        }
+    }
+    if (!G.atoms || G.Tr < 1) return false;
+    G.nchunks = G.Tc / 32;
+    G.half0 = (G.nchunks + 1) / 2;  // <= 4 chunks = 128 TMEM columns per half
+    G.glo = (G.PADC - R) / 32;
+    G.ghi = (G.PADC + 31 + R) / 32;
+    G.K1 = 32 * (G.ghi - G.glo + 1);
+    G.lanes16 = (2 * R + 1) * (2 * R + 1) > 127 ? 1 : 0;
+    const int ng = 4 * G.atoms;
+    if ((G.nchunks - 1) + G.ghi > ng - 1) return false;                                   // product-1 windows
+    if (G.nb == 1 && (G.nchunks - 1) + (G.PADC - 16) / 32 + 1 > ng - 1) return false;     // centre groups
+    if ((2 * R + 1) * (2 * R + 1) >= (1 << 15) || 2 * R + 1 > 255) return false;
+    // deepest X ring and double H buffers that fit, in that order of preference
+    static const int pref[][2] = {{4, 2}, {3, 2}, {2, 2}, {2, 1}, {1, 2}, {1, 1}};
+    for (const auto& pr : pref) {
+        if (smem_layout(pr[0], G.atoms, pr[1], G.K1, G.nb).total + 1024 <= kSmemLimit) {
+            G.stages = pr[0];
+            G.nhs = pr[1];
+            return true;
+        }
+    }
+    return false;
+}
+
 TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const Rule& rule, int device, char* why,
                                size_t why_len) {
     if (!tensor_supported(a.n, rule.radius, why, why_len)) return nullptr;
@@ -494,39 +629,36 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
         snprintf(why, why_len, "packed frames need a halo word");
         return nullptr;
     }
-    TensorPlan* P = new TensorPlan();
     const int R = rule.radius;
-    const int PADC = R <= 16 ? 16 : 48;
-    const int Tc = 256 - 2 * PADC;  // 224 or 160
-    const int Tr = 128 - 2 * R;
-    const int glo = (PADC - R) / 32;
-    const int ghi = (PADC + 31 + R) / 32;
-    const int K1 = 32 * (ghi - glo + 1);
-    const int nchunks = Tc / 32;
-    const int lanes16 = (2 * R + 1) * (2 * R + 1) > 127 ? 1 : 0;
-    const int bits = lanes16 ? 16 : 8;
-    const uint32_t bcast = lanes16 ? 0x00010001u : 0x01010101u;
+    TensorGeometry G{};
+    if (!tensor_geometry(R, G)) {
+        snprintf(why, why_len, "no tile shape for R=%d", R);
+        return nullptr;
+    }
+    TensorPlan* P = new TensorPlan();
+    const int bits = G.lanes16 ? 16 : 8;
+    const uint32_t bcast = G.lanes16 ? 0x00010001u : 0x01010101u;
     int nlo_d, hiH_d, nlo_s, hiH_s;
     lane_consts(rule.bmin, rule.bmax, bits, nlo_d, hiH_d);
     lane_consts(rule.smin + 1, rule.smax + 1, bits, nlo_s, hiH_s);
-    if (Tr < 1 || nchunks > kMaxChunks || (nchunks - 1) + (PADC - 16) / 32 + 1 > 7 || (nchunks - 1) + ghi > 7) {
-        snprintf(why, why_len, "no tile shape for R=%d", R);
-        delete P;
-        return nullptr;
-    }
-    // epilogue balance: the rule of chunk i runs on group i % 4; each
-    // re-quantisation (about a quarter of a rule chunk's work) goes to the
-    // group with the least work so far
+    // epilogue balance, per column half: the rule of the half's chunk c runs on
+    // group c % 4; each re-quantisation (about a quarter of a rule chunk's work,
+    // nb per tile) goes to the group with the least work in that half so far
     uint32_t rq_mask[kGroups] = {0, 0, 0, 0};
-    int load[kGroups] = {0, 0, 0, 0};
-    for (int i = 0; i < nchunks; ++i) load[i % kGroups] += 4;
-    for (int i = 0; i < nchunks; ++i) {
-        int g = 0;
-        for (int h = 1; h < kGroups; ++h)
-            if (load[h] < load[g]) g = h;
-        rq_mask[g] |= 1u << i;
-        load[g] += 1;
+    for (int h = 0; h < 2; ++h) {
+        const int c0 = h ? G.half0 : 0, c1 = h ? G.nchunks : G.half0;
+        int load[kGroups] = {0, 0, 0, 0};
+        for (int i = c0; i < c1; ++i) load[(i - c0) % kGroups] += 4;
+        for (int i = c0; i < c1; ++i) {
+            int g = 0;
+            for (int k = 1; k < kGroups; ++k)
+                if (load[k] < load[g]) g = k;
+            rq_mask[g] |= 1u << i;
+            load[g] += G.nb;
+        }
     }
+    const int ng = 4 * G.atoms;
+    const int nw = a.nw;
     const PackedFrame* src[2] = {&a, &b};
     const PackedFrame* dst[2] = {&b, &a};
     for (int i = 0; i < 2; ++i) {
@@ -535,18 +667,21 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
         q.dst = dst[i]->words + (size_t)dst[i]->HR * dst[i]->wpitch + dst[i]->HW;
         q.wpitch = (long long)a.wpitch;
         q.n = a.n;
-        q.nw = a.nw;
+        q.nw = nw;
         q.R = R;
-        q.PADC = PADC;
-        q.glo = glo;
-        q.K1 = K1;
-        q.Tr = Tr;
-        q.Tc = Tc;
-        q.nchunks = nchunks;
-        q.tiles_x = (a.n + Tc - 1) / Tc;
-        q.tiles_y = (a.n + Tr - 1) / Tr;
-        q.fast = (a.n % 32 == 0 && a.n >= 256) ? 1 : 0;
-        q.lanes16 = lanes16;
+        q.PADC = G.PADC;
+        q.glo = G.glo;
+        q.K1 = G.K1;
+        q.Tr = G.Tr;
+        q.Tc = G.Tc;
+        q.nchunks = G.nchunks;
+        q.half0 = G.half0;
+        q.atoms = G.atoms;
+        q.nb = G.nb;
+        q.stages = G.stages;
+        q.nhs = G.nhs;
+        q.tiles_x = (a.n + G.Tc - 1) / G.Tc;
+        q.tiles_y = (a.n + G.Tr - 1) / G.Tr;
         q.nlo0 = (uint32_t)nlo_d * bcast;
         q.dlo = (uint32_t)(nlo_s - nlo_d);
         q.hiH0 = (uint32_t)hiH_d * bcast;
@@ -564,11 +699,15 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
         q.wait_ns = kWaitLimitNs;
         q.inject_missing_commit = 0;
     }
-    P->smem_bytes = smem_layout(Tc, K1).total + 1024;
+    // one correction wraps a row (rows span [-R, n + 128 nb)) and a word index
+    // (words span [-(PADC + 16) / 32, nw + ng)); groups are word halves
+    const bool fast = a.n % 32 == 0 && nw > ng + 6 && a.n >= 128 * G.nb + R;
+    P->kernel = pick_kernel(G.lanes16 != 0, G.nb == 1, fast);
+    P->smem_bytes = smem_layout(G.stages, G.atoms, G.nhs, G.K1, G.nb).total + 1024;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     P->grid = std::min(P->prm[0].tiles_x * P->prm[0].tiles_y, sms);
-    if (cudaFuncSetAttribute(k_tensor_step, cudaFuncAttributeMaxDynamicSharedMemorySize, P->smem_bytes) !=
+    if (cudaFuncSetAttribute(P->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, P->smem_bytes) !=
         cudaSuccess) {
         snprintf(why, why_len, "cannot reserve %d bytes of shared memory", P->smem_bytes);
         cudaFree(P->err);
@@ -597,7 +736,7 @@ unsigned int* tensor_plan_error_flag(TensorPlan* p) { return p ? p->err : nullpt
 
 cudaError_t launch_tensor_pass(TensorPlan* p, bool src_is_a, cudaStream_t s) {
     const int i = src_is_a ? 0 : 1;
-    k_tensor_step<<<p->grid, kThreads, p->smem_bytes, s>>>(p->prm[i]);
+    p->kernel<<<p->grid, kThreads, p->smem_bytes, s>>>(p->prm[i]);
     return cudaGetLastError();
 }
 

@@ -1,5 +1,5 @@
 // tc_ptx.cuh -- sm_100a inline-PTX helpers of the tcgen05 step kernels:
-// mbarriers with bounded, hardware-suspended waits, TMEM allocation and loads,
+// mbarriers with bounded waits, TMEM allocation and loads,
 // tcgen05.mma issue and commit, shared-memory matrix descriptors.
 #pragma once
 
@@ -24,29 +24,29 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// One try at `phase` of `bar`.  The thread may be suspended in hardware for up
-// to `hint_ns` (or until the phase completes) before the try returns, so a
-// waiting warp issues a handful of instructions per wait instead of spinning.
-__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase, uint32_t hint_ns) {
+// One try at `phase` of `bar` (mbarrier.try_wait: the hardware may hold the
+// warp for a short, system-defined time before reporting "not yet").
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(phase), "r"(hint_ns)
+        : "r"(smem_u32(bar)), "r"(phase)
         : "memory");
     return done != 0;
 }
 
 // Bounded wait for `phase` of `bar`: false once `limit_ns` of wall time has
-// passed without the phase completing.  Each try suspends for up to `hint_ns`.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint64_t limit_ns,
-                                          uint32_t hint_ns = 20000u) {
-    if (mbar_try(bar, phase, hint_ns)) return true;
+// passed without the phase completing.  The clock is read once per 16 tries.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint64_t limit_ns) {
+    if (mbar_try(bar, phase)) return true;
     const uint64_t t0 = globaltimer();
     while (true) {
-        if (mbar_try(bar, phase, hint_ns)) return true;
+#pragma unroll 1
+        for (int i = 0; i < 16; ++i)
+            if (mbar_try(bar, phase)) return true;
         if (globaltimer() - t0 > limit_ns) return false;
     }
 }

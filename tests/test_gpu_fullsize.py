@@ -27,53 +27,64 @@ def sha(g):
 
 
 def run_variant(C, variant, start, radius, rule, steps):
+    """Generation 1, generation steps-1 and generation steps of one variant."""
     s = C.CUDASolver(N, radius, rule, variant=variant)
     try:
         s.setState(start)
-        s.doSteps(steps - 1)
+        s.doSteps(1)
+        first = s.getCurrentState()
+        s.doSteps(steps - 2)
         before = s.getCurrentState()
         s.doSteps(1)
         after = s.getCurrentState()
-        return before, after
+        return first, before, after
     finally:
         s.close()
 
 
 @pytest.mark.parametrize("radius", [1, 2, 4, 8, 16, 32])
 def test_radius_sweep_32768_200_steps(radius):
-    """Seed 2, d = 0.5, scaled interval rule, 200 steps (the radius-sweep workload)."""
+    """Seed 2, d = 0.5, scaled interval rule, 200 steps (the radius-sweep workload).
+    Every variant's generation 1 and its step 199 -> 200 are checked against the
+    oracle on their own, and all variants must end on the same grid."""
     import cat_cpu_b200 as C
     rule = O.scaled_rule(radius)
     start = C.start_grid(N, 2, 0.5, 1)
-    variants = [C.VARIANT_PACKED, C.VARIANT_TENSOR, C.VARIANT_PLAIN]
+    want1 = O.step(start, radius, rule)
     finals = {}
-    for v in variants:
-        before, after = run_variant(C, v, start, radius, rule, 200)
-        if v == variants[0]:
-            assert np.array_equal(O.step(before, radius, rule), after), f"R={radius}: step 200 differs from oracle"
-        finals[v] = sha(after)
+    for v in (C.VARIANT_PACKED, C.VARIANT_TENSOR, C.VARIANT_PLAIN):
+        first, before, after = run_variant(C, v, start, radius, rule, 200)
+        name = C.VARIANT_NAMES[v]
+        assert np.array_equal(first, want1), f"R={radius} {name}: generation 1 differs from the oracle"
+        assert np.array_equal(O.step(before, radius, rule), after), f"R={radius} {name}: step 200 differs"
+        finals[name] = sha(after)
     assert len(set(finals.values())) == 1, f"R={radius}: variants disagree {finals}"
 
 
 @pytest.mark.parametrize("radius", [64, 128])
 def test_large_radius_32768(radius):
     """Seed 3, d = 0.3 (dies at step 1 under the scaled rule) and d = 0.448 (stays
-    mixed for two steps): every step checked against the oracle."""
+    mixed for two steps): every step of every variant that takes the radius
+    checked against the oracle."""
     import cat_cpu_b200 as C
     rule = O.scaled_rule(radius)
+    variants = [C.VARIANT_PLAIN] + ([C.VARIANT_TENSOR] if radius <= 90 else [])
     for seed, d, steps in ((3, 0.3, 2), (3, 0.448, 2)):
         start = C.start_grid(N, seed, d, 1)
-        s = C.CUDASolver(N, radius, rule, variant=C.VARIANT_PLAIN)
-        try:
-            s.setState(start)
-            g = start
-            for k in range(steps):
-                s.doStep()
-                want = O.step(g, radius, rule)
-                got = s.getCurrentState()
-                assert np.array_equal(got, want), f"R={radius} d={d} step {k + 1}"
-                g = want
-            if d == 0.448:
-                assert 0 < int(g.sum()) < N * N or k == 0
-        finally:
-            s.close()
+        wants = []
+        g = start
+        for k in range(steps):
+            g = O.step(g, radius, rule)
+            wants.append(g)
+        if d == 0.448:
+            assert 0 < int(wants[-1].sum()) < N * N
+        for v in variants:
+            s = C.CUDASolver(N, radius, rule, variant=v)
+            try:
+                s.setState(start)
+                for k in range(steps):
+                    s.doStep()
+                    got = s.getCurrentState()
+                    assert np.array_equal(got, wants[k]), f"R={radius} d={d} {C.VARIANT_NAMES[v]} step {k + 1}"
+            finally:
+                s.close()

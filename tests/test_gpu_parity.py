@@ -31,7 +31,7 @@ def supported(variant, n, r):
     if variant == "packed":
         return r <= 32 and n >= r
     if variant == "tensor":
-        return r <= 32 and n >= r
+        return r <= 90 and n >= r
     return n >= r
 
 

@@ -40,19 +40,30 @@ def lane_consts(lo, hi, bits):
 
 
 def plan(n, R, rule):
+    """tensor_geometry + the rule constants of tensor_plan_create."""
     smin, smax, bmin, bmax = rule
-    PADC = 16 if R <= 16 else 48
-    Tc = 256 - 2 * PADC
-    Tr = 128 - 2 * R
+    PADC = 16 if R <= 16 else 16 + 32 * ((R - 16 + 31) // 32)
+    nb = 1 if R <= 32 else (128 + 2 * R + 127) // 128
+    Tr = 128 - 2 * R if nb == 1 else min(128, 128 * nb - 2 * R)
+    best, atoms, Tc = None, None, None
+    for a in (2, 3, 4):
+        tc = min(224, ((128 * a - 2 * PADC) // 32) * 32)
+        if tc < 32:
+            continue
+        cost = 128 * a / tc
+        if best is None or cost < best - 1e-9:
+            best, atoms, Tc = cost, a, tc
     glo = (PADC - R) // 32
     ghi = (PADC + 31 + R) // 32
     K1 = 32 * (ghi - glo + 1)
+    nchunks = Tc // 32
+    assert (nchunks - 1) + ghi <= 4 * atoms - 1
     lanes16 = (2 * R + 1) ** 2 > 127
     bits = 16 if lanes16 else 8
     bc = 0x00010001 if lanes16 else 0x01010101
     nlo_d, hih_d = lane_consts(bmin, bmax, bits)
     nlo_s, hih_s = lane_consts(smin + 1, smax + 1, bits)
-    return dict(PADC=PADC, Tc=Tc, Tr=Tr, glo=glo, K1=K1, nchunks=Tc // 32, lanes16=lanes16,
+    return dict(PADC=PADC, Tc=Tc, Tr=Tr, nb=nb, atoms=atoms, glo=glo, K1=K1, nchunks=nchunks, lanes16=lanes16,
                 nlo0=(nlo_d * bc) & 0xFFFFFFFF, dlo=(nlo_s - nlo_d) & 0xFFFFFFFF,
                 hiH0=(hih_d * bc) & 0xFFFFFFFF, dhi=(hih_s - hih_d) & 0xFFFFFFFF)
 
@@ -90,13 +101,17 @@ def tensor_step(grid, R, rule):
     """One generation exactly as k_tensor_step computes it (numpy, int arithmetic)."""
     n = grid.shape[0]
     P = plan(n, R, rule)
-    PADC, Tc, Tr = P["PADC"], P["Tc"], P["Tr"]
+    PADC, Tc, Tr, nb = P["PADC"], P["Tc"], P["Tr"], P["nb"]
+    XW = 128 * P["atoms"]
     assert Tr >= 1
     Bh = bh_matrix(P, R)
     m_ = np.arange(128)[:, None]
-    k_ = np.arange(128)[None, :]
+    k_ = np.arange(128 * nb)[None, :]
     Bv = ((k_ >= m_) & (k_ <= m_ + 2 * R)).astype(np.int64)
     nw = (n + 31) // 32
+    words = np.zeros((n, nw * 32), dtype=np.uint64)
+    words[:, :n] = grid
+    cur_words = (words.reshape(n, nw, 32) << np.arange(32, dtype=np.uint64)).sum(axis=2)  # packed input rows
     out_words = np.zeros((n, nw), dtype=np.uint64)
     tiles_x, tiles_y = -(-n // Tc), -(-n // Tr)
     q = np.arange(32)
@@ -104,23 +119,32 @@ def tensor_step(grid, R, rule):
     for ty in range(tiles_y):
         for tx in range(tiles_x):
             rbase, cbase = ty * Tr - R, tx * Tc - PADC
-            rows = (rbase + np.arange(128)) % n
             # X tile in shared-memory byte order: position 32g + q holds cell pi(q) of group g
-            cols = np.concatenate([(cbase + 32 * g + pi(q)) % n for g in range(8)])
-            X = grid[np.ix_(rows, cols)].astype(np.int64)
-            H = np.zeros((128, Tc), dtype=np.int64)
-            for i in range(P["nchunks"]):
-                w0 = 32 * (i + P["glo"])
-                H[:, 32 * i: 32 * i + 32] = X[:, w0: w0 + P["K1"]] @ Bh
+            cols = np.concatenate([(cbase + 32 * g + pi(q)) % n for g in range(XW // 32)])
+            H = np.zeros((128 * nb, Tc), dtype=np.int64)
+            Xb = []
+            for b in range(nb):  # row blocks: product 1 per block
+                rows = (rbase + 128 * b + np.arange(128)) % n
+                X = grid[np.ix_(rows, cols)].astype(np.int64)
+                Xb.append(X)
+                for i in range(P["nchunks"]):
+                    w0 = 32 * (i + P["glo"])
+                    H[128 * b: 128 * b + 128, 32 * i: 32 * i + 32] = X[:, w0: w0 + P["K1"]] @ Bh
             assert H.max() <= 2 * R + 1
-            C = Bv @ H  # box counts, centre included
+            C = Bv @ H  # box counts, centre included (product 2 over all blocks)
             aoff = (PADC - 16) >> 5
             xr = np.minimum(np.arange(128) + R, 127)
-            Xc = X[xr].astype(np.uint64)  # centre rows
+            Xc = Xb[0][xr].astype(np.uint64)  # centre rows (single-block tiles)
             for i in range(P["nchunks"]):
-                ga, gb = i + aoff, i + aoff + 1
-                Ga = [_word(Xc, 32 * ga + 4 * k) for k in range(8)]
-                Gb = [_word(Xc, 32 * gb + 4 * k) for k in range(8)]
+                wi = tx * (Tc // 32) + i
+                if nb == 1:
+                    ga, gb = i + aoff, i + aoff + 1
+                    Ga = [_word(Xc, 32 * ga + 4 * k) for k in range(8)]
+                    Gb = [_word(Xc, 32 * gb + 4 * k) for k in range(8)]
+                else:
+                    gi = ty * Tr + np.arange(128)
+                    ok = (gi < n) & (wi < nw)
+                    cw = np.where(ok, cur_words[np.minimum(gi, n - 1), min(wi, nw - 1)], np.uint64(0))
                 Cc = C[:, 32 * i: 32 * i + 32].astype(np.uint64)
                 # tcgen05.ld .pack::16b: register r = column 2r (low 16) | column 2r+1 (high 16)
                 v = [(Cc[:, 2 * r] & np.uint64(0xFFFF)) | ((Cc[:, 2 * r + 1] & np.uint64(0xFFFF)) << np.uint64(16))
@@ -129,7 +153,7 @@ def tensor_step(grid, R, rule):
                 if not P["lanes16"]:
                     for k in range(8):
                         B4 = prmt(v[2 * k], v[2 * k + 1], 0x6420)
-                        s4 = prmt(Ga[k], Gb[k], 0x5432)
+                        s4 = prmt(Ga[k], Gb[k], 0x5432) if nb == 1 else (cw >> np.uint64(k)) & np.uint64(0x01010101)
                         ge = (B4 + nlo0 + s4 * dlo) & M32
                         le = (hiH0 + s4 * dhi - B4) & M32
                         acc |= (ge & le & np.uint64(0x80808080)) >> np.uint64(7 - k)
@@ -137,11 +161,11 @@ def tensor_step(grid, R, rule):
                     for r in range(16):
                         h = r >> 3
                         sel = (2 + h) | 0x80 | ((4 + h) << 8) | 0x8000
-                        s2 = prmt(Ga[r & 7], Gb[r & 7], sel)
+                        s2 = prmt(Ga[r & 7], Gb[r & 7], sel) if nb == 1 else \
+                            (cw >> np.uint64(r)) & np.uint64(0x00010001)
                         ge = (v[r] + nlo0 + s2 * dlo) & M32
                         le = (hiH0 + s2 * dhi - v[r]) & M32
                         acc |= (ge & le & np.uint64(0x80008000)) >> np.uint64(15 - r)
-                wi = tx * (Tc // 32) + i
                 for mm in range(Tr):
                     gi = ty * Tr + mm
                     if gi < n and wi < nw:
@@ -163,6 +187,10 @@ CASES = [
     (100, 32, O.scaled_rule(32), 0.44, 9, 1),
     (33, 5, O.BOSCO_R5, 0.5, 10, 2),
     (20, 4, O.sweep_rule(4), 0.5, 11, 2),
+    (300, 40, O.scaled_rule(40), 0.45, 12, 1),   # two row blocks
+    (300, 64, O.scaled_rule(64), 0.45, 13, 1),   # two row blocks, 3-atom tile
+    (250, 90, O.scaled_rule(90), 0.45, 14, 1),   # three row blocks, 4-atom tile
+    (96, 33, O.scaled_rule(33), 0.45, 15, 1),
 ]
 
 
@@ -179,7 +207,7 @@ def test_tile_arithmetic_matches_oracle(n, R, rule, density, seed, steps):
 def test_rule_lanes_every_count():
     """Every box count and centre against the scalar rule, for rules with empty and
     out-of-range intervals, in both lane widths (through the same constants)."""
-    for R in (1, 2, 5, 6, 12, 32):
+    for R in (1, 2, 5, 6, 12, 32, 64, 90):
         N = (2 * R + 1) ** 2
         for rule in [O.scaled_rule(R), (0, N, 0, N), (N, 0, 5, 3), (-3, 2, N + 5, N + 9), (4, 4, 4, 4)]:
             P = plan(64, R, rule)
