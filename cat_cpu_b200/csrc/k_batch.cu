@@ -92,15 +92,37 @@ __device__ __forceinline__ uint32_t halo_word(const uint32_t* row, int fw, int n
     return packed_halo_word(row, fw, n, nw, [&] { return halo_word_bits(row, fw, n, nw); });
 }
 
+// One thread per inner row writes the row's three column-halo words: frame word
+// 0 (cells n-32 .. n-1), the last inner word's bits past n, and frame word nw + 1
+// (the cells that follow).  For n >= 64 it reads the four inner words they come
+// from once (first two, last two); smaller grids take the bit-by-bit path.
 __global__ void k_batch_halo_cols(uint32_t* __restrict__ arena, const BatchGrid* __restrict__ grids,
                                   const int* __restrict__ list) {
     const BatchGrid g = grids[list[blockIdx.y]];
     uint32_t* f = arena + g.off;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < g.n * 3; t += gridDim.x * blockDim.x) {
-        const int i = t / 3, k = t % 3;
-        const int fw = k == 0 ? 0 : g.nw + (k - 1);
+    const int n = g.n, nw = g.nw;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t* row = f + (size_t)(g.HR + i) * g.wp;
-        row[fw] = halo_word(row, fw, g.n, g.nw);
+        if (n >= 64) {
+            const uint32_t w1 = row[1], w2 = row[2];  // inner words 0 and 1
+            const uint32_t wl = row[nw], wp = row[nw - 1];  // inner words nw - 1 and nw - 2
+            const int ib = n - 32 * (nw - 1);  // inner bits of the last word, 1..32
+            // the last inner word with its bits past n filled from the row's start
+            const uint32_t last = ib >= 32 ? wl : ((wl & ((1u << ib) - 1u)) | (w1 << ib));
+            // frame word 0: cells n-32 .. n-1 = the 32 bits that end at inner bit ib of the last word
+            const uint32_t left = ib >= 32 ? wl : __funnelshift_r(wp, wl, ib);
+            // frame word nw + 1: cells 32 nw - n .. (the row's start shifted by the bits past n)
+            const int c = 32 * nw - n;
+            const uint32_t right = c ? __funnelshift_r(w1, w2, c) : w1;
+            row[0] = left;
+            row[nw] = last;
+            row[nw + 1] = right;
+        } else {
+            for (int k = 0; k < 3; ++k) {
+                const int fw = k == 0 ? 0 : nw + (k - 1);
+                row[fw] = halo_word(row, fw, n, nw);
+            }
+        }
     }
 }
 

@@ -158,6 +158,50 @@ __device__ __forceinline__ uint32_t fetch32(const uint32_t* __restrict__ row, in
     return v;
 }
 
+// Position in this CTA's stream of work, advanced incrementally (no integer
+// division in the loops).  Tiles t = blockIdx.x + j * gridDim.x, X blocks xi =
+// j * nb + b, units u = 2 xi + h (h = column half).
+struct Cursor {
+    int u, h;        // unit and its column half
+    int xi, b, j;    // X block, row block within the tile, tile count
+    int st, sph;     // X ring stage of block xi and its phase parity ((xi / stages) & 1)
+    int ty, tx;      // tile coordinates
+    int step_x, step_y, tiles_x, nb, stages;
+
+    __device__ void init(const TcParams& p) {
+        u = h = xi = b = j = st = sph = 0;
+        tiles_x = p.tiles_x;
+        nb = p.nb;
+        stages = p.stages;
+        ty = (int)blockIdx.x / tiles_x;
+        tx = (int)blockIdx.x - ty * tiles_x;
+        step_y = (int)gridDim.x / tiles_x;
+        step_x = (int)gridDim.x - step_y * tiles_x;
+    }
+    __device__ void next_block() {
+        ++xi;
+        if (++st == stages) {
+            st = 0;
+            sph ^= 1;
+        }
+        if (++b == nb) {
+            b = 0;
+            ++j;
+            tx += step_x;
+            ty += step_y;
+            if (tx >= tiles_x) {
+                tx -= tiles_x;
+                ++ty;
+            }
+        }
+    }
+    __device__ void next_unit() {
+        ++u;
+        h ^= 1;
+        if (h == 0) next_block();
+    }
+};
+
 // The work is a stream of units u = ((tile j * nb + row block b) * 2 + column
 // half h).  Per X block (j, b) the unpack warps fill one stage; per unit the MMA
 // warp runs product 1 for the half's chunks into TMEM half h of H, the epilogue
@@ -168,25 +212,26 @@ __device__ __forceinline__ uint32_t fetch32(const uint32_t* __restrict__ row, in
 //
 // LANES16: rule lanes (four 8-bit, or two 16-bit); CENTRE_SMEM: centre cells
 // from the X tile (single-block tiles) or from the packed input word; FAST:
-// n % 32 == 0 and large enough that rows and words wrap with one correction.
-template <bool LANES16, bool CENTRE_SMEM, bool FAST>
+// n % 32 == 0 and large enough that rows and words wrap with one correction;
+// ATOMS: X tile width in 128-column swizzle atoms.
+template <bool LANES16, bool CENTRE_SMEM, bool FAST, int ATOMS>
 __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_constant__ TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const SmemLayout L = smem_layout(p.stages, p.atoms, p.nhs, p.K1, p.nb);
+    const SmemLayout L = smem_layout(p.stages, ATOMS, p.nhs, p.K1, p.nb);
     uint8_t* xs = smem + L.x_off;
     uint8_t* hs = smem + L.hs_off;
     uint8_t* bh = smem + L.bh_off;
     uint8_t* bv = smem + L.bv_off;
     uint64_t* bars = (uint64_t*)(smem + L.bar_off);
     uint32_t* tmem_slot = (uint32_t*)(smem + L.tmem_off);
+    constexpr int kXB = ATOMS * kAtomBytes;  // bytes of one X stage
+    constexpr int kNG = 4 * ATOMS;           // 32-column groups per X row
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int R = p.R, Tc = p.Tc, K1 = p.K1, nb = p.nb, S = p.stages, nhs = p.nhs;
-    const int xbytes = p.atoms * kAtomBytes;
     const int ntiles = p.tiles_x * p.tiles_y;
-    int mine = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) ++mine;
+    const int mine = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const int units = mine * nb * 2;
     constexpr uint32_t kTmemCols = 512;
 
@@ -245,53 +290,56 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             const uint32_t id1 = idesc_u8(kN1, false);
             const uint32_t id2a = idesc_u8(32 * half0, true), id2b = idesc_u8(32 * (nch - half0), true);
             const int ksteps = K1 / 32;
-            auto product1 = [&](int u) -> bool {
-                const int h = u & 1, xi = u >> 1;  // X block index (j * nb + b)
-                const int st = xi % S;
-                if (!mbar_wait(&bars[X_FULL + st], (uint32_t)(xi / S) & 1u, p.wait_ns)) return false;
+            Cursor c1, c2;  // product 1 runs two units ahead of product 2
+            c1.init(p);
+            c2.init(p);
+            auto product1 = [&](const Cursor& c) -> bool {
+                if (!mbar_wait(&bars[X_FULL + c.st], (uint32_t)c.sph, p.wait_ns)) return false;
                 fence_after();
-                const uint32_t xa = smem_u32(xs + st * xbytes);
-                const int c0 = h ? half0 : 0, c1 = h ? nch : half0;
-                for (int i = c0; i < c1; ++i) {
+                const uint32_t xa = smem_u32(xs + c.st * kXB);
+                const int i0 = c.h ? half0 : 0, i1 = c.h ? nch : half0;
+                for (int i = i0; i < i1; ++i) {
                     for (int s = 0; s < ksteps; ++s) {
                         const int col = 32 * (i + p.glo + s);  // X column of this K step
                         const uint64_t ad = desc_k_sw128(xa + (col >> 7) * kAtomBytes + (col & 127));
                         const uint64_t bd = desc_noswz(ba + s * 2 * kN1 * 16, kN1 * 16, 128);
-                        mma_i8(tmem + kHCol + kHalfCols * h + kN1 * (i - c0), ad, bd, id1, s > 0 ? 1u : 0u);
+                        mma_i8(tmem + kHCol + kHalfCols * c.h + kN1 * (i - i0), ad, bd, id1, s > 0 ? 1u : 0u);
                     }
                 }
-                if (!(p.inject_missing_commit && u == 0)) mma_commit(&bars[H_FULL + h]);
+                if (!(p.inject_missing_commit && c.u == 0)) mma_commit(&bars[H_FULL + c.h]);
                 // the centre cells come from global memory: the stage is free once both halves read it
-                if (!CENTRE_SMEM && h == 1) mma_commit(&bars[X_EMPTY + st]);
+                if (!CENTRE_SMEM && c.h == 1) mma_commit(&bars[X_EMPTY + c.st]);
                 return true;
             };
-            // product 2 of unit u: C[h] (+)= B_v[:, 128b ..] * H(u), H(u) in buffer u % nhs
-            auto product2 = [&](int u) -> bool {
-                const int h = u & 1, xi = u >> 1, b = xi % nb, j = xi / nb;
-                if (b == 0 && j >= 1 && !mbar_wait(&bars[C_EMPTY + h], (uint32_t)(j - 1) & 1u, p.wait_ns))
+            // product 2 of unit c: C[h] (+)= B_v[:, 128b ..] * H(u), H(u) in buffer u % nhs
+            auto product2 = [&](const Cursor& c) -> bool {
+                if (c.b == 0 && c.j >= 1 && !mbar_wait(&bars[C_EMPTY + c.h], (uint32_t)(c.j - 1) & 1u, p.wait_ns))
                     return false;
                 fence_after();
-                const uint32_t ha = ha0 + (u % nhs) * 128 * kHalfCols;
+                const int hb = nhs == 2 ? c.h : 0;
+                const uint32_t ha = ha0 + hb * 128 * kHalfCols;
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
-                    const uint64_t ad = desc_noswz(va + (4 * b + s) * 2 * 128 * 16, 128 * 16, 128);
+                    const uint64_t ad = desc_noswz(va + (4 * c.b + s) * 2 * 128 * 16, 128 * 16, 128);
                     const uint64_t bd = desc_noswz(ha + s * 32 * 16, 128, 128 * 16);
-                    mma_i8(tmem + kCCol + kHalfCols * h, ad, bd, h ? id2b : id2a, (b > 0 || s > 0) ? 1u : 0u);
+                    mma_i8(tmem + kCCol + kHalfCols * c.h, ad, bd, c.h ? id2b : id2a, (c.b > 0 || s > 0) ? 1u : 0u);
                 }
-                mma_commit(&bars[HS_EMPTY + (u % nhs)]);
-                if (b == nb - 1) mma_commit(&bars[C_FULL + h]);
+                mma_commit(&bars[HS_EMPTY + hb]);
+                if (c.b == nb - 1) mma_commit(&bars[C_FULL + c.h]);
                 return true;
             };
             // Per unit u, once H(u) has been read back: product 2 of unit u (the
             // epilogue waits for it next), then product 1 of unit u+2 into the
             // TMEM half that H(u) has just left.
             bool ok = true;
-            if (units >= 1) ok = product1(0);
-            if (ok && units >= 2) ok = product1(1);
-            for (int u = 0; u < units && ok; ++u) {
-                ok = mbar_wait(&bars[HS_FULL + (u & 1)], (uint32_t)(u >> 1) & 1u, p.wait_ns);
-                if (ok) ok = product2(u);
-                if (ok && u + 2 < units) ok = product1(u + 2);
+            if (units >= 1) ok = product1(c1);
+            c1.next_unit();
+            if (ok && units >= 2) ok = product1(c1);
+            c1.next_unit();
+            for (; c2.u < units && ok; c2.next_unit(), c1.next_unit()) {
+                ok = mbar_wait(&bars[HS_FULL + c2.h], (uint32_t)(c2.xi & 1), p.wait_ns);
+                if (ok) ok = product2(c2);
+                if (ok && c1.u < units) ok = product1(c1);
             }
             if (!ok) atomicOr(p.err, 2u);
             // never leave with an MMA in flight (TMEM is freed below)
@@ -300,72 +348,71 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         }
     } else if (warp < kEpiWarp0) {
         // ------------------------------ unpack ------------------------------
-        // Thread `row` (0..127) fills X row `row` of every stage: the 4*atoms
-        // groups of 32 columns of one packed row.  The words of the next X block
-        // are loaded right after this one is stored, so their latency is spent
+        // Thread `row` (0..127) fills X row `row` of every stage: the kNG groups
+        // of 32 columns of one packed row.  The words of the next X block are
+        // loaded right after this one is stored, so their latency is spent
         // waiting for a free stage rather than on the critical path.
         const int row = tid - 32;
-        const int ng = 4 * p.atoms;
         const int sw = row & 7;
         const int blocks = mine * nb;
-        uint32_t w[kMaxGroups + 1];
-        // FAST: the ng + 1 words that hold X row `row` of block xi (group g = upper
-        // half of word g, lower half of word g + 1); otherwise the ng groups
-        auto gather = [&](int xi) {
-            const int t = blockIdx.x + (xi / nb) * gridDim.x;
-            const int ty = t / p.tiles_x, tx = t % p.tiles_x;
-            const int gr0 = ty * p.Tr - R + 128 * (xi % nb) + row;
-            const int cbase = tx * Tc - p.PADC;  // column of X-tile column 0 (16 mod 32)
+        uint32_t w[kNG + 1];
+        // FAST: the kNG + 1 words that hold X row `row` of the cursor's block (group
+        // g = upper half of word g, lower half of word g + 1); otherwise the groups
+        auto gather = [&](const Cursor& c) {
+            const int gr0 = c.ty * p.Tr - R + 128 * c.b + row;
+            const int cbase = c.tx * Tc - p.PADC;  // column of X-tile column 0 (16 mod 32)
             if (FAST) {
                 int gr = gr0;
                 if (gr < 0) gr += p.n;
                 else if (gr >= p.n) gr -= p.n;
                 const uint32_t* rp = p.src + (size_t)gr * (size_t)p.wpitch;
-                const int wl0 = (cbase - 16) >> 5;  // word holding X column 0
+                int wi = (cbase - 16) >> 5;  // word holding X column 0
+                if (wi < 0) wi += p.nw;
 #pragma unroll
-                for (int k = 0; k <= kMaxGroups; ++k) {
-                    if (k <= ng) {
-                        int wi = wl0 + k;
-                        if (wi < 0) wi += p.nw;
-                        else if (wi >= p.nw) wi -= p.nw;
-                        w[k] = __ldg(rp + wi);
-                    }
+                for (int k = 0; k <= kNG; ++k) {
+                    w[k] = __ldg(rp + wi);
+                    if (++wi == p.nw) wi = 0;
                 }
             } else {
                 const uint32_t* rp = p.src + (size_t)wrap_slow(gr0, p.n) * (size_t)p.wpitch;
+                int a = wrap_slow(cbase, p.n);
 #pragma unroll
-                for (int k = 0; k < kMaxGroups; ++k)
-                    if (k < ng) w[k] = fetch32(rp, wrap_slow(cbase + 32 * k, p.n), p.n);
+                for (int k = 0; k < kNG; ++k) {
+                    w[k] = fetch32(rp, a, p.n);
+                    a += 32;
+                    while (a >= p.n) a -= p.n;
+                }
             }
         };
         bool ok = true;
-        if (blocks > 0) gather(0);
-        for (int xi = 0; xi < blocks; ++xi) {
-            const int st = xi % S;
-            if (xi >= S) {
+        Cursor c, cn;  // the block being stored and the one being loaded
+        c.init(p);
+        cn.init(p);
+        if (blocks > 0) gather(cn);
+        cn.next_block();
+        for (; c.xi < blocks; c.next_block(), cn.next_block()) {
+            if (c.xi >= S) {
                 bool wt = true;
-                if (lane == 0) wt = mbar_wait(&bars[X_EMPTY + st], ((uint32_t)(xi / S) & 1u) ^ 1u, p.wait_ns);
+                if (lane == 0) wt = mbar_wait(&bars[X_EMPTY + c.st], (uint32_t)(c.sph ^ 1), p.wait_ns);
                 ok = __shfl_sync(0xffffffffu, wt, 0);
                 if (!ok) break;
             }
-            uint8_t* xrow = xs + st * xbytes + row * 128;
+            uint8_t* xrow = xs + c.st * kXB + row * 128;
 #pragma unroll
-            for (int g = 0; g < kMaxGroups; ++g) {
-                if (g < ng) {
-                    const uint32_t x = FAST ? prmt(w[g], w[g + 1], 0x5432u) : w[g];
-                    uint32_t v[8];
+            for (int g = 0; g < kNG; ++g) {
+                const uint32_t x = FAST ? prmt(w[g], w[g + 1], 0x5432u) : w[g];
+                uint32_t v[8];
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) v[k] = (x >> k) & 0x01010101u;
-                    uint8_t* ap = xrow + (g >> 2) * kAtomBytes;
-                    const int ch = 2 * (g & 3);
-                    *(uint4*)(ap + ((ch ^ sw) << 4)) = make_uint4(v[0], v[1], v[2], v[3]);
-                    *(uint4*)(ap + (((ch + 1) ^ sw) << 4)) = make_uint4(v[4], v[5], v[6], v[7]);
-                }
+                for (int k = 0; k < 8; ++k) v[k] = (x >> k) & 0x01010101u;
+                uint8_t* ap = xrow + (g >> 2) * kAtomBytes;
+                const int ch = 2 * (g & 3);
+                *(uint4*)(ap + ((ch ^ sw) << 4)) = make_uint4(v[0], v[1], v[2], v[3]);
+                *(uint4*)(ap + (((ch + 1) ^ sw) << 4)) = make_uint4(v[4], v[5], v[6], v[7]);
             }
             fence_proxy_async();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bars[X_FULL + st]);
-            if (xi + 1 < blocks) gather(xi + 1);
+            if (lane == 0) mbar_arrive(&bars[X_FULL + c.st]);
+            if (cn.xi < blocks) gather(cn);
         }
         if (!ok && lane == 0) atomicOr(p.err, 4u);
     } else {
@@ -378,24 +425,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         const uint32_t rq_mask = p.rq_mask[grp];
         const int aoff = (p.PADC - 16) >> 5;  // centre groups of chunk i: i + aoff, i + aoff + 1
         const uint32_t nlo0 = p.nlo0, dlo = p.dlo, hiH0 = p.hiH0, dhi = p.dhi;
+        const int xr = min(m + R, 127);  // X row of this output row's centre cells (rows >= Tr are not stored)
+        const int xsw = xr & 7;
         bool ok = true;
         auto wait_all = [&](uint64_t* bar, uint32_t ph) -> bool {
             const bool wt = mbar_wait(bar, ph, p.wait_ns);
             return __all_sync(0xffffffffu, wt);
         };
-        // re-quantise H(u) to u8 into shared-memory buffer u % nhs (MN-major B operand of product 2)
-        auto requant = [&](int u) -> bool {
-            const int h = u & 1;
-            if (!wait_all(&bars[H_FULL + h], (uint32_t)(u >> 1) & 1u)) return false;
-            const int k = u / nhs;
-            if (k >= 1 && !wait_all(&bars[HS_EMPTY + (u % nhs)], (uint32_t)(k - 1) & 1u)) return false;
+        // re-quantise H(u) to u8 into its shared-memory buffer (MN-major B operand of product 2)
+        auto requant = [&](const Cursor& c) -> bool {
+            if (!wait_all(&bars[H_FULL + c.h], (uint32_t)(c.xi & 1))) return false;
+            const int hb = nhs == 2 ? c.h : 0;
+            const int k = nhs == 2 ? c.xi : c.u;  // earlier uses of this buffer
+            if (k >= 1 && !wait_all(&bars[HS_EMPTY + hb], (uint32_t)((k - 1) & 1))) return false;
             fence_after();
-            uint8_t* hsb = hs + (u % nhs) * 128 * kHalfCols;
-            const int c0 = h ? half0 : 0, c1 = h ? nch : half0;
-            for (int i = c0; i < c1; ++i) {
+            uint8_t* hsb = hs + hb * 128 * kHalfCols;
+            const int i0 = c.h ? half0 : 0, i1 = c.h ? nch : half0;
+            for (int i = i0; i < i1; ++i) {
                 if (!((rq_mask >> i) & 1u)) continue;
                 uint32_t v[16];
-                tmem_ld32p(tmem + lane_off + kHCol + kHalfCols * h + kN1 * (i - c0), v);
+                tmem_ld32p(tmem + lane_off + kHCol + kHalfCols * c.h + kN1 * (i - i0), v);
                 tmem_wait16(v);
 #pragma unroll
                 for (int hh = 0; hh < 2; ++hh) {
@@ -404,34 +453,29 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                     wv.y = prmt(v[8 * hh + 2], v[8 * hh + 3], 0x6420u);
                     wv.z = prmt(v[8 * hh + 4], v[8 * hh + 5], 0x6420u);
                     wv.w = prmt(v[8 * hh + 6], v[8 * hh + 7], 0x6420u);
-                    *(uint4*)(hsb + ((2 * (i - c0) + hh) * 128 + m) * 16) = wv;
+                    *(uint4*)(hsb + ((2 * (i - i0) + hh) * 128 + m) * 16) = wv;
                 }
             }
             fence_proxy_async();
             fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bars[HS_FULL + h]);
+            if (lane == 0) mbar_arrive(&bars[HS_FULL + c.h]);
             return true;
         };
-        // rule + store of column half h of C(j)
-        auto rule = [&](int j, int h) -> bool {
-            if (!wait_all(&bars[C_FULL + h], (uint32_t)j & 1u)) return false;
+        // rule + store of column half c.h of C(c.j)
+        auto rule = [&](const Cursor& c) -> bool {
+            if (!wait_all(&bars[C_FULL + c.h], (uint32_t)(c.j & 1))) return false;
             fence_after();
-            const int t = blockIdx.x + j * gridDim.x;
-            const int st = j % S;  // (CENTRE_SMEM: one X block per tile)
-            const int ty = t / p.tiles_x, tx = t % p.tiles_x;
-            const int gi = ty * p.Tr + m;
+            const int gi = c.ty * p.Tr + m;
             const bool row_ok = (m < p.Tr) && (gi < p.n);
-            const int xr = min(m + R, 127);  // X row of this output row's centre cells (rows >= Tr are not stored)
-            const uint8_t* xrow = xs + st * xbytes + xr * 128;
-            const int sw = xr & 7;
+            const uint8_t* xrow = xs + c.st * kXB + xr * 128;  // (CENTRE_SMEM: one X block per tile)
             uint32_t* orow = p.dst + (size_t)(row_ok ? gi : 0) * (size_t)p.wpitch;
             const uint32_t* crow = p.src + (size_t)(row_ok ? gi : 0) * (size_t)p.wpitch;
-            const int w0 = tx * (Tc >> 5);
-            const int c0 = h ? half0 : 0, c1 = h ? nch : half0;
-            for (int i = c0 + grp; i < c1; i += kGroups) {
+            const int w0 = c.tx * (Tc >> 5);
+            const int i0 = c.h ? half0 : 0, i1 = c.h ? nch : half0;
+            for (int i = i0 + grp; i < i1; i += kGroups) {
                 uint32_t v[16];
-                tmem_ld32p(tmem + lane_off + kCCol + kHalfCols * h + kN1 * (i - c0), v);
+                tmem_ld32p(tmem + lane_off + kCCol + kHalfCols * c.h + kN1 * (i - i0), v);
                 const int wi = w0 + i;
                 const bool store = row_ok && wi < p.nw;
                 uint32_t Ga[8], Gb[8];
@@ -439,12 +483,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                 if (CENTRE_SMEM) {
                     // centre cells: groups ga and ga + 1 of the X row (8 words each)
                     const int ga = i + aoff, gb = ga + 1;
-                    const uint4 a0 = *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3)) ^ sw) << 4));
+                    const uint4 a0 = *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3)) ^ xsw) << 4));
                     const uint4 a1 =
-                        *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3) + 1) ^ sw) << 4));
-                    const uint4 b0 = *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3)) ^ sw) << 4));
+                        *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3) + 1) ^ xsw) << 4));
+                    const uint4 b0 = *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3)) ^ xsw) << 4));
                     const uint4 b1 =
-                        *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3) + 1) ^ sw) << 4));
+                        *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3) + 1) ^ xsw) << 4));
                     Ga[0] = a0.x; Ga[1] = a0.y; Ga[2] = a0.z; Ga[3] = a0.w;
                     Ga[4] = a1.x; Ga[5] = a1.y; Ga[6] = a1.z; Ga[7] = a1.w;
                     Gb[0] = b0.x; Gb[1] = b0.y; Gb[2] = b0.z; Gb[3] = b0.w;
@@ -485,19 +529,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             fence_before();
             __syncwarp();
             if (lane == 0) {
-                mbar_arrive(&bars[C_EMPTY + h]);
-                if (CENTRE_SMEM && h == 1) mbar_arrive(&bars[X_EMPTY + st]);
+                mbar_arrive(&bars[C_EMPTY + c.h]);
+                if (CENTRE_SMEM && c.h == 1) mbar_arrive(&bars[X_EMPTY + c.st]);
             }
             return true;
         };
-        if (units >= 1) ok = requant(0);
-        for (int u = 0; u < units && ok; ++u) {
-            if (u + 1 < units && !requant(u + 1)) {
-                ok = false;
-                break;
+        Cursor cq, cr;  // the unit to re-quantise next, the unit whose rule comes next
+        cq.init(p);
+        cr.init(p);
+        if (units >= 1) ok = requant(cq);
+        cq.next_unit();
+        for (; cr.u < units && ok; cr.next_unit()) {
+            if (cq.u < units) {
+                if (!requant(cq)) {
+                    ok = false;
+                    break;
+                }
+                cq.next_unit();
             }
-            const int xi = u >> 1;
-            if (xi % nb == nb - 1 && !rule(xi / nb, u & 1)) ok = false;
+            if (cr.b == nb - 1 && !rule(cr)) ok = false;
         }
         if (!ok && lane == 0) atomicOr(p.err, 8u);
     }
@@ -523,13 +573,25 @@ struct TensorPlan {
     unsigned int* err;
 };
 
-template <bool L16, bool CS>
+// The instantiations that exist: 8-bit lanes only with single-block tiles of 2
+// atoms (R <= 5); 16-bit lanes with single-block 2-atom tiles (R <= 32) or with
+// multi-block tiles of 2, 3 or 4 atoms.
+template <bool L16, bool CS, int A>
 static TcKernel pick_fast(bool fast) {
-    return fast ? k_tensor_step<L16, CS, true> : k_tensor_step<L16, CS, false>;
+    return fast ? k_tensor_step<L16, CS, true, A> : k_tensor_step<L16, CS, false, A>;
 }
-static TcKernel pick_kernel(bool lanes16, bool centre_smem, bool fast) {
-    if (lanes16) return centre_smem ? pick_fast<true, true>(fast) : pick_fast<true, false>(fast);
-    return centre_smem ? pick_fast<false, true>(fast) : pick_fast<false, false>(fast);
+static TcKernel pick_kernel(bool lanes16, bool centre_smem, bool fast, int atoms) {
+    if (centre_smem) {
+        if (atoms != 2) return nullptr;
+        return lanes16 ? pick_fast<true, true, 2>(fast) : pick_fast<false, true, 2>(fast);
+    }
+    if (!lanes16) return nullptr;
+    switch (atoms) {
+        case 2: return pick_fast<true, false, 2>(fast);
+        case 3: return pick_fast<true, false, 3>(fast);
+        case 4: return pick_fast<true, false, 4>(fast);
+    }
+    return nullptr;
 }
 
 // Largest radius of the tensor step: box counts (2R+1)^2 must fit the 16-bit
@@ -702,7 +764,13 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
     // one correction wraps a row (rows span [-R, n + 128 nb)) and a word index
     // (words span [-(PADC + 16) / 32, nw + ng)); groups are word halves
     const bool fast = a.n % 32 == 0 && nw > ng + 6 && a.n >= 128 * G.nb + R;
-    P->kernel = pick_kernel(G.lanes16 != 0, G.nb == 1, fast);
+    P->kernel = pick_kernel(G.lanes16 != 0, G.nb == 1, fast, G.atoms);
+    if (!P->kernel) {
+        snprintf(why, why_len, "no kernel instantiation for R=%d", R);
+        cudaFree(P->err);
+        delete P;
+        return nullptr;
+    }
     P->smem_bytes = smem_layout(G.stages, G.atoms, G.nhs, G.K1, G.nb).total + 1024;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);

@@ -38,7 +38,7 @@ extern "C" {
  * CASolverFactory.cpp:10-119; the reference's own codes 0-6 are CPU solvers). */
 #define LTL_VARIANT_AUTO (-1)  /* pick the fastest exact variant for (n, R) */
 #define LTL_VARIANT_PLAIN 0    /* CUDA-core SWAR stencil, uint8 cells */
-#define LTL_VARIANT_TENSOR 1   /* tcgen05 banded products B_v * X * B_h, uint8 cells */
+#define LTL_VARIANT_TENSOR 1   /* tcgen05 banded products B_v * X * B_h, bit-packed grid */
 #define LTL_VARIANT_PACKED 2   /* bit-packed cells (64 per uint64), CUDA-core bit logic */
 
 typedef struct ltl_ctx ltl_ctx;
@@ -60,7 +60,7 @@ typedef struct {
  * GPU codes; radius and rule are run-time values instead of the RADIUS/SMIN/
  * SMAX/BMIN/BMAX macros (Makefile:10-14).  n >= radius is required (the
  * reference's torus halo is only defined there, HostSolver.tpp:93-140).
- * Radius ranges: plain 1..2038, packed and tensor 1..32; outside them
+ * Radius ranges: plain 1..2038, packed 1..32, tensor 1..90; outside them
  * LTL_EUNSUPPORTED. */
 int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin, int smax, int bmin, int bmax,
                int variant);

@@ -1,8 +1,10 @@
 """Batched grids (ltl_batch_*): every grid bit-exact against the CPU oracle.
 
-Marked `gpu`.  The full 4096-grid workload is checked at sampled steps: the
-oracle advances the GPU's own state one generation and must land on the GPU's
-next state, for every grid.
+Marked `gpu`.  The full 4096-grid workload is checked two ways: for every grid
+the oracle advances the GPU's state at step 255 one generation and must land on
+the GPU's step 256; for a stratified sample (all grids of side <= 96, the 8
+largest, 64 random others) the oracle runs the whole 256-step trajectory from
+the start grid.
 """
 import concurrent.futures as cf
 import os
@@ -96,11 +98,18 @@ def test_full_batched_workload_sampled():
         ok = list(ex.map(check, range(len(cfg))))
     bad = [k for k, v in enumerate(ok) if not v]
     assert not bad, f"{len(bad)} grids differ at step 256, first {bad[:5]}"
-    # whole trajectories for the small grids
-    small = [k for k, c in enumerate(cfg) if c[0] <= 128][:64]
-    for k in small:
+    # whole 256-step trajectories for a stratified sample: every grid of side
+    # <= 96, the 8 largest grids (sides near 2048) and 64 others drawn at random
+    by_size = sorted(range(len(cfg)), key=lambda k: cfg[k][0])
+    small = [k for k in by_size if cfg[k][0] <= 96]
+    large = by_size[-8:]
+    rest = [k for k in by_size if k not in set(small) | set(large)]
+    mid = list(np.random.default_rng(2).choice(rest, size=min(64, len(rest)), replace=False))
+    sample = small + large + [int(k) for k in mid]
+    assert max(cfg[k][0] for k in sample) >= 1900
+    for k in sample:
         n, r, rule, d, s = cfg[k]
-        assert np.array_equal(O.run(grids[k], r, rule, 256), s256[k]), k
+        assert np.array_equal(O.run(grids[k], r, rule, 256), s256[k]), f"grid {k} n={n} r={r}: trajectory differs"
 
 
 def test_batch_errors():
