@@ -285,67 +285,83 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
 
     if (warp == 0) {
         // --------------------------- MMA issuer -----------------------------
-        if (lane == 0) {
-            const uint32_t ba = smem_u32(bh), va = smem_u32(bv), ha0 = smem_u32(hs);
-            const uint32_t id1 = idesc_u8(kN1, false);
-            const uint32_t id2a = idesc_u8(32 * half0, true), id2b = idesc_u8(32 * (nch - half0), true);
-            const int ksteps = K1 / 32;
-            Cursor c1, c2;  // product 1 runs two units ahead of product 2
-            c1.init(p);
-            c2.init(p);
-            auto product1 = [&](const Cursor& c) -> bool {
-                if (!mbar_wait(&bars[X_FULL + c.st], (uint32_t)c.sph, p.wait_ns)) return false;
-                fence_after();
-                const uint32_t xa = smem_u32(xs + c.st * kXB);
+        // The whole warp runs the loop (waits and descriptor arithmetic are
+        // warp-uniform); lane 0 alone issues the MMAs and the commits, so that
+        // every commit tracks every MMA before it.  Descriptors are 64-bit bases
+        // plus start-address offsets (in 16-byte units, within the 14-bit field).
+        const uint32_t id1 = idesc_u8(kN1, false);
+        const uint32_t id2a = idesc_u8(32 * half0, true), id2b = idesc_u8(32 * (nch - half0), true);
+        const int ksteps = K1 / 32;
+        const uint64_t xd0 = desc_k_sw128(smem_u32(xs));
+        const uint64_t bhd0 = desc_noswz(smem_u32(bh), kN1 * 16, 128);
+        const uint64_t bvd0 = desc_noswz(smem_u32(bv), 128 * 16, 128);
+        const uint64_t hsd0 = desc_noswz(smem_u32(hs), 128, 128 * 16);
+        const bool leader = lane == 0;
+        Cursor c1, c2;  // product 1 runs two units ahead of product 2
+        c1.init(p);
+        c2.init(p);
+        auto product1 = [&](const Cursor& c) -> bool {
+            if (!__all_sync(0xffffffffu, mbar_wait(&bars[X_FULL + c.st], (uint32_t)c.sph, p.wait_ns))) return false;
+            fence_after();
+            if (leader) {
                 const int i0 = c.h ? half0 : 0, i1 = c.h ? nch : half0;
-                for (int i = i0; i < i1; ++i) {
+                const uint64_t xs0 = xd0 + (uint64_t)((c.st * kXB) >> 4);
+                uint32_t d = tmem + kHCol + kHalfCols * c.h;
+                for (int i = i0; i < i1; ++i, d += kN1) {
                     for (int s = 0; s < ksteps; ++s) {
                         const int col = 32 * (i + p.glo + s);  // X column of this K step
-                        const uint64_t ad = desc_k_sw128(xa + (col >> 7) * kAtomBytes + (col & 127));
-                        const uint64_t bd = desc_noswz(ba + s * 2 * kN1 * 16, kN1 * 16, 128);
-                        mma_i8(tmem + kHCol + kHalfCols * c.h + kN1 * (i - i0), ad, bd, id1, s > 0 ? 1u : 0u);
+                        const uint64_t ad = xs0 + (uint64_t)((((col >> 7) * kAtomBytes) + (col & 127)) >> 4);
+                        const uint64_t bd = bhd0 + (uint64_t)((s * 2 * kN1 * 16) >> 4);
+                        mma_i8(d, ad, bd, id1, s > 0 ? 1u : 0u);
                     }
                 }
                 if (!(p.inject_missing_commit && c.u == 0)) mma_commit(&bars[H_FULL + c.h]);
                 // the centre cells come from global memory: the stage is free once both halves read it
                 if (!CENTRE_SMEM && c.h == 1) mma_commit(&bars[X_EMPTY + c.st]);
-                return true;
-            };
-            // product 2 of unit c: C[h] (+)= B_v[:, 128b ..] * H(u), H(u) in buffer u % nhs
-            auto product2 = [&](const Cursor& c) -> bool {
-                if (c.b == 0 && c.j >= 1 && !mbar_wait(&bars[C_EMPTY + c.h], (uint32_t)(c.j - 1) & 1u, p.wait_ns))
-                    return false;
-                fence_after();
+            }
+            __syncwarp();
+            return true;
+        };
+        // product 2 of unit c: C[h] (+)= B_v[:, 128b ..] * H(u), H(u) in buffer u % nhs
+        auto product2 = [&](const Cursor& c) -> bool {
+            if (c.b == 0 && c.j >= 1 &&
+                !__all_sync(0xffffffffu, mbar_wait(&bars[C_EMPTY + c.h], (uint32_t)(c.j - 1) & 1u, p.wait_ns)))
+                return false;
+            fence_after();
+            if (leader) {
                 const int hb = nhs == 2 ? c.h : 0;
-                const uint32_t ha = ha0 + hb * 128 * kHalfCols;
+                const uint64_t hd = hsd0 + (uint64_t)((hb * 128 * kHalfCols) >> 4);
+                const uint64_t vd = bvd0 + (uint64_t)((4 * c.b * 2 * 128 * 16) >> 4);
+                const uint32_t id2 = c.h ? id2b : id2a;
+                const uint32_t d = tmem + kCCol + kHalfCols * c.h;
 #pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    const uint64_t ad = desc_noswz(va + (4 * c.b + s) * 2 * 128 * 16, 128 * 16, 128);
-                    const uint64_t bd = desc_noswz(ha + s * 32 * 16, 128, 128 * 16);
-                    mma_i8(tmem + kCCol + kHalfCols * c.h, ad, bd, c.h ? id2b : id2a, (c.b > 0 || s > 0) ? 1u : 0u);
-                }
+                for (int s = 0; s < 4; ++s)
+                    mma_i8(d, vd + (uint64_t)((s * 2 * 128 * 16) >> 4), hd + (uint64_t)((s * 32 * 16) >> 4), id2,
+                           (c.b > 0 || s > 0) ? 1u : 0u);
                 mma_commit(&bars[HS_EMPTY + hb]);
                 if (c.b == nb - 1) mma_commit(&bars[C_FULL + c.h]);
-                return true;
-            };
-            // Per unit u, once H(u) has been read back: product 2 of unit u (the
-            // epilogue waits for it next), then product 1 of unit u+2 into the
-            // TMEM half that H(u) has just left.
-            bool ok = true;
-            if (units >= 1) ok = product1(c1);
-            c1.next_unit();
-            if (ok && units >= 2) ok = product1(c1);
-            c1.next_unit();
-            for (; c2.u < units && ok; c2.next_unit(), c1.next_unit()) {
-                ok = mbar_wait(&bars[HS_FULL + c2.h], (uint32_t)(c2.xi & 1), p.wait_ns);
-                if (ok) ok = product2(c2);
-                if (ok && c1.u < units) ok = product1(c1);
             }
-            if (!ok) atomicOr(p.err, 2u);
-            // never leave with an MMA in flight (TMEM is freed below)
-            mma_commit(&bars[DRAIN]);
-            if (!mbar_wait(&bars[DRAIN], 0u, p.wait_ns)) atomicOr(p.err, 32u);
+            __syncwarp();
+            return true;
+        };
+        // Per unit u, once H(u) has been read back: product 2 of unit u (the
+        // epilogue waits for it next), then product 1 of unit u+2 into the
+        // TMEM half that H(u) has just left.
+        bool ok = true;
+        if (units >= 1) ok = product1(c1);
+        c1.next_unit();
+        if (ok && units >= 2) ok = product1(c1);
+        c1.next_unit();
+        for (; c2.u < units && ok; c2.next_unit(), c1.next_unit()) {
+            ok = __all_sync(0xffffffffu, mbar_wait(&bars[HS_FULL + c2.h], (uint32_t)(c2.xi & 1), p.wait_ns));
+            if (ok) ok = product2(c2);
+            if (ok && c1.u < units) ok = product1(c1);
         }
+        if (!ok && leader) atomicOr(p.err, 2u);
+        // never leave with an MMA in flight (TMEM is freed below)
+        if (leader) mma_commit(&bars[DRAIN]);
+        __syncwarp();
+        if (!__all_sync(0xffffffffu, mbar_wait(&bars[DRAIN], 0u, p.wait_ns)) && leader) atomicOr(p.err, 32u);
     } else if (warp < kEpiWarp0) {
         // ------------------------------ unpack ------------------------------
         // Thread `row` (0..127) fills X row `row` of every stage: the kNG groups
@@ -432,57 +448,50 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             const bool wt = mbar_wait(bar, ph, p.wait_ns);
             return __all_sync(0xffffffffu, wt);
         };
-        // re-quantise H(u) to u8 into its shared-memory buffer (MN-major B operand of product 2)
-        auto requant = [&](const Cursor& c) -> bool {
-            if (!wait_all(&bars[H_FULL + c.h], (uint32_t)(c.xi & 1))) return false;
-            const int hb = nhs == 2 ? c.h : 0;
-            const int k = nhs == 2 ? c.xi : c.u;  // earlier uses of this buffer
-            if (k >= 1 && !wait_all(&bars[HS_EMPTY + hb], (uint32_t)((k - 1) & 1))) return false;
-            fence_after();
-            uint8_t* hsb = hs + hb * 128 * kHalfCols;
-            const int i0 = c.h ? half0 : 0, i1 = c.h ? nch : half0;
-            for (int i = i0; i < i1; ++i) {
-                if (!((rq_mask >> i) & 1u)) continue;
-                uint32_t v[16];
-                tmem_ld32p(tmem + lane_off + kHCol + kHalfCols * c.h + kN1 * (i - i0), v);
-                tmem_wait16(v);
-#pragma unroll
-                for (int hh = 0; hh < 2; ++hh) {
-                    uint4 wv;
-                    wv.x = prmt(v[8 * hh + 0], v[8 * hh + 1], 0x6420u);
-                    wv.y = prmt(v[8 * hh + 2], v[8 * hh + 3], 0x6420u);
-                    wv.z = prmt(v[8 * hh + 4], v[8 * hh + 5], 0x6420u);
-                    wv.w = prmt(v[8 * hh + 6], v[8 * hh + 7], 0x6420u);
-                    *(uint4*)(hsb + ((2 * (i - i0) + hh) * 128 + m) * 16) = wv;
-                }
+        // Per step of the loop: the re-quantisation of unit cq (H of its column half
+        // -> u8 in shared memory, the B operand of product 2) and the rule of unit
+        // cr = cq - 1 (if that unit ends a tile).  Both TMEM loads are issued before
+        // one wait, so their latencies overlap.  Each group has at most one chunk of
+        // each per unit (a half has <= 4 chunks; the host plan spreads them).
+        auto stage = [&](const Cursor* q, const Cursor* r) -> bool {
+            int hb = 0;
+            if (q) {
+                if (!wait_all(&bars[H_FULL + q->h], (uint32_t)(q->xi & 1))) return false;
+                hb = nhs == 2 ? q->h : 0;
+                const int k = nhs == 2 ? q->xi : q->u;  // earlier uses of this buffer
+                if (k >= 1 && !wait_all(&bars[HS_EMPTY + hb], (uint32_t)((k - 1) & 1))) return false;
             }
-            fence_proxy_async();
-            fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bars[HS_FULL + c.h]);
-            return true;
-        };
-        // rule + store of column half c.h of C(c.j)
-        auto rule = [&](const Cursor& c) -> bool {
-            if (!wait_all(&bars[C_FULL + c.h], (uint32_t)(c.j & 1))) return false;
+            if (r && !wait_all(&bars[C_FULL + r->h], (uint32_t)(r->j & 1))) return false;
             fence_after();
-            const int gi = c.ty * p.Tr + m;
-            const bool row_ok = (m < p.Tr) && (gi < p.n);
-            const uint8_t* xrow = xs + c.st * kXB + xr * 128;  // (CENTRE_SMEM: one X block per tile)
-            uint32_t* orow = p.dst + (size_t)(row_ok ? gi : 0) * (size_t)p.wpitch;
-            const uint32_t* crow = p.src + (size_t)(row_ok ? gi : 0) * (size_t)p.wpitch;
-            const int w0 = c.tx * (Tc >> 5);
-            const int i0 = c.h ? half0 : 0, i1 = c.h ? nch : half0;
-            for (int i = i0 + grp; i < i1; i += kGroups) {
-                uint32_t v[16];
-                tmem_ld32p(tmem + lane_off + kCCol + kHalfCols * c.h + kN1 * (i - i0), v);
-                const int wi = w0 + i;
-                const bool store = row_ok && wi < p.nw;
-                uint32_t Ga[8], Gb[8];
-                uint32_t cw = 0u;
+            // this group's chunks: at most one to re-quantise, at most one rule chunk
+            int iq = -1, ir = -1, iq0 = 0, ir0 = 0;
+            if (q) {
+                iq0 = q->h ? half0 : 0;
+                const int i1 = q->h ? nch : half0;
+                for (int i = iq0; i < i1; ++i)
+                    if ((rq_mask >> i) & 1u) iq = i;
+            }
+            if (r) {
+                ir0 = r->h ? half0 : 0;
+                const int i1 = r->h ? nch : half0;
+                if (ir0 + grp < i1) ir = ir0 + grp;
+            }
+            uint32_t vq[16], vr[16];
+            if (iq >= 0) tmem_ld32p(tmem + lane_off + kHCol + kHalfCols * q->h + kN1 * (iq - iq0), vq);
+            if (ir >= 0) tmem_ld32p(tmem + lane_off + kCCol + kHalfCols * r->h + kN1 * (ir - ir0), vr);
+            // rule operands that do not come from TMEM, fetched while the loads are in flight
+            int gi = 0, wi = 0;
+            bool store = false;
+            uint32_t Ga[8], Gb[8];
+            uint32_t cw = 0u;
+            if (ir >= 0) {
+                gi = r->ty * p.Tr + m;
+                wi = r->tx * (Tc >> 5) + ir;
+                store = (m < p.Tr) && (gi < p.n) && wi < p.nw;
                 if (CENTRE_SMEM) {
                     // centre cells: groups ga and ga + 1 of the X row (8 words each)
-                    const int ga = i + aoff, gb = ga + 1;
+                    const uint8_t* xrow = xs + r->st * kXB + xr * 128;  // one X block per tile
+                    const int ga = ir + aoff, gb = ga + 1;
                     const uint4 a0 = *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3)) ^ xsw) << 4));
                     const uint4 a1 =
                         *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3) + 1) ^ xsw) << 4));
@@ -495,59 +504,76 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                     Gb[4] = b1.x; Gb[5] = b1.y; Gb[6] = b1.z; Gb[7] = b1.w;
                 } else {
                     // the output word's own cells in the current grid (word-aligned)
-                    cw = store ? __ldg(crow + wi) : 0u;
+                    cw = store ? __ldg(p.src + (size_t)gi * (size_t)p.wpitch + wi) : 0u;
                 }
-                tmem_wait16(v);
-                uint32_t acc = 0u;
-                if (!LANES16) {
-                    // accumulator column 4k+j = output cell 8j+k: four box counts per
-                    // register, bit 7 of each byte lane = the rule's result
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const uint32_t B4 = prmt(v[2 * k], v[2 * k + 1], 0x6420u);
-                        const uint32_t s4 = CENTRE_SMEM ? prmt(Ga[k], Gb[k], 0x5432u) : (cw >> k) & 0x01010101u;
-                        const uint32_t ge = (B4 + nlo0) + s4 * dlo;  // bit 7: B >= lo(s)
-                        const uint32_t le = (hiH0 + s4 * dhi) - B4;  // bit 7: B <= hi(s)
-                        acc |= (ge & le & 0x80808080u) >> (7 - k);
-                    }
-                } else {
-                    // accumulator column 2r+e = output cell 16e+r: two box counts per
-                    // register, bit 15 of each 16-bit lane = the rule's result
-#pragma unroll
-                    for (int r = 0; r < 16; ++r) {
-                        const uint32_t hsel = (uint32_t)(r >> 3);
-                        const uint32_t s2 = CENTRE_SMEM ? prmt(Ga[r & 7], Gb[r & 7],
-                                                               (2u + hsel) | 0x80u | ((4u + hsel) << 8) | 0x8000u)
-                                                        : (cw >> r) & 0x00010001u;
-                        const uint32_t ge = (v[r] + nlo0) + s2 * dlo;
-                        const uint32_t le = (hiH0 + s2 * dhi) - v[r];
-                        acc |= (ge & le & 0x80008000u) >> (15 - r);
-                    }
-                }
-                if (store) orow[wi] = acc;
             }
-            fence_before();
-            __syncwarp();
-            if (lane == 0) {
-                mbar_arrive(&bars[C_EMPTY + c.h]);
-                if (CENTRE_SMEM && c.h == 1) mbar_arrive(&bars[X_EMPTY + c.st]);
+            tmem_wait_2x16(vq, vr);
+            if (q) {
+                if (iq >= 0) {
+                    uint8_t* hsb = hs + hb * 128 * kHalfCols;
+#pragma unroll
+                    for (int hh = 0; hh < 2; ++hh) {
+                        uint4 wv;
+                        wv.x = prmt(vq[8 * hh + 0], vq[8 * hh + 1], 0x6420u);
+                        wv.y = prmt(vq[8 * hh + 2], vq[8 * hh + 3], 0x6420u);
+                        wv.z = prmt(vq[8 * hh + 4], vq[8 * hh + 5], 0x6420u);
+                        wv.w = prmt(vq[8 * hh + 6], vq[8 * hh + 7], 0x6420u);
+                        *(uint4*)(hsb + ((2 * (iq - iq0) + hh) * 128 + m) * 16) = wv;
+                    }
+                }
+                fence_proxy_async();
+                fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bars[HS_FULL + q->h]);
+            }
+            if (r) {
+                if (ir >= 0) {
+                    uint32_t acc = 0u;
+                    if (!LANES16) {
+                        // accumulator column 4k+j = output cell 8j+k: four box counts per
+                        // register, bit 7 of each byte lane = the rule's result
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            const uint32_t B4 = prmt(vr[2 * k], vr[2 * k + 1], 0x6420u);
+                            const uint32_t s4 = CENTRE_SMEM ? prmt(Ga[k], Gb[k], 0x5432u) : (cw >> k) & 0x01010101u;
+                            const uint32_t ge = (B4 + nlo0) + s4 * dlo;  // bit 7: B >= lo(s)
+                            const uint32_t le = (hiH0 + s4 * dhi) - B4;  // bit 7: B <= hi(s)
+                            acc |= (ge & le & 0x80808080u) >> (7 - k);
+                        }
+                    } else {
+                        // accumulator column 2r+e = output cell 16e+r: two box counts per
+                        // register, bit 15 of each 16-bit lane = the rule's result
+#pragma unroll
+                        for (int k = 0; k < 16; ++k) {
+                            const uint32_t hsel = (uint32_t)(k >> 3);
+                            const uint32_t s2 = CENTRE_SMEM ? prmt(Ga[k & 7], Gb[k & 7],
+                                                                   (2u + hsel) | 0x80u | ((4u + hsel) << 8) | 0x8000u)
+                                                            : (cw >> k) & 0x00010001u;
+                            const uint32_t ge = (vr[k] + nlo0) + s2 * dlo;
+                            const uint32_t le = (hiH0 + s2 * dhi) - vr[k];
+                            acc |= (ge & le & 0x80008000u) >> (15 - k);
+                        }
+                    }
+                    if (store) p.dst[(size_t)gi * (size_t)p.wpitch + wi] = acc;
+                }
+                fence_before();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&bars[C_EMPTY + r->h]);
+                    if (CENTRE_SMEM && r->h == 1) mbar_arrive(&bars[X_EMPTY + r->st]);
+                }
             }
             return true;
         };
         Cursor cq, cr;  // the unit to re-quantise next, the unit whose rule comes next
         cq.init(p);
         cr.init(p);
-        if (units >= 1) ok = requant(cq);
+        if (units >= 1) ok = stage(&cq, nullptr);
         cq.next_unit();
         for (; cr.u < units && ok; cr.next_unit()) {
-            if (cq.u < units) {
-                if (!requant(cq)) {
-                    ok = false;
-                    break;
-                }
-                cq.next_unit();
-            }
-            if (cr.b == nb - 1 && !rule(cr)) ok = false;
+            const bool has_q = cq.u < units;
+            ok = stage(has_q ? &cq : nullptr, cr.b == nb - 1 ? &cr : nullptr);
+            if (has_q) cq.next_unit();
         }
         if (!ok && lane == 0) atomicOr(p.err, 8u);
     }
@@ -703,21 +729,15 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
     int nlo_d, hiH_d, nlo_s, hiH_s;
     lane_consts(rule.bmin, rule.bmax, bits, nlo_d, hiH_d);
     lane_consts(rule.smin + 1, rule.smax + 1, bits, nlo_s, hiH_s);
-    // epilogue balance, per column half: the rule of the half's chunk c runs on
-    // group c % 4; each re-quantisation (about a quarter of a rule chunk's work,
-    // nb per tile) goes to the group with the least work in that half so far
+    // epilogue balance, per column half (<= 4 chunks): the rule of the half's
+    // chunk c runs on group c; its re-quantisations go first to the groups
+    // without a rule chunk, then round-robin, so that no group has more than one
+    // chunk of each kind per unit (the epilogue issues both TMEM loads at once)
     uint32_t rq_mask[kGroups] = {0, 0, 0, 0};
     for (int h = 0; h < 2; ++h) {
         const int c0 = h ? G.half0 : 0, c1 = h ? G.nchunks : G.half0;
-        int load[kGroups] = {0, 0, 0, 0};
-        for (int i = c0; i < c1; ++i) load[(i - c0) % kGroups] += 4;
-        for (int i = c0; i < c1; ++i) {
-            int g = 0;
-            for (int k = 1; k < kGroups; ++k)
-                if (load[k] < load[g]) g = k;
-            rq_mask[g] |= 1u << i;
-            load[g] += G.nb;
-        }
+        const int nc = c1 - c0;  // 1..4
+        for (int k = 0; k < nc; ++k) rq_mask[(nc + k) % kGroups] |= 1u << (c0 + k);
     }
     const int ng = 4 * G.atoms;
     const int nw = a.nw;

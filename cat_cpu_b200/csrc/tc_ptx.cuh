@@ -129,6 +129,19 @@ __device__ __forceinline__ void tmem_wait16(uint32_t (&v)[16]) {
                  : "memory");
 }
 
+// Waits for every tcgen05.ld this thread issued; both arrays count as written
+// by the wait (see tmem_wait16).
+__device__ __forceinline__ void tmem_wait_2x16(uint32_t (&a)[16], uint32_t (&b)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7]),
+                   "+r"(a[8]), "+r"(a[9]), "+r"(a[10]), "+r"(a[11]), "+r"(a[12]), "+r"(a[13]), "+r"(a[14]),
+                   "+r"(a[15]), "+r"(b[0]), "+r"(b[1]), "+r"(b[2]), "+r"(b[3]), "+r"(b[4]), "+r"(b[5]), "+r"(b[6]),
+                   "+r"(b[7]), "+r"(b[8]), "+r"(b[9]), "+r"(b[10]), "+r"(b[11]), "+r"(b[12]), "+r"(b[13]),
+                   "+r"(b[14]), "+r"(b[15])
+                 :
+                 : "memory");
+}
+
 // prmt.b32 in its default mode: result byte i is byte (sel nibble i & 7) of
 // {a, b} (a = bytes 0..3, b = bytes 4..7); a nibble with bit 3 set replicates
 // the selected byte's bit 7 instead (0x00 for a 0/1 byte).
