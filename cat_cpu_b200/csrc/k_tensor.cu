@@ -66,6 +66,10 @@ constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);
 constexpr int kMaxChunks = 7;  // Tc <= 224
 constexpr int kSmemLimit = 227 * 1024;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any legitimate wait
+// Back-off between barrier tries of the unpack and epilogue warps: they share
+// every scheduler with the single MMA-issuing warp, whose issue rate sets the
+// pace, so their spinning must not take its issue slots.
+constexpr uint32_t kSleepNs = 64;
 
 struct TcParams {
     const uint32_t* src;  // inner word (0, 0) of the current packed frame
@@ -409,7 +413,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         for (; c.xi < blocks; c.next_block(), cn.next_block()) {
             if (c.xi >= S) {
                 bool wt = true;
-                if (lane == 0) wt = mbar_wait(&bars[X_EMPTY + c.st], (uint32_t)(c.sph ^ 1), p.wait_ns);
+                if (lane == 0) wt = mbar_wait(&bars[X_EMPTY + c.st], (uint32_t)(c.sph ^ 1), p.wait_ns, kSleepNs);
                 ok = __shfl_sync(0xffffffffu, wt, 0);
                 if (!ok) break;
             }
@@ -445,7 +449,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         const int xsw = xr & 7;
         bool ok = true;
         auto wait_all = [&](uint64_t* bar, uint32_t ph) -> bool {
-            const bool wt = mbar_wait(bar, ph, p.wait_ns);
+            const bool wt = mbar_wait(bar, ph, p.wait_ns, kSleepNs);
             return __all_sync(0xffffffffu, wt);
         };
         // Per step of the loop: the re-quantisation of unit cq (H of its column half

@@ -40,13 +40,18 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
 
 // Bounded wait for `phase` of `bar`: false once `limit_ns` of wall time has
 // passed without the phase completing.  The clock is read once per 16 tries.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint64_t limit_ns) {
+// sleep_ns > 0 suspends the warp that long between tries, leaving the issue
+// slots of its scheduler to the warps that share it (for waiters off the
+// critical path; the MMA-issuing warp spins).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint64_t limit_ns, uint32_t sleep_ns = 0) {
     if (mbar_try(bar, phase)) return true;
     const uint64_t t0 = globaltimer();
     while (true) {
 #pragma unroll 1
-        for (int i = 0; i < 16; ++i)
+        for (int i = 0; i < 16; ++i) {
             if (mbar_try(bar, phase)) return true;
+            if (sleep_ns) __nanosleep(sleep_ns);
+        }
         if (globaltimer() - t0 > limit_ns) return false;
     }
 }
