@@ -217,8 +217,9 @@ struct Cursor {
 // LANES16: rule lanes (four 8-bit, or two 16-bit); CENTRE_SMEM: centre cells
 // from the X tile (single-block tiles) or from the packed input word; FAST:
 // n % 32 == 0 and large enough that rows and words wrap with one correction;
-// ATOMS: X tile width in 128-column swizzle atoms.
-template <bool LANES16, bool CENTRE_SMEM, bool FAST, int ATOMS>
+// ATOMS: X tile width in 128-column swizzle atoms; KS: product-1 K steps per
+// chunk (K1 / 32).  The window of chunk i starts at X group i (PADC - R < 32).
+template <bool LANES16, bool CENTRE_SMEM, bool FAST, int ATOMS, int KS>
 __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_constant__ TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -295,7 +296,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         // plus start-address offsets (in 16-byte units, within the 14-bit field).
         const uint32_t id1 = idesc_u8(kN1, false);
         const uint32_t id2a = idesc_u8(32 * half0, true), id2b = idesc_u8(32 * (nch - half0), true);
-        const int ksteps = K1 / 32;
         const uint64_t xd0 = desc_k_sw128(smem_u32(xs));
         const uint64_t bhd0 = desc_noswz(smem_u32(bh), kN1 * 16, 128);
         const uint64_t bvd0 = desc_noswz(smem_u32(bv), 128 * 16, 128);
@@ -308,15 +308,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             if (!__all_sync(0xffffffffu, mbar_wait(&bars[X_FULL + c.st], (uint32_t)c.sph, p.wait_ns))) return false;
             fence_after();
             if (leader) {
-                const int i0 = c.h ? half0 : 0, i1 = c.h ? nch : half0;
+                const int i0 = c.h ? half0 : 0, nci = c.h ? nch - half0 : half0;  // this half's chunks
                 const uint64_t xs0 = xd0 + (uint64_t)((c.st * kXB) >> 4);
-                uint32_t d = tmem + kHCol + kHalfCols * c.h;
-                for (int i = i0; i < i1; ++i, d += kN1) {
-                    for (int s = 0; s < ksteps; ++s) {
-                        const int col = 32 * (i + p.glo + s);  // X column of this K step
-                        const uint64_t ad = xs0 + (uint64_t)((((col >> 7) * kAtomBytes) + (col & 127)) >> 4);
-                        const uint64_t bd = bhd0 + (uint64_t)((s * 2 * kN1 * 16) >> 4);
-                        mma_i8(d, ad, bd, id1, s > 0 ? 1u : 0u);
+                const uint32_t d0 = tmem + kHCol + kHalfCols * c.h;
+#pragma unroll
+                for (int ci = 0; ci < 4; ++ci) {
+                    if (ci < nci) {
+#pragma unroll
+                        for (int s = 0; s < KS; ++s) {
+                            const int g = i0 + ci + s;  // X group of this K step: 16-byte units (g / 4) atoms + 2 (g % 4)
+                            const uint64_t ad = xs0 + (uint64_t)((g >> 2) * (kAtomBytes >> 4) + (g & 3) * 2);
+                            mma_i8(d0 + kN1 * ci, ad, bhd0 + (uint64_t)(s * 2 * kN1), id1, s > 0 ? 1u : 0u);
+                        }
                     }
                 }
                 if (!(p.inject_missing_commit && c.u == 0)) mma_commit(&bars[H_FULL + c.h]);
@@ -603,24 +606,28 @@ struct TensorPlan {
     unsigned int* err;
 };
 
-// The instantiations that exist: 8-bit lanes only with single-block tiles of 2
-// atoms (R <= 5); 16-bit lanes with single-block 2-atom tiles (R <= 32) or with
-// multi-block tiles of 2, 3 or 4 atoms.
-template <bool L16, bool CS, int A>
+// The instantiations that exist (R ranges as tensor_geometry lays them out):
+//   R <= 5       8-bit lanes, single block, 2 atoms, 2 K steps
+//   R 6..16      16-bit lanes, single block, 2 atoms, 2 K steps
+//   R 17..32     16-bit lanes, single block, 2 atoms, 4 K steps
+//   R 33..48     16-bit lanes, row blocks,   2 atoms, 4 K steps
+//   R 49..80     16-bit lanes, row blocks,   3 atoms, 6 K steps
+//   R 81..90     16-bit lanes, row blocks,   4 atoms, 8 K steps
+template <bool L16, bool CS, int A, int KS>
 static TcKernel pick_fast(bool fast) {
-    return fast ? k_tensor_step<L16, CS, true, A> : k_tensor_step<L16, CS, false, A>;
+    return fast ? k_tensor_step<L16, CS, true, A, KS> : k_tensor_step<L16, CS, false, A, KS>;
 }
-static TcKernel pick_kernel(bool lanes16, bool centre_smem, bool fast, int atoms) {
+static TcKernel pick_kernel(bool lanes16, bool centre_smem, bool fast, int atoms, int ks) {
+    if (!lanes16) return (centre_smem && atoms == 2 && ks == 2) ? pick_fast<false, true, 2, 2>(fast) : nullptr;
     if (centre_smem) {
         if (atoms != 2) return nullptr;
-        return lanes16 ? pick_fast<true, true, 2>(fast) : pick_fast<false, true, 2>(fast);
+        if (ks == 2) return pick_fast<true, true, 2, 2>(fast);
+        if (ks == 4) return pick_fast<true, true, 2, 4>(fast);
+        return nullptr;
     }
-    if (!lanes16) return nullptr;
-    switch (atoms) {
-        case 2: return pick_fast<true, false, 2>(fast);
-        case 3: return pick_fast<true, false, 3>(fast);
-        case 4: return pick_fast<true, false, 4>(fast);
-    }
+    if (atoms == 2 && ks == 4) return pick_fast<true, false, 2, 4>(fast);
+    if (atoms == 3 && ks == 6) return pick_fast<true, false, 3, 6>(fast);
+    if (atoms == 4 && ks == 8) return pick_fast<true, false, 4, 8>(fast);
     return nullptr;
 }
 
@@ -788,7 +795,7 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
     // one correction wraps a row (rows span [-R, n + 128 nb)) and a word index
     // (words span [-(PADC + 16) / 32, nw + ng)); groups are word halves
     const bool fast = a.n % 32 == 0 && nw > ng + 6 && a.n >= 128 * G.nb + R;
-    P->kernel = pick_kernel(G.lanes16 != 0, G.nb == 1, fast, G.atoms);
+    P->kernel = G.glo == 0 ? pick_kernel(G.lanes16 != 0, G.nb == 1, fast, G.atoms, G.K1 / 32) : nullptr;
     if (!P->kernel) {
         snprintf(why, why_len, "no kernel instantiation for R=%d", R);
         cudaFree(P->err);
