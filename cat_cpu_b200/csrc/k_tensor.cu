@@ -9,34 +9,41 @@
 //   - unpack warps read the tile's packed input words (rows and words taken
 //     modulo n: the torus wrap happens here, so no halo pass runs between
 //     generations) and spread every bit to a byte in shared memory, in the
-//     128-byte-swizzled K-major layout the MMA reads (128 rows x 256 columns);
-//   - product 1:  H = X * B_h   (row sums; M = 128 tile rows, N = 32-column
-//     chunks, K = the chunk's column window; u8 x u8 -> s32 in TMEM);
+//     128-byte-swizzled K-major layout the MMA reads (128 rows x 256..512 columns);
+//   - product 1:  H = X * B_h   (row sums; M = 128 tile rows, N = Tc, one MMA
+//     per 32-column K step of the tile's window; u8 x u8 -> s32 in TMEM);
 //   - H (<= 2R+1) is read back with tcgen05.ld, re-quantised to u8 and stored
 //     as the MN-major B operand of
-//   - product 2:  C = B_v * H   (column sums; M = 128, N = Tc, K = 128) with
-//     B_v[m][k] = [m <= k <= m + 2R], so the reference's transposed scatter
-//     between the two products (AMXSolver.cpp:321-325) disappears;
+//   - product 2:  C = B_v * H   (column sums; M = 128, N = Tc, K = 128 per row
+//     block) with B_v[m][k] = [m <= k <= m + 2R], so the reference's transposed
+//     scatter between the two products (AMXSolver.cpp:321-325) disappears;
 //   - epilogue: C is the box count including the centre; the birth/survival
 //     interval rule (HostSolver.tpp:47-73, k = C - centre) runs on four 8-bit
 //     (R <= 5) or two 16-bit lanes per register, and the result bits are
 //     gathered straight into the output word.
 //
+// MMA count.  A tcgen05.mma costs the issuing warp a few tens of cycles plus a
+// round trip through the barriers per batch, whatever its N, so a tile is done
+// in few, wide MMAs: product 1 is one MMA of N = Tc per K step (8 at R <= 16),
+// product 2 one per 32 rows of K (4 per row block).  The band matrix B_h of a
+// K step is the same matrix shifted by 32 columns per step, so one Toeplitz
+// matrix W of (KS + nchunks - 1) * 32 rows serves every step: the step's B
+// descriptor starts 32 rows further up.
+//
 // Column order.  A packed word w spreads to bytes with (w >> k) & 0x01010101,
 // k = 0..7: register k holds cells k, 8+k, 16+k, 24+k.  The shared-memory tile
 // keeps that order: within each 32-column group, byte position 4k+j holds the
 // group's cell 8j+k (the permutation pi(4k+j) = 8j+k).  Product 1 contracts over
-// the positions, so B_h's rows follow pi, and its columns (the N order of H
-// and C) are chosen so that the rule's result bits land in the output word's
-// own bit order with one shift per register (sigma below).  No byte is moved
-// to undo the permutation.
+// the positions, so W's K index follows pi, and its N index (the column order
+// of H and C within each 32-column chunk) is chosen so that the rule's result
+// bits land in the output word's own bit order with one shift per register
+// (sigma below).  No byte is moved to undo the permutation.
 //
-// Exactness: inputs are 0/1, H <= 2R+1 <= 65 fits u8, C <= (2R+1)^2 in s32.
+// Exactness: inputs are 0/1, H <= 2R+1 <= 181 fits u8, C <= (2R+1)^2 in s32.
 //
-// Every wait on an mbarrier is bounded (globaltimer, hardware-suspended
-// tries); on timeout the kernel sets a bit in an error word that the host
-// reads (ltl_synchronize), waits (bounded) for its own MMAs, frees its TMEM and
-// returns.
+// Every wait on an mbarrier is bounded (globaltimer); on timeout the kernel
+// sets a bit in an error word that the host reads (ltl_synchronize), waits
+// (bounded) for its own MMAs, frees its TMEM and returns.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -52,74 +59,80 @@ using namespace tc;
 // Geometry
 // ---------------------------------------------------------------------------
 constexpr int kAtomBytes = 128 * 128;  // one 128-row x 128-byte swizzle atom
-constexpr int kMaxAtoms = 4;           // X tile: 2..4 atoms = 256..512 columns
-constexpr int kMaxGroups = 4 * kMaxAtoms;  // 32-column groups per X row
 constexpr int kMaxStages = 4;
-constexpr int kHCol = 0;    // TMEM column of H
-constexpr int kCCol = 256;  // TMEM column of C
-constexpr int kN1 = 32;     // product-1 column chunk = one output word
-constexpr int kGroups = 4;  // epilogue column groups
-constexpr int kEpiWarps = 4 * kGroups;
-constexpr int kUnpackWarps = 4;              // one X row per unpack thread
-constexpr int kEpiWarp0 = 1 + kUnpackWarps;  // warp 0: MMA, 1..4: unpack, 5..20: epilogue
-constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);
-constexpr int kMaxChunks = 7;  // Tc <= 224
+constexpr int kTc = 128;     // output columns per tile
+constexpr int kChunks = kTc / 32;
+constexpr int kN1 = 32;      // one chunk = one output word
+constexpr int kUnpackWarps = 4;       // one X row per unpack thread
+constexpr int kRqWarps = 2 * 4;       // re-quantisation: two chunks per warp, four lane quarters
+constexpr int kRuleWarps = kChunks * 4;  // rule: one chunk per warp
+// warp 0: product-1 MMAs, warp 1: product-2 MMAs, 2..5: unpack,
+// 6..13: re-quantisation, 14..29: rule
+constexpr int kUnpackWarp0 = 2;
+constexpr int kRqWarp0 = kUnpackWarp0 + kUnpackWarps;
+constexpr int kRuleWarp0 = kRqWarp0 + kRqWarps;
+constexpr int kThreads = 32 * (kRuleWarp0 + kRuleWarps);
+constexpr int kWordDepth = 4;  // packed-word ring of the unpack warps: units in flight
 constexpr int kSmemLimit = 227 * 1024;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any legitimate wait
 // Back-off between barrier tries of the unpack and epilogue warps: they share
-// every scheduler with the single MMA-issuing warp, whose issue rate sets the
-// pace, so their spinning must not take its issue slots.
-constexpr uint32_t kSleepNs = 64;
+// every scheduler with the single MMA-issuing warp, whose waits are the
+// critical ones and do not sleep.
+constexpr uint32_t kSleepNs = 32;
+// TMEM columns: H in two buffers (units alternate), C in two buffers (tiles alternate)
+__host__ __device__ constexpr uint32_t h_col(int buf) { return 128u * (uint32_t)buf; }
+__host__ __device__ constexpr uint32_t c_col(int buf) { return 256u + 128u * (uint32_t)buf; }
 
 struct TcParams {
     const uint32_t* src;  // inner word (0, 0) of the current packed frame
     uint32_t* dst;        // inner word (0, 0) of the next packed frame
     long long wpitch;     // words per frame row
     int n, nw;
-    int R, PADC, glo, K1;  // column halo of a tile (16 mod 32), first window group, product-1 K
-    int Tr, Tc, nchunks;
-    int half0;        // chunks of column half 0 (half 1 has nchunks - half0); each <= 4
-    int atoms;        // X tile width = 128 * atoms columns
+    int R, PADC;      // radius, column halo of a tile (16 mod 32)
+    int Tr;           // output rows per tile
     int nb;           // 128-row X blocks per tile: product 2 contracts over 128 * nb rows
     int stages;       // X ring stages
-    int nhs;          // H buffers in shared memory (1 or 2)
     int tiles_x, tiles_y;
     uint32_t nlo0, dlo, hiH0, dhi;  // rule constants (lane-broadcast; d* = live minus dead, mod 2^32)
-    uint32_t rq_mask[kGroups];      // bit i: this epilogue group re-quantises chunk i
     unsigned int* err;
     unsigned long long wait_ns;
     int inject_missing_commit;  // test hook: product 1 of the first unit never signals
 };
 
 struct SmemLayout {
-    int x_off, hs_off, bh_off, bv_off, bar_off, tmem_off, total;
+    int x_off, wr_off, hs_off, w_off, bv_off, bar_off, tmem_off, total;
 };
 
 enum Bar {
     X_FULL = 0,
     X_EMPTY = kMaxStages,
-    H_FULL = 2 * kMaxStages,  // [2]: per TMEM column half
-    HS_FULL = H_FULL + 2,     // [2]
-    HS_EMPTY = HS_FULL + 2,   // [2]: per shared-memory H buffer
-    C_FULL = HS_EMPTY + 2,    // [2]
+    H_FULL = 2 * kMaxStages,  // [2] per H buffer
+    H_EMPTY = H_FULL + 2,     // [2]
+    HS_FULL = H_EMPTY + 2,    // [2] per shared-memory H buffer
+    HS_EMPTY = HS_FULL + 2,   // [2]
+    C_FULL = HS_EMPTY + 2,    // [2] per C buffer
     C_EMPTY = C_FULL + 2,     // [2]
-    DRAIN = C_EMPTY + 2,
-    NBARS
+    DRAIN = C_EMPTY + 2,      // [2] per MMA-issuing warp
+    NBARS = DRAIN + 2
 };
 
-constexpr int kHalfCols = 128;  // TMEM columns of one half's H or C (4 chunks)
+// W: (ng + kChunks - 1) * 32 rows (the N index) x 32 bytes (the K index of one step)
+__host__ __device__ constexpr int w_rows(int ng) { return 32 * (ng + kChunks - 1); }
+__host__ __device__ constexpr int atoms_for(int ng) { return (ng + 3) / 4; }
 
-__host__ __device__ inline SmemLayout smem_layout(int stages, int atoms, int nhs, int K1, int nb) {
+__host__ __device__ inline SmemLayout smem_layout(int stages, int ng, int nb, bool fast) {
     SmemLayout L{};
     int o = 0;
     L.x_off = o;
-    o += stages * atoms * kAtomBytes;  // 1024-aligned stages
+    o += stages * atoms_for(ng) * kAtomBytes;  // 1024-aligned stages
+    L.wr_off = o;
+    o += fast ? kWordDepth * (ng + 1) * 128 * 4 : 0;  // packed words of the next units
     L.hs_off = o;
-    o += nhs * 128 * kHalfCols;        // one half's H as u8, MN-major, one or two buffers
-    L.bh_off = o;
-    o += kN1 * K1;                     // B_h
+    o += 2 * 128 * kTc;                        // H as u8, MN-major, two buffers
+    L.w_off = o;
+    o += 32 * w_rows(ng);                      // W
     L.bv_off = o;
-    o += 128 * 128 * nb;               // B_v, 128 x (128 nb)
+    o += 128 * 128 * nb;                       // B_v, 128 x (128 nb)
     o = (o + 7) & ~7;
     L.bar_off = o;
     o += NBARS * 8;
@@ -163,107 +176,109 @@ __device__ __forceinline__ uint32_t fetch32(const uint32_t* __restrict__ row, in
 }
 
 // Position in this CTA's stream of work, advanced incrementally (no integer
-// division in the loops).  Tiles t = blockIdx.x + j * gridDim.x, X blocks xi =
-// j * nb + b, units u = 2 xi + h (h = column half).
-struct Cursor {
-    int u, h;        // unit and its column half
-    int xi, b, j;    // X block, row block within the tile, tile count
-    int st, sph;     // X ring stage of block xi and its phase parity ((xi / stages) & 1)
-    int ty, tx;      // tile coordinates
+// division in the loops).  Tiles t = blockIdx.x + j * gridDim.x, units (X
+// blocks) u = j * nb + b.  The strides live in a Walk shared by the cursors
+// of a thread.
+struct Walk {
     int step_x, step_y, tiles_x, nb, stages;
-
-    __device__ void init(const TcParams& p) {
-        u = h = xi = b = j = st = sph = 0;
+    __device__ explicit Walk(const TcParams& p) {
         tiles_x = p.tiles_x;
         nb = p.nb;
         stages = p.stages;
-        ty = (int)blockIdx.x / tiles_x;
-        tx = (int)blockIdx.x - ty * tiles_x;
         step_y = (int)gridDim.x / tiles_x;
         step_x = (int)gridDim.x - step_y * tiles_x;
     }
-    __device__ void next_block() {
-        ++xi;
-        if (++st == stages) {
+};
+
+struct Cursor {
+    int u, b, j;  // unit, row block within the tile, tile count
+    int st, sph;  // X ring stage of unit u and its phase parity ((u / stages) & 1)
+    int ty, tx;   // tile coordinates
+
+    __device__ void init(const Walk& w) {
+        u = b = j = st = sph = 0;
+        ty = (int)blockIdx.x / w.tiles_x;
+        tx = (int)blockIdx.x - ty * w.tiles_x;
+    }
+    __device__ void next(const Walk& w) {
+        ++u;
+        if (++st == w.stages) {
             st = 0;
             sph ^= 1;
         }
-        if (++b == nb) {
+        if (++b == w.nb) {
             b = 0;
             ++j;
-            tx += step_x;
-            ty += step_y;
-            if (tx >= tiles_x) {
-                tx -= tiles_x;
+            tx += w.step_x;
+            ty += w.step_y;
+            if (tx >= w.tiles_x) {
+                tx -= w.tiles_x;
                 ++ty;
             }
         }
     }
-    __device__ void next_unit() {
-        ++u;
-        h ^= 1;
-        if (h == 0) next_block();
-    }
 };
 
-// The work is a stream of units u = ((tile j * nb + row block b) * 2 + column
-// half h).  Per X block (j, b) the unpack warps fill one stage; per unit the MMA
-// warp runs product 1 for the half's chunks into TMEM half h of H, the epilogue
-// re-quantises it to shared memory, and product 2 adds B_v[:, 128b ..] * H to
-// TMEM half h of C.  After a tile's last block the epilogue applies the rule to
-// C half h.  The two halves use separate TMEM columns (H: [0, 256), C: [256,
-// 512)), so the tensor core works on one half while the epilogue reads the other.
+// The work is a stream of units u = tile j * nb + row block b.  Per unit the
+// unpack warps fill one X stage, one MMA warp runs product 1 into H buffer
+// u % 2, the epilogue re-quantises H to shared-memory buffer u % 2, and
+// another MMA warp adds product 2, B_v[:, 128b ..] * H, to C buffer j % 2.
+// After a tile's last block the epilogue applies the rule to C.  With two
+// buffers at every hand-over and the epilogue re-quantising unit u before it
+// applies the rule to unit u - 1, the tensor core has the next unit's product 1
+// queued while the epilogue finishes the previous one.
 //
-// LANES16: rule lanes (four 8-bit, or two 16-bit); CENTRE_SMEM: centre cells
-// from the X tile (single-block tiles) or from the packed input word; FAST:
-// n % 32 == 0 and large enough that rows and words wrap with one correction;
-// ATOMS: X tile width in 128-column swizzle atoms; KS: product-1 K steps per
-// chunk (K1 / 32).  The window of chunk i starts at X group i (PADC - R < 32).
-template <bool LANES16, bool CENTRE_SMEM, bool FAST, int ATOMS, int KS>
+// LANES16: rule lanes (four 8-bit, or two 16-bit); FAST: n % 32 == 0 and
+// large enough that rows and words wrap with one correction; NG: product-1 K
+// steps = X groups of 32 columns per row.
+template <bool LANES16, bool FAST, int NG>
 __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_constant__ TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const SmemLayout L = smem_layout(p.stages, ATOMS, p.nhs, p.K1, p.nb);
+    constexpr int ATOMS = atoms_for(NG);
+    const int nb = p.nb, S = p.stages, R = p.R;
+    const SmemLayout L = smem_layout(S, NG, nb, FAST);
     uint8_t* xs = smem + L.x_off;
     uint8_t* hs = smem + L.hs_off;
-    uint8_t* bh = smem + L.bh_off;
+    uint8_t* wm = smem + L.w_off;
     uint8_t* bv = smem + L.bv_off;
     uint64_t* bars = (uint64_t*)(smem + L.bar_off);
     uint32_t* tmem_slot = (uint32_t*)(smem + L.tmem_off);
     constexpr int kXB = ATOMS * kAtomBytes;  // bytes of one X stage
-    constexpr int kNG = 4 * ATOMS;           // 32-column groups per X row
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int R = p.R, Tc = p.Tc, K1 = p.K1, nb = p.nb, S = p.stages, nhs = p.nhs;
     const int ntiles = p.tiles_x * p.tiles_y;
     const int mine = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-    const int units = mine * nb * 2;
+    const int units = mine * nb;
     constexpr uint32_t kTmemCols = 512;
 
     if (tid == 0) {
         for (int i = 0; i < S; ++i) {
             mbar_init(&bars[X_FULL + i], kUnpackWarps);
-            mbar_init(&bars[X_EMPTY + i], CENTRE_SMEM ? kEpiWarps : 1);
+            mbar_init(&bars[X_EMPTY + i], 1);
         }
-        for (int h = 0; h < 2; ++h) {
-            mbar_init(&bars[H_FULL + h], 1);
-            mbar_init(&bars[HS_FULL + h], kEpiWarps);
-            mbar_init(&bars[HS_EMPTY + h], 1);
-            mbar_init(&bars[C_FULL + h], 1);
-            mbar_init(&bars[C_EMPTY + h], kEpiWarps);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&bars[H_FULL + i], 1);
+            mbar_init(&bars[H_EMPTY + i], kRqWarps);
+            mbar_init(&bars[HS_FULL + i], kRqWarps);
+            mbar_init(&bars[HS_EMPTY + i], 1);
+            mbar_init(&bars[C_FULL + i], 1);
+            mbar_init(&bars[C_EMPTY + i], kRuleWarps);
+            mbar_init(&bars[DRAIN + i], 1);
         }
-        mbar_init(&bars[DRAIN], 1);
         fence_mbar_init();
     }
     if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
-    // B_h (K-major, no swizzle: [k / 16][n][16 bytes]), K1 x 32.  Row k is byte
-    // position k of the chunk's window (group glo + k / 32, permuted by pi), column
-    // n is accumulator column n (output cell sigma(n) of the chunk).
-    for (int idx = tid; idx < kN1 * K1; idx += kThreads) {
-        const int k = idx / kN1, nn = idx % kN1;
-        const int xc = 32 * (p.glo + (k >> 5)) + perm_pi(k & 31);  // X column relative to the chunk
-        const int d = xc - p.PADC - perm_sigma(nn, LANES16);
-        bh[((k >> 4) * kN1 + nn) * 16 + (k & 15)] = (d >= -R && d <= R) ? 1 : 0;
+    // W (B operand of product 1, K-major, no swizzle: [m / 8][k / 16][8][16 bytes],
+    // m < w_rows, k < 32).  Row m belongs to chunk offset D = NG - 1 - m / 32 and
+    // accumulator column m % 32 of that chunk; byte k is position k of a group (cell
+    // pi(k)).  K step s reads rows [32 (NG - 1 - s), + kTc): there, accumulator
+    // column n of chunk c = n / 32 meets X group s, D = s - c.
+    for (int idx = tid; idx < w_rows(NG) * 32; idx += kThreads) {
+        const int m = idx >> 5, k = idx & 31;
+        const int D = NG - 1 - (m >> 5);
+        const int d = 32 * D + perm_pi(k) - p.PADC - perm_sigma(m & 31, LANES16);
+        wm[((m >> 3) * 2 + (k >> 4)) * 128 + (m & 7) * 16 + (k & 15)] = (d >= -R && d <= R) ? 1 : 0;
     }
     // B_v[m][k] = [m <= k <= m + 2R], m < 128, k < 128 nb (K-major, no swizzle, 16 bytes per store)
     for (int idx = tid; idx < 8 * nb * 128; idx += kThreads) {
@@ -286,144 +301,101 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tmem_slot;
-    const int half0 = p.half0, nch = p.nchunks;
 
-    if (warp == 0) {
-        // --------------------------- MMA issuer -----------------------------
-        // The whole warp runs the loop (waits and descriptor arithmetic are
-        // warp-uniform); lane 0 alone issues the MMAs and the commits, so that
-        // every commit tracks every MMA before it.  Descriptors are 64-bit bases
-        // plus start-address offsets (in 16-byte units, within the 14-bit field).
-        const uint32_t id1 = idesc_u8(kN1, false);
-        const uint32_t id2a = idesc_u8(32 * half0, true), id2b = idesc_u8(32 * (nch - half0), true);
-        const uint64_t xd0 = desc_k_sw128(smem_u32(xs));
-        const uint64_t bhd0 = desc_noswz(smem_u32(bh), kN1 * 16, 128);
-        const uint64_t bvd0 = desc_noswz(smem_u32(bv), 128 * 16, 128);
-        const uint64_t hsd0 = desc_noswz(smem_u32(hs), 128, 128 * 16);
+    if (warp < kUnpackWarp0) {
+        // --------------------------- MMA issuers ----------------------------
+        // Warp 0 issues product 1 of every unit, warp 1 product 2, so that the
+        // tensor core queue gets the next unit's product 1 while product 2 waits
+        // for the epilogue, and the reverse.  Each warp runs its loop whole
+        // (waits and descriptor arithmetic are warp-uniform); its lane 0 alone
+        // issues the MMAs and the commits, so that every commit tracks every MMA
+        // of that warp before it.  Descriptors are 64-bit bases plus
+        // start-address offsets in 16-byte units (within the 14-bit field).
         const bool leader = lane == 0;
-        Cursor c1, c2;  // product 1 runs two units ahead of product 2
-        c1.init(p);
-        c2.init(p);
-        auto product1 = [&](const Cursor& c) -> bool {
-            if (!__all_sync(0xffffffffu, mbar_wait(&bars[X_FULL + c.st], (uint32_t)c.sph, p.wait_ns))) return false;
-            fence_after();
-            if (leader) {
-                const int i0 = c.h ? half0 : 0, nci = c.h ? nch - half0 : half0;  // this half's chunks
-                const uint64_t xs0 = xd0 + (uint64_t)((c.st * kXB) >> 4);
-                const uint32_t d0 = tmem + kHCol + kHalfCols * c.h;
-#pragma unroll
-                for (int ci = 0; ci < 4; ++ci) {
-                    if (ci < nci) {
-#pragma unroll
-                        for (int s = 0; s < KS; ++s) {
-                            const int g = i0 + ci + s;  // X group of this K step: 16-byte units (g / 4) atoms + 2 (g % 4)
-                            const uint64_t ad = xs0 + (uint64_t)((g >> 2) * (kAtomBytes >> 4) + (g & 3) * 2);
-                            mma_i8(d0 + kN1 * ci, ad, bhd0 + (uint64_t)(s * 2 * kN1), id1, s > 0 ? 1u : 0u);
-                        }
-                    }
-                }
-                if (!(p.inject_missing_commit && c.u == 0)) mma_commit(&bars[H_FULL + c.h]);
-                // the centre cells come from global memory: the stage is free once both halves read it
-                if (!CENTRE_SMEM && c.h == 1) mma_commit(&bars[X_EMPTY + c.st]);
-            }
-            __syncwarp();
-            return true;
+        auto wait = [&](uint64_t* bar, uint32_t ph) -> bool {
+            return __all_sync(0xffffffffu, mbar_wait(bar, ph, p.wait_ns));
         };
-        // product 2 of unit c: C[h] (+)= B_v[:, 128b ..] * H(u), H(u) in buffer u % nhs
-        auto product2 = [&](const Cursor& c) -> bool {
-            if (c.b == 0 && c.j >= 1 &&
-                !__all_sync(0xffffffffu, mbar_wait(&bars[C_EMPTY + c.h], (uint32_t)(c.j - 1) & 1u, p.wait_ns)))
-                return false;
-            fence_after();
-            if (leader) {
-                const int hb = nhs == 2 ? c.h : 0;
-                const uint64_t hd = hsd0 + (uint64_t)((hb * 128 * kHalfCols) >> 4);
-                const uint64_t vd = bvd0 + (uint64_t)((4 * c.b * 2 * 128 * 16) >> 4);
-                const uint32_t id2 = c.h ? id2b : id2a;
-                const uint32_t d = tmem + kCCol + kHalfCols * c.h;
-#pragma unroll
-                for (int s = 0; s < 4; ++s)
-                    mma_i8(d, vd + (uint64_t)((s * 2 * 128 * 16) >> 4), hd + (uint64_t)((s * 32 * 16) >> 4), id2,
-                           (c.b > 0 || s > 0) ? 1u : 0u);
-                mma_commit(&bars[HS_EMPTY + hb]);
-                if (c.b == nb - 1) mma_commit(&bars[C_FULL + c.h]);
-            }
-            __syncwarp();
-            return true;
-        };
-        // Per unit u, once H(u) has been read back: product 2 of unit u (the
-        // epilogue waits for it next), then product 1 of unit u+2 into the
-        // TMEM half that H(u) has just left.
+        const Walk wk(p);
+        Cursor c;
+        c.init(wk);
         bool ok = true;
-        if (units >= 1) ok = product1(c1);
-        c1.next_unit();
-        if (ok && units >= 2) ok = product1(c1);
-        c1.next_unit();
-        for (; c2.u < units && ok; c2.next_unit(), c1.next_unit()) {
-            ok = __all_sync(0xffffffffu, mbar_wait(&bars[HS_FULL + c2.h], (uint32_t)(c2.xi & 1), p.wait_ns));
-            if (ok) ok = product2(c2);
-            if (ok && c1.u < units) ok = product1(c1);
+        if (warp == 0) {
+            // product 1 of unit c: H(u % 2) = X(u) * B_h
+            constexpr uint32_t id1 = idesc_u8(kTc, false);
+            const uint64_t xd0 = desc_k_sw128(smem_u32(xs));
+            const uint64_t wd0 = desc_noswz(smem_u32(wm), 128, 256);
+            for (; c.u < units && ok; c.next(wk)) {
+                const int hb = c.u & 1;
+                ok = wait(&bars[X_FULL + c.st], (uint32_t)c.sph);
+                if (ok && c.u >= 2) ok = wait(&bars[H_EMPTY + hb], (uint32_t)(((c.u >> 1) - 1) & 1));
+                if (!ok) break;
+                fence_after();
+                if (leader) {
+                    const uint64_t xs0 = xd0 + (uint64_t)((c.st * kXB) >> 4);
+#pragma unroll
+                    for (int s = 0; s < NG; ++s) {
+                        // X group s: atom s / 4, byte 32 (s % 4) of its rows; W from row 32 (NG - 1 - s)
+                        const uint64_t ad = xs0 + (uint64_t)((s >> 2) * (kAtomBytes >> 4) + (s & 3) * 2);
+                        const uint64_t bd = wd0 + (uint64_t)((NG - 1 - s) * 4 * (256 >> 4));
+                        mma_i8(tmem + h_col(hb), ad, bd, id1, s > 0 ? 1u : 0u);
+                    }
+                    if (!(p.inject_missing_commit && c.u == 0)) mma_commit(&bars[H_FULL + hb]);
+                    mma_commit(&bars[X_EMPTY + c.st]);  // the stage is free once product 1 has read it
+                }
+                __syncwarp();
+            }
+        } else {
+            // product 2 of unit c: C(j % 2) (+)= B_v[:, 128b ..] * H(u), H(u) from
+            // shared-memory buffer u % 2
+            constexpr uint32_t id2 = idesc_u8(kTc, true);
+            const uint64_t bvd0 = desc_noswz(smem_u32(bv), 128 * 16, 128);
+            const uint64_t hsd0 = desc_noswz(smem_u32(hs), 128, 128 * 16);
+            for (; c.u < units && ok; c.next(wk)) {
+                const int hb = c.u & 1, cb = c.j & 1;
+                ok = wait(&bars[HS_FULL + hb], (uint32_t)((c.u >> 1) & 1));
+                if (ok && c.b == 0 && c.j >= 2) ok = wait(&bars[C_EMPTY + cb], (uint32_t)(((c.j >> 1) - 1) & 1));
+                if (!ok) break;
+                fence_after();
+                if (leader) {
+                    const uint64_t hd = hsd0 + (uint64_t)((hb * 128 * kTc) >> 4);
+                    const uint64_t vd = bvd0 + (uint64_t)((c.b * 8 * 128 * 16) >> 4);
+#pragma unroll
+                    for (int s = 0; s < 4; ++s)
+                        mma_i8(tmem + c_col(cb), vd + (uint64_t)((s * 2 * 128 * 16) >> 4),
+                               hd + (uint64_t)((s * 32 * 16) >> 4), id2, (c.b > 0 || s > 0) ? 1u : 0u);
+                    mma_commit(&bars[HS_EMPTY + hb]);
+                    if (c.b == nb - 1) mma_commit(&bars[C_FULL + cb]);
+                }
+                __syncwarp();
+            }
         }
         if (!ok && leader) atomicOr(p.err, 2u);
         // never leave with an MMA in flight (TMEM is freed below)
-        if (leader) mma_commit(&bars[DRAIN]);
+        if (leader) mma_commit(&bars[DRAIN + warp]);
         __syncwarp();
-        if (!__all_sync(0xffffffffu, mbar_wait(&bars[DRAIN], 0u, p.wait_ns)) && leader) atomicOr(p.err, 32u);
-    } else if (warp < kEpiWarp0) {
+        if (!__all_sync(0xffffffffu, mbar_wait(&bars[DRAIN + warp], 0u, p.wait_ns)) && leader) atomicOr(p.err, 32u);
+    } else if (warp < kRqWarp0) {
         // ------------------------------ unpack ------------------------------
-        // Thread `row` (0..127) fills X row `row` of every stage: the kNG groups
-        // of 32 columns of one packed row.  The words of the next X block are
-        // loaded right after this one is stored, so their latency is spent
-        // waiting for a free stage rather than on the critical path.
-        const int row = tid - 32;
+        // Thread `row` (0..127) fills X row `row` of every stage: NG groups of 32
+        // columns of one packed row.
+        const int row = tid - 32 * kUnpackWarp0;
         const int sw = row & 7;
-        const int blocks = mine * nb;
-        uint32_t w[kNG + 1];
-        // FAST: the kNG + 1 words that hold X row `row` of the cursor's block (group
-        // g = upper half of word g, lower half of word g + 1); otherwise the groups
-        auto gather = [&](const Cursor& c) {
-            const int gr0 = c.ty * p.Tr - R + 128 * c.b + row;
-            const int cbase = c.tx * Tc - p.PADC;  // column of X-tile column 0 (16 mod 32)
-            if (FAST) {
-                int gr = gr0;
-                if (gr < 0) gr += p.n;
-                else if (gr >= p.n) gr -= p.n;
-                const uint32_t* rp = p.src + (size_t)gr * (size_t)p.wpitch;
-                int wi = (cbase - 16) >> 5;  // word holding X column 0
-                if (wi < 0) wi += p.nw;
-#pragma unroll
-                for (int k = 0; k <= kNG; ++k) {
-                    w[k] = __ldg(rp + wi);
-                    if (++wi == p.nw) wi = 0;
-                }
-            } else {
-                const uint32_t* rp = p.src + (size_t)wrap_slow(gr0, p.n) * (size_t)p.wpitch;
-                int a = wrap_slow(cbase, p.n);
-#pragma unroll
-                for (int k = 0; k < kNG; ++k) {
-                    w[k] = fetch32(rp, a, p.n);
-                    a += 32;
-                    while (a >= p.n) a -= p.n;
-                }
-            }
-        };
+        const Walk wk(p);
+        Cursor c, cn;  // the unit being stored and the one being fetched
+        c.init(wk);
+        cn.init(wk);
         bool ok = true;
-        Cursor c, cn;  // the block being stored and the one being loaded
-        c.init(p);
-        cn.init(p);
-        if (blocks > 0) gather(cn);
-        cn.next_block();
-        for (; c.xi < blocks; c.next_block(), cn.next_block()) {
-            if (c.xi >= S) {
+        // spreads X row `row` of unit c to the stage: group g from x_of(g)
+        auto store = [&](const Cursor& cc, auto x_of) -> bool {
+            if (cc.u >= S) {
                 bool wt = true;
-                if (lane == 0) wt = mbar_wait(&bars[X_EMPTY + c.st], (uint32_t)(c.sph ^ 1), p.wait_ns, kSleepNs);
-                ok = __shfl_sync(0xffffffffu, wt, 0);
-                if (!ok) break;
+                if (lane == 0) wt = mbar_wait(&bars[X_EMPTY + cc.st], (uint32_t)(cc.sph ^ 1), p.wait_ns, kSleepNs);
+                if (!__shfl_sync(0xffffffffu, wt, 0)) return false;
             }
-            uint8_t* xrow = xs + c.st * kXB + row * 128;
+            uint8_t* xrow = xs + cc.st * kXB + row * 128;
 #pragma unroll
-            for (int g = 0; g < kNG; ++g) {
-                const uint32_t x = FAST ? prmt(w[g], w[g + 1], 0x5432u) : w[g];
+            for (int g = 0; g < NG; ++g) {
+                const uint32_t x = x_of(g);
                 uint32_t v[8];
 #pragma unroll
                 for (int k = 0; k < 8; ++k) v[k] = (x >> k) & 0x01010101u;
@@ -434,153 +406,177 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             }
             fence_proxy_async();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bars[X_FULL + c.st]);
-            if (cn.xi < blocks) gather(cn);
+            if (lane == 0) mbar_arrive(&bars[X_FULL + cc.st]);
+            return true;
+        };
+        if (FAST) {
+            // The NG + 1 packed words that hold X row `row` of a unit (group g =
+            // upper half of word g, lower half of word g + 1) travel by cp.async
+            // into a ring of kWordDepth units, so that several units' loads are in
+            // flight while this thread unpacks.
+            constexpr int NW1 = NG + 1;
+            uint32_t* ring = (uint32_t*)(smem + L.wr_off) + row;  // [kWordDepth][NW1][128]
+            auto fetch = [&](const Cursor& cc) {
+                int gr = cc.ty * p.Tr - R + 128 * cc.b + row;
+                if (gr < 0) gr += p.n;
+                else if (gr >= p.n) gr -= p.n;
+                const uint32_t* rp = p.src + (size_t)gr * (size_t)p.wpitch;
+                int wi = (cc.tx * kTc - p.PADC - 16) >> 5;  // word holding X column 0
+                if (wi < 0) wi += p.nw;
+                uint32_t* d = ring + (cc.u & (kWordDepth - 1)) * NW1 * 128;
+#pragma unroll
+                for (int k = 0; k < NW1; ++k) {
+                    cp_async4(d + k * 128, rp + wi);
+                    if (++wi == p.nw) wi = 0;
+                }
+            };
+#pragma unroll
+            for (int d = 0; d < kWordDepth - 1; ++d) {
+                if (cn.u < units) fetch(cn);
+                cp_async_commit();
+                cn.next(wk);
+            }
+            for (; c.u < units; c.next(wk)) {
+                if (cn.u < units) fetch(cn);
+                cp_async_commit();
+                cn.next(wk);
+                cp_async_wait<kWordDepth - 1>();  // unit c's words have landed
+                const uint32_t* d = ring + (c.u & (kWordDepth - 1)) * NW1 * 128;
+                uint32_t w[NW1];
+#pragma unroll
+                for (int k = 0; k < NW1; ++k) w[k] = d[k * 128];
+                ok = store(c, [&](int g) { return prmt(w[g], w[g + 1], 0x5432u); });
+                if (!ok) break;
+            }
+            cp_async_wait<0>();
+        } else {
+            uint32_t w[NG];
+            // the NG groups of X row `row` of unit cc, rows and columns taken modulo n
+            auto gather = [&](const Cursor& cc) {
+                const int gr0 = cc.ty * p.Tr - R + 128 * cc.b + row;
+                const uint32_t* rp = p.src + (size_t)wrap_slow(gr0, p.n) * (size_t)p.wpitch;
+                int a = wrap_slow(cc.tx * kTc - p.PADC, p.n);
+#pragma unroll
+                for (int k = 0; k < NG; ++k) {
+                    w[k] = fetch32(rp, a, p.n);
+                    a += 32;
+                    while (a >= p.n) a -= p.n;
+                }
+            };
+            for (; c.u < units; c.next(wk)) {
+                gather(c);
+                ok = store(c, [&](int g) { return w[g]; });
+                if (!ok) break;
+            }
         }
         if (!ok && lane == 0) atomicOr(p.err, 4u);
     } else {
         // ---------------------------- epilogue ------------------------------
-        const int ew = warp - kEpiWarp0;
-        const int q = warp & 3;          // TMEM lane quarter this warp may access
-        const int grp = ew >> 2;         // column group
-        const int m = q * 32 + lane;     // tile row (TMEM lane)
-        const uint32_t lane_off = (uint32_t)(q * 32) << 16;
-        const uint32_t rq_mask = p.rq_mask[grp];
-        const int aoff = (p.PADC - 16) >> 5;  // centre groups of chunk i: i + aoff, i + aoff + 1
-        const uint32_t nlo0 = p.nlo0, dlo = p.dlo, hiH0 = p.hiH0, dhi = p.dhi;
-        const int xr = min(m + R, 127);  // X row of this output row's centre cells (rows >= Tr are not stored)
-        const int xsw = xr & 7;
-        bool ok = true;
+        // TMEM lane quarter q (= warp % 4, the lanes a warp may access) holds tile
+        // rows 32q .. 32q + 31, one per thread.
+        const int q = warp & 3;
+        const int m = q * 32 + lane;  // tile row (TMEM lane)
         auto wait_all = [&](uint64_t* bar, uint32_t ph) -> bool {
             const bool wt = mbar_wait(bar, ph, p.wait_ns, kSleepNs);
             return __all_sync(0xffffffffu, wt);
         };
-        // Per step of the loop: the re-quantisation of unit cq (H of its column half
-        // -> u8 in shared memory, the B operand of product 2) and the rule of unit
-        // cr = cq - 1 (if that unit ends a tile).  Both TMEM loads are issued before
-        // one wait, so their latencies overlap.  Each group has at most one chunk of
-        // each per unit (a half has <= 4 chunks; the host plan spreads them).
-        auto stage = [&](const Cursor* q, const Cursor* r) -> bool {
-            int hb = 0;
-            if (q) {
-                if (!wait_all(&bars[H_FULL + q->h], (uint32_t)(q->xi & 1))) return false;
-                hb = nhs == 2 ? q->h : 0;
-                const int k = nhs == 2 ? q->xi : q->u;  // earlier uses of this buffer
-                if (k >= 1 && !wait_all(&bars[HS_EMPTY + hb], (uint32_t)((k - 1) & 1))) return false;
-            }
-            if (r && !wait_all(&bars[C_FULL + r->h], (uint32_t)(r->j & 1))) return false;
-            fence_after();
-            // this group's chunks: at most one to re-quantise, at most one rule chunk
-            int iq = -1, ir = -1, iq0 = 0, ir0 = 0;
-            if (q) {
-                iq0 = q->h ? half0 : 0;
-                const int i1 = q->h ? nch : half0;
-                for (int i = iq0; i < i1; ++i)
-                    if ((rq_mask >> i) & 1u) iq = i;
-            }
-            if (r) {
-                ir0 = r->h ? half0 : 0;
-                const int i1 = r->h ? nch : half0;
-                if (ir0 + grp < i1) ir = ir0 + grp;
-            }
-            uint32_t vq[16], vr[16];
-            if (iq >= 0) tmem_ld32p(tmem + lane_off + kHCol + kHalfCols * q->h + kN1 * (iq - iq0), vq);
-            if (ir >= 0) tmem_ld32p(tmem + lane_off + kCCol + kHalfCols * r->h + kN1 * (ir - ir0), vr);
-            // rule operands that do not come from TMEM, fetched while the loads are in flight
-            int gi = 0, wi = 0;
-            bool store = false;
-            uint32_t Ga[8], Gb[8];
-            uint32_t cw = 0u;
-            if (ir >= 0) {
-                gi = r->ty * p.Tr + m;
-                wi = r->tx * (Tc >> 5) + ir;
-                store = (m < p.Tr) && (gi < p.n) && wi < p.nw;
-                if (CENTRE_SMEM) {
-                    // centre cells: groups ga and ga + 1 of the X row (8 words each)
-                    const uint8_t* xrow = xs + r->st * kXB + xr * 128;  // one X block per tile
-                    const int ga = ir + aoff, gb = ga + 1;
-                    const uint4 a0 = *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3)) ^ xsw) << 4));
-                    const uint4 a1 =
-                        *(const uint4*)(xrow + (ga >> 2) * kAtomBytes + (((2 * (ga & 3) + 1) ^ xsw) << 4));
-                    const uint4 b0 = *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3)) ^ xsw) << 4));
-                    const uint4 b1 =
-                        *(const uint4*)(xrow + (gb >> 2) * kAtomBytes + (((2 * (gb & 3) + 1) ^ xsw) << 4));
-                    Ga[0] = a0.x; Ga[1] = a0.y; Ga[2] = a0.z; Ga[3] = a0.w;
-                    Ga[4] = a1.x; Ga[5] = a1.y; Ga[6] = a1.z; Ga[7] = a1.w;
-                    Gb[0] = b0.x; Gb[1] = b0.y; Gb[2] = b0.z; Gb[3] = b0.w;
-                    Gb[4] = b1.x; Gb[5] = b1.y; Gb[6] = b1.z; Gb[7] = b1.w;
-                } else {
-                    // the output word's own cells in the current grid (word-aligned)
-                    cw = store ? __ldg(p.src + (size_t)gi * (size_t)p.wpitch + wi) : 0u;
-                }
-            }
-            tmem_wait_2x16(vq, vr);
-            if (q) {
-                if (iq >= 0) {
-                    uint8_t* hsb = hs + hb * 128 * kHalfCols;
+        const Walk wk(p);
+        Cursor c;
+        c.init(wk);
+        bool ok = true;
+        if (warp < kRuleWarp0) {
+            // re-quantisation: H(u) -> u8 in shared-memory buffer u % 2 (MN-major B
+            // operand of product 2), chunks 2h and 2h + 1 of this lane quarter
+            const int h = (warp - kRqWarp0) >> 2;
+            const uint32_t lane_off = ((uint32_t)(q * 32) << 16) + (uint32_t)(2 * kN1 * h);
+            for (; c.u < units && ok; c.next(wk)) {
+                const int hb = c.u & 1;
+                ok = wait_all(&bars[H_FULL + hb], (uint32_t)((c.u >> 1) & 1));
+                if (!ok) break;
+                fence_after();
+                uint32_t va[16], vb[16];
+                tmem_ld32p(tmem + lane_off + h_col(hb), va);
+                tmem_ld32p(tmem + lane_off + h_col(hb) + kN1, vb);
+                tmem_wait_2x16(va, vb);
+                fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bars[H_EMPTY + hb]);
+                // product 2 of unit u - 2 has read the buffer
+                if (c.u >= 2) ok = wait_all(&bars[HS_EMPTY + hb], (uint32_t)(((c.u >> 1) - 1) & 1));
+                if (!ok) break;
+                uint8_t* hsb = hs + hb * 128 * kTc + m * 16;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const uint32_t* v = e ? vb : va;
 #pragma unroll
                     for (int hh = 0; hh < 2; ++hh) {
                         uint4 wv;
-                        wv.x = prmt(vq[8 * hh + 0], vq[8 * hh + 1], 0x6420u);
-                        wv.y = prmt(vq[8 * hh + 2], vq[8 * hh + 3], 0x6420u);
-                        wv.z = prmt(vq[8 * hh + 4], vq[8 * hh + 5], 0x6420u);
-                        wv.w = prmt(vq[8 * hh + 6], vq[8 * hh + 7], 0x6420u);
-                        *(uint4*)(hsb + ((2 * (iq - iq0) + hh) * 128 + m) * 16) = wv;
+                        wv.x = prmt(v[8 * hh + 0], v[8 * hh + 1], 0x6420u);
+                        wv.y = prmt(v[8 * hh + 2], v[8 * hh + 3], 0x6420u);
+                        wv.z = prmt(v[8 * hh + 4], v[8 * hh + 5], 0x6420u);
+                        wv.w = prmt(v[8 * hh + 6], v[8 * hh + 7], 0x6420u);
+                        *(uint4*)(hsb + (4 * h + 2 * e + hh) * 128 * 16) = wv;
                     }
                 }
                 fence_proxy_async();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bars[HS_FULL + hb]);
+            }
+        } else {
+            // rule: chunk grp of C(j % 2) for every tile j, bits straight into the output word
+            const int grp = (warp - kRuleWarp0) >> 2;
+            const uint32_t lane_off = ((uint32_t)(q * 32) << 16) + (uint32_t)(kN1 * grp);
+            const uint32_t nlo0 = p.nlo0, dlo = p.dlo, hiH0 = p.hiH0, dhi = p.dhi;
+            // output word of this thread in the tile of cursor c (offset, or -1)
+            auto out_at = [&](const Cursor& cc) -> long long {
+                const int gi = cc.ty * p.Tr + m;
+                const int wi = cc.tx * kChunks + grp;
+                if (m >= p.Tr || gi >= p.n || wi >= p.nw) return -1;
+                return (long long)gi * p.wpitch + wi;
+            };
+            // the centre word (the output word's own cells in the current grid) of
+            // the next tile is loaded while this one is processed
+            long long at = mine > 0 ? out_at(c) : -1;
+            uint32_t cw = at >= 0 ? __ldg(p.src + at) : 0u;
+            for (int j = 0; j < mine && ok; ++j) {
+                const int cb = j & 1;
+                ok = wait_all(&bars[C_FULL + cb], (uint32_t)((j >> 1) & 1));
+                if (!ok) break;
+                fence_after();
+                uint32_t v[16];
+                tmem_ld32p(tmem + lane_off + c_col(cb), v);
+                tmem_wait16(v);
                 fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&bars[HS_FULL + q->h]);
-            }
-            if (r) {
-                if (ir >= 0) {
-                    uint32_t acc = 0u;
-                    if (!LANES16) {
-                        // accumulator column 4k+j = output cell 8j+k: four box counts per
-                        // register, bit 7 of each byte lane = the rule's result
+                if (lane == 0) mbar_arrive(&bars[C_EMPTY + cb]);
+                uint32_t acc = 0u;
+                if (!LANES16) {
+                    // accumulator column 4k+j = output cell 8j+k: four box counts per
+                    // register, bit 7 of each byte lane = the rule's result
 #pragma unroll
-                        for (int k = 0; k < 8; ++k) {
-                            const uint32_t B4 = prmt(vr[2 * k], vr[2 * k + 1], 0x6420u);
-                            const uint32_t s4 = CENTRE_SMEM ? prmt(Ga[k], Gb[k], 0x5432u) : (cw >> k) & 0x01010101u;
-                            const uint32_t ge = (B4 + nlo0) + s4 * dlo;  // bit 7: B >= lo(s)
-                            const uint32_t le = (hiH0 + s4 * dhi) - B4;  // bit 7: B <= hi(s)
-                            acc |= (ge & le & 0x80808080u) >> (7 - k);
-                        }
-                    } else {
-                        // accumulator column 2r+e = output cell 16e+r: two box counts per
-                        // register, bit 15 of each 16-bit lane = the rule's result
-#pragma unroll
-                        for (int k = 0; k < 16; ++k) {
-                            const uint32_t hsel = (uint32_t)(k >> 3);
-                            const uint32_t s2 = CENTRE_SMEM ? prmt(Ga[k & 7], Gb[k & 7],
-                                                                   (2u + hsel) | 0x80u | ((4u + hsel) << 8) | 0x8000u)
-                                                            : (cw >> k) & 0x00010001u;
-                            const uint32_t ge = (vr[k] + nlo0) + s2 * dlo;
-                            const uint32_t le = (hiH0 + s2 * dhi) - vr[k];
-                            acc |= (ge & le & 0x80008000u) >> (15 - k);
-                        }
+                    for (int k = 0; k < 8; ++k) {
+                        const uint32_t B4 = prmt(v[2 * k], v[2 * k + 1], 0x6420u);
+                        const uint32_t s4 = (cw >> k) & 0x01010101u;
+                        const uint32_t ge = (B4 + nlo0) + s4 * dlo;  // bit 7: B >= lo(s)
+                        const uint32_t le = (hiH0 + s4 * dhi) - B4;  // bit 7: B <= hi(s)
+                        acc |= (ge & le & 0x80808080u) >> (7 - k);
                     }
-                    if (store) p.dst[(size_t)gi * (size_t)p.wpitch + wi] = acc;
+                } else {
+                    // accumulator column 2r+e = output cell 16e+r: two box counts per
+                    // register, bit 15 of each 16-bit lane = the rule's result
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const uint32_t s2 = (cw >> k) & 0x00010001u;
+                        const uint32_t ge = (v[k] + nlo0) + s2 * dlo;
+                        const uint32_t le = (hiH0 + s2 * dhi) - v[k];
+                        acc |= (ge & le & 0x80008000u) >> (15 - k);
+                    }
                 }
-                fence_before();
-                __syncwarp();
-                if (lane == 0) {
-                    mbar_arrive(&bars[C_EMPTY + r->h]);
-                    if (CENTRE_SMEM && r->h == 1) mbar_arrive(&bars[X_EMPTY + r->st]);
-                }
+                if (at >= 0) p.dst[at] = acc;
+                for (int b = 0; b < nb; ++b) c.next(wk);
+                at = j + 1 < mine ? out_at(c) : -1;
+                cw = at >= 0 ? __ldg(p.src + at) : 0u;
             }
-            return true;
-        };
-        Cursor cq, cr;  // the unit to re-quantise next, the unit whose rule comes next
-        cq.init(p);
-        cr.init(p);
-        if (units >= 1) ok = stage(&cq, nullptr);
-        cq.next_unit();
-        for (; cr.u < units && ok; cr.next_unit()) {
-            const bool has_q = cq.u < units;
-            ok = stage(has_q ? &cq : nullptr, cr.b == nb - 1 ? &cr : nullptr);
-            if (has_q) cq.next_unit();
         }
         if (!ok && lane == 0) atomicOr(p.err, 8u);
     }
@@ -607,28 +603,24 @@ struct TensorPlan {
 };
 
 // The instantiations that exist (R ranges as tensor_geometry lays them out):
-//   R <= 5       8-bit lanes, single block, 2 atoms, 2 K steps
-//   R 6..16      16-bit lanes, single block, 2 atoms, 2 K steps
-//   R 17..32     16-bit lanes, single block, 2 atoms, 4 K steps
-//   R 33..48     16-bit lanes, row blocks,   2 atoms, 4 K steps
-//   R 49..80     16-bit lanes, row blocks,   3 atoms, 6 K steps
-//   R 81..90     16-bit lanes, row blocks,   4 atoms, 8 K steps
-template <bool L16, bool CS, int A, int KS>
+//   R <= 5       8-bit lanes,  5 K steps
+//   R 6..16      16-bit lanes, 5 K steps
+//   R 17..48     16-bit lanes, 7 K steps (row blocks from R = 33)
+//   R 49..80     16-bit lanes, 9 K steps
+//   R 81..90     16-bit lanes, 11 K steps
+template <bool L16, int NG>
 static TcKernel pick_fast(bool fast) {
-    return fast ? k_tensor_step<L16, CS, true, A, KS> : k_tensor_step<L16, CS, false, A, KS>;
+    return fast ? k_tensor_step<L16, true, NG> : k_tensor_step<L16, false, NG>;
 }
-static TcKernel pick_kernel(bool lanes16, bool centre_smem, bool fast, int atoms, int ks) {
-    if (!lanes16) return (centre_smem && atoms == 2 && ks == 2) ? pick_fast<false, true, 2, 2>(fast) : nullptr;
-    if (centre_smem) {
-        if (atoms != 2) return nullptr;
-        if (ks == 2) return pick_fast<true, true, 2, 2>(fast);
-        if (ks == 4) return pick_fast<true, true, 2, 4>(fast);
-        return nullptr;
+static TcKernel pick_kernel(bool lanes16, bool fast, int ng) {
+    if (!lanes16) return ng == 5 ? pick_fast<false, 5>(fast) : nullptr;
+    switch (ng) {
+        case 5: return pick_fast<true, 5>(fast);
+        case 7: return pick_fast<true, 7>(fast);
+        case 9: return pick_fast<true, 9>(fast);
+        case 11: return pick_fast<true, 11>(fast);
+        default: return nullptr;
     }
-    if (atoms == 2 && ks == 4) return pick_fast<true, false, 2, 4>(fast);
-    if (atoms == 3 && ks == 6) return pick_fast<true, false, 3, 6>(fast);
-    if (atoms == 4 && ks == 8) return pick_fast<true, false, 4, 8>(fast);
-    return nullptr;
 }
 
 // Largest radius of the tensor step: box counts (2R+1)^2 must fit the 16-bit
@@ -665,50 +657,29 @@ static void lane_consts(int lo, int hi, int bits, int& nlo, int& hiH) {
 }
 
 // Tile geometry for radius R (also restated in tests/test_tensor_tiles.py):
-//   PADC = 16 + 32a >= R columns of halo on each side of the Tc output columns
+//   Tc = 128 output columns per tile (H and C, two buffers each, fill the 512
+//          TMEM columns);
+//   PADC = 16 + 32a >= R columns of halo on each side of the output columns
 //          (16 mod 32, so that every X group straddles two packed words by halves);
-//   the X tile is 2..4 swizzle atoms wide, chosen to minimise X columns per output
-//          column, with Tc <= 224 so that H and C fit 512 TMEM columns;
 //   nb = 1 row block for R <= 32 (Tr = 128 - 2R output rows per tile), else
 //          enough 128-row blocks for Tr = 128 rows plus 2R halo rows;
-//   K1 = the product-1 window of one 32-column chunk, whole 32-column groups.
+//   ng = ceil((PADC + Tc + R) / 32) product-1 K steps reach every X column
+//          that any output column of the tile needs.
 struct TensorGeometry {
-    int PADC, atoms, Tc, Tr, nb, glo, ghi, K1, nchunks, half0, lanes16, stages, nhs;
+    int PADC, Tr, nb, ng, lanes16, stages;
 };
 
-static bool tensor_geometry(int R, TensorGeometry& G) {
+static bool tensor_geometry(int R, bool fast, TensorGeometry& G) {
     G.PADC = R <= 16 ? 16 : 16 + 32 * ((R - 16 + 31) / 32);
     G.nb = R <= 32 ? 1 : (128 + 2 * R + 127) / 128;
     G.Tr = G.nb == 1 ? 128 - 2 * R : std::min(128, 128 * G.nb - 2 * R);
-    G.atoms = 0;
-    double best = 1e30;
-    for (int a = 2; a <= kMaxAtoms; ++a) {
-        const int tc = std::min(32 * kMaxChunks, ((128 * a - 2 * G.PADC) / 32) * 32);
-        if (tc < 32) continue;
-        const double cost = 128.0 * a / tc;
-        if (cost < best - 1e-9) {
-            best = cost;
-            G.atoms = a;
-            G.Tc = tc;
-        }
-    }
-    if (!G.atoms || G.Tr < 1) return false;
-    G.nchunks = G.Tc / 32;
-    G.half0 = (G.nchunks + 1) / 2;  // <= 4 chunks = 128 TMEM columns per half
-    G.glo = (G.PADC - R) / 32;
-    G.ghi = (G.PADC + 31 + R) / 32;
-    G.K1 = 32 * (G.ghi - G.glo + 1);
+    G.ng = (G.PADC + kTc + R + 31) / 32;
     G.lanes16 = (2 * R + 1) * (2 * R + 1) > 127 ? 1 : 0;
-    const int ng = 4 * G.atoms;
-    if ((G.nchunks - 1) + G.ghi > ng - 1) return false;                                   // product-1 windows
-    if (G.nb == 1 && (G.nchunks - 1) + (G.PADC - 16) / 32 + 1 > ng - 1) return false;     // centre groups
-    if ((2 * R + 1) * (2 * R + 1) >= (1 << 15) || 2 * R + 1 > 255) return false;
-    // deepest X ring and double H buffers that fit, in that order of preference
-    static const int pref[][2] = {{4, 2}, {3, 2}, {2, 2}, {2, 1}, {1, 2}, {1, 1}};
-    for (const auto& pr : pref) {
-        if (smem_layout(pr[0], G.atoms, pr[1], G.K1, G.nb).total + 1024 <= kSmemLimit) {
-            G.stages = pr[0];
-            G.nhs = pr[1];
+    if (G.Tr < 1 || (2 * R + 1) * (2 * R + 1) >= (1 << 15) || 2 * R + 1 > 255) return false;
+    // the deepest X ring that fits
+    for (int st = kMaxStages; st >= 2; --st) {
+        if (smem_layout(st, G.ng, G.nb, fast).total + 1024 <= kSmemLimit) {
+            G.stages = st;
             return true;
         }
     }
@@ -729,8 +700,13 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
         return nullptr;
     }
     const int R = rule.radius;
+    const int nw = a.nw;
+    // one correction wraps a row (rows span [-R, n + 128 nb)) and a word index
+    // (words span [-4, nw + ng)); groups are word halves
+    const int nb_of_r = R <= 32 ? 1 : (128 + 2 * R + 127) / 128;
+    const bool fast = a.n % 32 == 0 && nw >= 4 && a.n >= 128 * nb_of_r + R;
     TensorGeometry G{};
-    if (!tensor_geometry(R, G)) {
+    if (!tensor_geometry(R, fast, G)) {
         snprintf(why, why_len, "no tile shape for R=%d", R);
         return nullptr;
     }
@@ -740,18 +716,6 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
     int nlo_d, hiH_d, nlo_s, hiH_s;
     lane_consts(rule.bmin, rule.bmax, bits, nlo_d, hiH_d);
     lane_consts(rule.smin + 1, rule.smax + 1, bits, nlo_s, hiH_s);
-    // epilogue balance, per column half (<= 4 chunks): the rule of the half's
-    // chunk c runs on group c; its re-quantisations go first to the groups
-    // without a rule chunk, then round-robin, so that no group has more than one
-    // chunk of each kind per unit (the epilogue issues both TMEM loads at once)
-    uint32_t rq_mask[kGroups] = {0, 0, 0, 0};
-    for (int h = 0; h < 2; ++h) {
-        const int c0 = h ? G.half0 : 0, c1 = h ? G.nchunks : G.half0;
-        const int nc = c1 - c0;  // 1..4
-        for (int k = 0; k < nc; ++k) rq_mask[(nc + k) % kGroups] |= 1u << (c0 + k);
-    }
-    const int ng = 4 * G.atoms;
-    const int nw = a.nw;
     const PackedFrame* src[2] = {&a, &b};
     const PackedFrame* dst[2] = {&b, &a};
     for (int i = 0; i < 2; ++i) {
@@ -763,23 +727,15 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
         q.nw = nw;
         q.R = R;
         q.PADC = G.PADC;
-        q.glo = G.glo;
-        q.K1 = G.K1;
         q.Tr = G.Tr;
-        q.Tc = G.Tc;
-        q.nchunks = G.nchunks;
-        q.half0 = G.half0;
-        q.atoms = G.atoms;
         q.nb = G.nb;
         q.stages = G.stages;
-        q.nhs = G.nhs;
-        q.tiles_x = (a.n + G.Tc - 1) / G.Tc;
+        q.tiles_x = (a.n + kTc - 1) / kTc;
         q.tiles_y = (a.n + G.Tr - 1) / G.Tr;
         q.nlo0 = (uint32_t)nlo_d * bcast;
         q.dlo = (uint32_t)(nlo_s - nlo_d);
         q.hiH0 = (uint32_t)hiH_d * bcast;
         q.dhi = (uint32_t)(hiH_s - hiH_d);
-        for (int g = 0; g < kGroups; ++g) q.rq_mask[g] = rq_mask[g];
     }
     if (cudaMalloc(&P->err, sizeof(unsigned int)) != cudaSuccess) {
         snprintf(why, why_len, "error-flag allocation failed");
@@ -792,17 +748,14 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
         q.wait_ns = kWaitLimitNs;
         q.inject_missing_commit = 0;
     }
-    // one correction wraps a row (rows span [-R, n + 128 nb)) and a word index
-    // (words span [-(PADC + 16) / 32, nw + ng)); groups are word halves
-    const bool fast = a.n % 32 == 0 && nw > ng + 6 && a.n >= 128 * G.nb + R;
-    P->kernel = G.glo == 0 ? pick_kernel(G.lanes16 != 0, G.nb == 1, fast, G.atoms, G.K1 / 32) : nullptr;
+    P->kernel = pick_kernel(G.lanes16 != 0, fast, G.ng);
     if (!P->kernel) {
         snprintf(why, why_len, "no kernel instantiation for R=%d", R);
         cudaFree(P->err);
         delete P;
         return nullptr;
     }
-    P->smem_bytes = smem_layout(G.stages, G.atoms, G.nhs, G.K1, G.nb).total + 1024;
+    P->smem_bytes = smem_layout(G.stages, G.ng, G.nb, fast).total + 1024;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     P->grid = std::min(P->prm[0].tiles_x * P->prm[0].tiles_y, sms);

@@ -156,6 +156,18 @@ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
     return d;
 }
 
+// 4-byte asynchronous copy global -> shared (L1-allocating), tracked by the
+// issuing thread's commit groups.
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Wait until at most N of this thread's commit groups are still pending.
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Shared-memory matrix descriptors (tcgen05 "version 1" format).
 // K-major, 128-byte swizzle: 8-row atoms of 1024 B (SBO), LBO unused.
 __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t addr) {

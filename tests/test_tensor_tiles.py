@@ -4,16 +4,16 @@ oracle on the CPU.
 
 The kernel reads the packed grid, spreads each 32-cell group to bytes with
 (w >> k) & 0x01010101 (byte position 4k+j of a group holds cell pi(4k+j) =
-8j+k), contracts product 1 over those permuted positions with a band matrix
-B_h whose rows follow pi and whose columns follow sigma (the output cell of
-accumulator column n), sums rows with B_v in product 2, and applies the rule on
-8-bit (R <= 5) or 16-bit lanes with the centre cells taken from the same
-shared-memory tile through one byte permute per register.  The result bits are
-gathered into the output word by one shift per register.  This test runs that
-exact sequence (tile geometry, windows, torus wrap of rows and words, lane
-constants with 32-bit wraparound, byte permutes, gather) on whole small grids
-and compares every generation with the oracle, so that the index algebra is
-settled before the kernel runs on a GPU."""
+8j+k), and runs product 1 as one MMA of N = Tc per 32-column K step s of the
+whole X tile, against rows 32 (ks1 - 1 - s) .. of one Toeplitz band matrix W
+whose K index follows pi and whose N index follows sigma (the output cell of
+accumulator column n).  Product 2 sums rows with B_v, and the rule runs on
+8-bit (R <= 5) or 16-bit lanes with the centre cells taken from the packed
+input word.  The result bits are gathered into the output word by one shift
+per register.  This test runs that exact sequence (tile geometry, K steps,
+torus wrap of rows and words, lane constants with 32-bit wraparound, byte
+permutes, gather) on whole small grids and compares every generation with the
+oracle, so that the index algebra is settled before the kernel runs on a GPU."""
 import numpy as np
 import pytest
 
@@ -42,38 +42,31 @@ def lane_consts(lo, hi, bits):
 def plan(n, R, rule):
     """tensor_geometry + the rule constants of tensor_plan_create."""
     smin, smax, bmin, bmax = rule
+    Tc = 128
     PADC = 16 if R <= 16 else 16 + 32 * ((R - 16 + 31) // 32)
     nb = 1 if R <= 32 else (128 + 2 * R + 127) // 128
     Tr = 128 - 2 * R if nb == 1 else min(128, 128 * nb - 2 * R)
-    best, atoms, Tc = None, None, None
-    for a in (2, 3, 4):
-        tc = min(224, ((128 * a - 2 * PADC) // 32) * 32)
-        if tc < 32:
-            continue
-        cost = 128 * a / tc
-        if best is None or cost < best - 1e-9:
-            best, atoms, Tc = cost, a, tc
-    glo = (PADC - R) // 32
-    ghi = (PADC + 31 + R) // 32
-    K1 = 32 * (ghi - glo + 1)
+    ks1 = (PADC + Tc + R + 31) // 32
+    atoms = (ks1 + 3) // 4
     nchunks = Tc // 32
-    assert (nchunks - 1) + ghi <= 4 * atoms - 1
     lanes16 = (2 * R + 1) ** 2 > 127
     bits = 16 if lanes16 else 8
     bc = 0x00010001 if lanes16 else 0x01010101
     nlo_d, hih_d = lane_consts(bmin, bmax, bits)
     nlo_s, hih_s = lane_consts(smin + 1, smax + 1, bits)
-    return dict(PADC=PADC, Tc=Tc, Tr=Tr, nb=nb, atoms=atoms, glo=glo, K1=K1, nchunks=nchunks, lanes16=lanes16,
+    return dict(PADC=PADC, Tc=Tc, Tr=Tr, nb=nb, atoms=atoms, ks1=ks1, nchunks=nchunks, lanes16=lanes16,
                 nlo0=(nlo_d * bc) & 0xFFFFFFFF, dlo=(nlo_s - nlo_d) & 0xFFFFFFFF,
                 hiH0=(hih_d * bc) & 0xFFFFFFFF, dhi=(hih_s - hih_d) & 0xFFFFFFFF)
 
 
-def bh_matrix(P, R):
-    K1, glo, PADC, lanes16 = P["K1"], P["glo"], P["PADC"], P["lanes16"]
-    k = np.arange(K1)[:, None]
-    nn = np.arange(32)[None, :]
-    xc = 32 * (glo + (k >> 5)) + pi(k & 31)
-    d = xc - PADC - sigma(nn, lanes16)
+def w_matrix(P, R):
+    """W[m][k], m < 32 (ks1 + nchunks - 1), k < 32: row m serves chunk offset
+    D = ks1 - 1 - m // 32 and accumulator column m % 32; byte k of a group is cell pi(k)."""
+    ks1, nch, PADC, lanes16 = P["ks1"], P["nchunks"], P["PADC"], P["lanes16"]
+    m = np.arange(32 * (ks1 + nch - 1))[:, None]
+    k = np.arange(32)[None, :]
+    D = ks1 - 1 - (m >> 5)
+    d = 32 * D + pi(k) - PADC - sigma(m & 31, lanes16)
     return ((d >= -R) & (d <= R)).astype(np.int64)
 
 
@@ -91,12 +84,6 @@ def prmt(a, b, sel):
     return out
 
 
-def _word(Xc, base):
-    """Four consecutive bytes of every row of Xc as one little-endian 32-bit value."""
-    return (Xc[:, base] | (Xc[:, base + 1] << np.uint64(8)) | (Xc[:, base + 2] << np.uint64(16)) |
-            (Xc[:, base + 3] << np.uint64(24)))
-
-
 def tensor_step(grid, R, rule):
     """One generation exactly as k_tensor_step computes it (numpy, int arithmetic)."""
     n = grid.shape[0]
@@ -104,7 +91,9 @@ def tensor_step(grid, R, rule):
     PADC, Tc, Tr, nb = P["PADC"], P["Tc"], P["Tr"], P["nb"]
     XW = 128 * P["atoms"]
     assert Tr >= 1
-    Bh = bh_matrix(P, R)
+    W = w_matrix(P, R)
+    ks1 = P["ks1"]
+    assert 32 * ks1 <= XW
     m_ = np.arange(128)[:, None]
     k_ = np.arange(128 * nb)[None, :]
     Bv = ((k_ >= m_) & (k_ <= m_ + 2 * R)).astype(np.int64)
@@ -122,29 +111,21 @@ def tensor_step(grid, R, rule):
             # X tile in shared-memory byte order: position 32g + q holds cell pi(q) of group g
             cols = np.concatenate([(cbase + 32 * g + pi(q)) % n for g in range(XW // 32)])
             H = np.zeros((128 * nb, Tc), dtype=np.int64)
-            Xb = []
-            for b in range(nb):  # row blocks: product 1 per block
+            for b in range(nb):  # row blocks: product 1 per block, one MMA per K step
                 rows = (rbase + 128 * b + np.arange(128)) % n
                 X = grid[np.ix_(rows, cols)].astype(np.int64)
-                Xb.append(X)
-                for i in range(P["nchunks"]):
-                    w0 = 32 * (i + P["glo"])
-                    H[128 * b: 128 * b + 128, 32 * i: 32 * i + 32] = X[:, w0: w0 + P["K1"]] @ Bh
+                Hb = np.zeros((128, Tc), dtype=np.int64)
+                for st in range(ks1):
+                    m0 = 32 * (ks1 - 1 - st)
+                    Hb += X[:, 32 * st: 32 * st + 32] @ W[m0: m0 + Tc].T
+                H[128 * b: 128 * b + 128] = Hb
             assert H.max() <= 2 * R + 1
             C = Bv @ H  # box counts, centre included (product 2 over all blocks)
-            aoff = (PADC - 16) >> 5
-            xr = np.minimum(np.arange(128) + R, 127)
-            Xc = Xb[0][xr].astype(np.uint64)  # centre rows (single-block tiles)
             for i in range(P["nchunks"]):
                 wi = tx * (Tc // 32) + i
-                if nb == 1:
-                    ga, gb = i + aoff, i + aoff + 1
-                    Ga = [_word(Xc, 32 * ga + 4 * k) for k in range(8)]
-                    Gb = [_word(Xc, 32 * gb + 4 * k) for k in range(8)]
-                else:
-                    gi = ty * Tr + np.arange(128)
-                    ok = (gi < n) & (wi < nw)
-                    cw = np.where(ok, cur_words[np.minimum(gi, n - 1), min(wi, nw - 1)], np.uint64(0))
+                gi = ty * Tr + np.arange(128)
+                ok = (gi < n) & (wi < nw)
+                cw = np.where(ok, cur_words[np.minimum(gi, n - 1), min(wi, nw - 1)], np.uint64(0))
                 Cc = C[:, 32 * i: 32 * i + 32].astype(np.uint64)
                 # tcgen05.ld .pack::16b: register r = column 2r (low 16) | column 2r+1 (high 16)
                 v = [(Cc[:, 2 * r] & np.uint64(0xFFFF)) | ((Cc[:, 2 * r + 1] & np.uint64(0xFFFF)) << np.uint64(16))
@@ -153,16 +134,13 @@ def tensor_step(grid, R, rule):
                 if not P["lanes16"]:
                     for k in range(8):
                         B4 = prmt(v[2 * k], v[2 * k + 1], 0x6420)
-                        s4 = prmt(Ga[k], Gb[k], 0x5432) if nb == 1 else (cw >> np.uint64(k)) & np.uint64(0x01010101)
+                        s4 = (cw >> np.uint64(k)) & np.uint64(0x01010101)
                         ge = (B4 + nlo0 + s4 * dlo) & M32
                         le = (hiH0 + s4 * dhi - B4) & M32
                         acc |= (ge & le & np.uint64(0x80808080)) >> np.uint64(7 - k)
                 else:
                     for r in range(16):
-                        h = r >> 3
-                        sel = (2 + h) | 0x80 | ((4 + h) << 8) | 0x8000
-                        s2 = prmt(Ga[r & 7], Gb[r & 7], sel) if nb == 1 else \
-                            (cw >> np.uint64(r)) & np.uint64(0x00010001)
+                        s2 = (cw >> np.uint64(r)) & np.uint64(0x00010001)
                         ge = (v[r] + nlo0 + s2 * dlo) & M32
                         le = (hiH0 + s2 * dhi - v[r]) & M32
                         acc |= (ge & le & np.uint64(0x80008000)) >> np.uint64(15 - r)
@@ -188,8 +166,8 @@ CASES = [
     (33, 5, O.BOSCO_R5, 0.5, 10, 2),
     (20, 4, O.sweep_rule(4), 0.5, 11, 2),
     (300, 40, O.scaled_rule(40), 0.45, 12, 1),   # two row blocks
-    (300, 64, O.scaled_rule(64), 0.45, 13, 1),   # two row blocks, 3-atom tile
-    (250, 90, O.scaled_rule(90), 0.45, 14, 1),   # three row blocks, 4-atom tile
+    (300, 64, O.scaled_rule(64), 0.45, 13, 1),   # two row blocks, 9 K steps
+    (250, 90, O.scaled_rule(90), 0.45, 14, 1),   # three row blocks, 11 K steps
     (96, 33, O.scaled_rule(33), 0.45, 15, 1),
 ]
 
