@@ -19,16 +19,18 @@
 //     scatter between the two products (AMXSolver.cpp:321-325) disappears;
 //   - epilogue: C is the box count including the centre; the birth/survival
 //     interval rule (HostSolver.tpp:47-73, k = C - centre) runs on four 8-bit
-//     (R <= 5) or two 16-bit lanes per register, and the result bits are
-//     gathered straight into the output word.
+//     (R <= 5), two 16-bit (R <= 90) or one 32-bit lane per register, and the
+//     result bits are gathered straight into the output word.
 //
 // MMA count.  A tcgen05.mma costs the issuing warp a few tens of cycles plus a
 // round trip through the barriers per batch, whatever its N, so a tile is done
-// in few, wide MMAs: product 1 is one MMA of N = Tc per K step (8 at R <= 16),
-// product 2 one per 32 rows of K (4 per row block).  The band matrix B_h of a
-// K step is the same matrix shifted by 32 columns per step, so one Toeplitz
-// matrix W of (KS + nchunks - 1) * 32 rows serves every step: the step's B
-// descriptor starts 32 rows further up.
+// in few, wide MMAs: product 1 is one MMA of N = Tc per K step (5 at R <= 16),
+// product 2 one per 32 bytes of K (4 per row block with u8 row sums, 8 with
+// f16).  The band matrix B_h of a K step is the same matrix shifted by 32
+// columns per step, so one Toeplitz matrix W of (KS + nchunks - 1) * 32 rows
+// serves every step: the step's B descriptor starts 32 rows further up.  B_v
+// is Toeplitz too and is stored the same way (G), which keeps it small enough
+// for the f16 operands of R = 128.
 //
 // Column order.  A packed word w spreads to bytes with (w >> k) & 0x01010101,
 // k = 0..7: register k holds cells k, 8+k, 16+k, 24+k.  The shared-memory tile
@@ -39,7 +41,19 @@
 // bits land in the output word's own bit order with one shift per register
 // (sigma below).  No byte is moved to undo the permutation.
 //
-// Exactness: inputs are 0/1, H <= 2R+1 <= 181 fits u8, C <= (2R+1)^2 in s32.
+// Operand precision per radius (the exactness bound decides, not a tolerance):
+// inputs are 0/1 and product 1 runs in kind::i8 (u8 x u8 -> s32).  The row
+// sums H <= 2R+1 go back to the tensor core for product 2 as
+//   u8   while 2R+1 <= 255 (R <= 127): kind::i8 again, C in s32;
+//   f16  above (R = 128, H up to 257): kind::f16 with f32 accumulation.  H is
+//        stored as the f16 of H + 1024, whose bit pattern is 0x6400 + H for
+//        0 <= H <= 1024 (one integer add per two values), so C arrives as the
+//        f32 of C + 1024 (2R+1) -- every row of B_v holds 2R+1 ones -- exact
+//        while that stays below 2^24.  The rule compares raw f32 bit
+//        patterns, which order non-negative floats like their values, against
+//        thresholds shifted by the same constant.
+// Box counts (2R+1)^2 decide the rule lanes: 8 bits while <= 127, 16 bits while
+// < 2^15 (R <= 90), 32 bits above.
 //
 // Every wait on an mbarrier is bounded (globaltimer); on timeout the kernel
 // sets a bit in an error word that the host reads (ltl_synchronize), waits
@@ -116,11 +130,29 @@ enum Bar {
     NBARS = DRAIN + 2
 };
 
+// Rule lanes and product-2 operand type (the template parameter MODE):
+enum TcMode {
+    kLanes8 = 0,   // four 8-bit rule lanes per register, H as u8
+    kLanes16 = 1,  // two 16-bit rule lanes, H as u8
+    kLanes32 = 2,  // one 32-bit rule lane (s32 box counts), H as u8
+    kF16 = 3       // one 32-bit rule lane on f32 bit patterns, H as f16 (kind::f16)
+};
+__host__ __device__ constexpr int h_bytes(int mode) { return mode == kF16 ? 2 : 1; }
+// K rows of one product-2 MMA (32 bytes of K either way)
+__host__ __device__ constexpr int k2_rows(int mode) { return mode == kF16 ? 16 : 32; }
+// f16 row sums are stored as H + kF16Offset (see the header)
+constexpr int kF16Offset = 1024;
+
 // W: (ng + kChunks - 1) * 32 rows (the N index) x 32 bytes (the K index of one step)
 __host__ __device__ constexpr int w_rows(int ng) { return 32 * (ng + kChunks - 1); }
 __host__ __device__ constexpr int atoms_for(int ng) { return (ng + 3) / 4; }
+// G, the Toeplitz store of B_v: 128 + k2 (T - 1) rows x 32 bytes, T = 128 nb / k2
+// product-2 K steps per tile; step t reads rows k2 (T - 1 - t) .. + 127.
+__host__ __device__ constexpr int g_rows(int nb, int mode) {
+    return 128 + k2_rows(mode) * (128 * nb / k2_rows(mode) - 1);
+}
 
-__host__ __device__ inline SmemLayout smem_layout(int stages, int ng, int nb, bool fast) {
+__host__ __device__ inline SmemLayout smem_layout(int stages, int ng, int nb, bool fast, int mode) {
     SmemLayout L{};
     int o = 0;
     L.x_off = o;
@@ -128,11 +160,11 @@ __host__ __device__ inline SmemLayout smem_layout(int stages, int ng, int nb, bo
     L.wr_off = o;
     o += fast ? kWordDepth * (ng + 1) * 128 * 4 : 0;  // packed words of the next units
     L.hs_off = o;
-    o += 2 * 128 * kTc;                        // H as u8, MN-major, two buffers
+    o += 2 * 128 * kTc * h_bytes(mode);        // H (u8 or f16), MN-major, two buffers
     L.w_off = o;
     o += 32 * w_rows(ng);                      // W
     L.bv_off = o;
-    o += 128 * 128 * nb;                       // B_v, 128 x (128 nb)
+    o += 32 * g_rows(nb, mode);                // G (B_v)
     o = (o + 7) & ~7;
     L.bar_off = o;
     o += NBARS * 8;
@@ -145,8 +177,8 @@ __host__ __device__ inline SmemLayout smem_layout(int stages, int ng, int nb, bo
 // Column permutation inside a 32-column group: byte position q holds cell pi(q).
 __host__ __device__ constexpr int perm_pi(int q) { return 8 * (q & 3) + (q >> 2); }
 // Output cell (within a 32-column chunk) of accumulator column n.
-__host__ __device__ constexpr int perm_sigma(int n, int lanes16) {
-    return lanes16 ? 16 * (n & 1) + (n >> 1) : perm_pi(n);
+__host__ __device__ constexpr int perm_sigma(int n, int mode) {
+    return mode == kLanes8 ? perm_pi(n) : mode == kLanes16 ? 16 * (n & 1) + (n >> 1) : n;
 }
 
 __device__ __forceinline__ int wrap_slow(int v, int n) {
@@ -228,16 +260,19 @@ struct Cursor {
 // applies the rule to unit u - 1, the tensor core has the next unit's product 1
 // queued while the epilogue finishes the previous one.
 //
-// LANES16: rule lanes (four 8-bit, or two 16-bit); FAST: n % 32 == 0 and
+// MODE: rule lanes and product-2 operand type (TcMode); FAST: n % 32 == 0 and
 // large enough that rows and words wrap with one correction; NG: product-1 K
 // steps = X groups of 32 columns per row.
-template <bool LANES16, bool FAST, int NG>
+template <int MODE, bool FAST, int NG>
 __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_constant__ TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     constexpr int ATOMS = atoms_for(NG);
+    constexpr int HB = h_bytes(MODE);   // bytes per H value in shared memory
+    constexpr int K2 = k2_rows(MODE);   // K rows per product-2 MMA
+    constexpr int S2 = 128 / K2;        // product-2 MMAs per row block
     const int nb = p.nb, S = p.stages, R = p.R;
-    const SmemLayout L = smem_layout(S, NG, nb, FAST);
+    const SmemLayout L = smem_layout(S, NG, nb, FAST, MODE);
     uint8_t* xs = smem + L.x_off;
     uint8_t* hs = smem + L.hs_off;
     uint8_t* wm = smem + L.w_off;
@@ -277,24 +312,40 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
     for (int idx = tid; idx < w_rows(NG) * 32; idx += kThreads) {
         const int m = idx >> 5, k = idx & 31;
         const int D = NG - 1 - (m >> 5);
-        const int d = 32 * D + perm_pi(k) - p.PADC - perm_sigma(m & 31, LANES16);
+        const int d = 32 * D + perm_pi(k) - p.PADC - perm_sigma(m & 31, MODE);
         wm[((m >> 3) * 2 + (k >> 4)) * 128 + (m & 7) * 16 + (k & 15)] = (d >= -R && d <= R) ? 1 : 0;
     }
-    // B_v[m][k] = [m <= k <= m + 2R], m < 128, k < 128 nb (K-major, no swizzle, 16 bytes per store)
-    for (int idx = tid; idx < 8 * nb * 128; idx += kThreads) {
-        const int kc = idx / 128, m = idx % 128;
-        uint32_t w[4];
+    // G, the A operand of product 2 (K-major, no swizzle: [i / 8][two 16-byte
+    // halves][8][16 bytes], like W).  B_v[m][k] = [m <= k <= m + 2R] depends on
+    // k - m only, so product-2 K step t (rows K2 t .. K2 t + K2 - 1 of the
+    // tile's 128 nb X rows) is the 128-row window of G from row K2 (T2 - 1 - t):
+    // G[i][kk] = [0 <= K2 (T2 - 1) + kk - i <= 2R].  Entries are u8 1 or f16 1.0.
+    {
+        const int T2 = S2 * nb;
+        const int grows = g_rows(nb, MODE);
+        for (int idx = tid; idx < grows * 2; idx += kThreads) {
+            const int i = idx >> 1, half = idx & 1;  // row, 16-byte half of the row's 32 bytes
+            uint32_t w[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            uint32_t v = 0;
+            for (int q = 0; q < 4; ++q) {
+                uint32_t v = 0;
+                if (MODE == kF16) {
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int k = kc * 16 + 4 * q + e;
-                v |= (uint32_t)(k >= m && k <= m + 2 * R) << (8 * e);
+                    for (int e = 0; e < 2; ++e) {
+                        const int d = K2 * (T2 - 1) + (8 * half + 2 * q + e) - i;
+                        v |= (d >= 0 && d <= 2 * R) ? (0x3C00u << (16 * e)) : 0u;
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int d = K2 * (T2 - 1) + (16 * half + 4 * q + e) - i;
+                        v |= (uint32_t)(d >= 0 && d <= 2 * R) << (8 * e);
+                    }
+                }
+                w[q] = v;
             }
-            w[q] = v;
+            *(uint4*)(bv + (((i >> 3) * 2 + half) * 128 + (i & 7) * 16)) = make_uint4(w[0], w[1], w[2], w[3]);
         }
-        *(uint4*)(bv + (kc * 128 + m) * 16) = make_uint4(w[0], w[1], w[2], w[3]);
     }
     fence_proxy_async();
     fence_before();
@@ -347,9 +398,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         } else {
             // product 2 of unit c: C(j % 2) (+)= B_v[:, 128b ..] * H(u), H(u) from
             // shared-memory buffer u % 2
-            constexpr uint32_t id2 = idesc_u8(kTc, true);
-            const uint64_t bvd0 = desc_noswz(smem_u32(bv), 128 * 16, 128);
+            constexpr uint32_t id2 = MODE == kF16 ? idesc_f16(kTc, true) : idesc_u8(kTc, true);
+            const uint64_t gd0 = desc_noswz(smem_u32(bv), 128, 256);
             const uint64_t hsd0 = desc_noswz(smem_u32(hs), 128, 128 * 16);
+            const int T2 = S2 * nb;
             for (; c.u < units && ok; c.next(wk)) {
                 const int hb = c.u & 1, cb = c.j & 1;
                 ok = wait(&bars[HS_FULL + hb], (uint32_t)((c.u >> 1) & 1));
@@ -357,12 +409,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                 if (!ok) break;
                 fence_after();
                 if (leader) {
-                    const uint64_t hd = hsd0 + (uint64_t)((hb * 128 * kTc) >> 4);
-                    const uint64_t vd = bvd0 + (uint64_t)((c.b * 8 * 128 * 16) >> 4);
+                    const uint64_t hd = hsd0 + (uint64_t)((hb * 128 * kTc * HB) >> 4);
+                    // K step t = S2 b + s starts at G row K2 (T2 - 1 - t): 32 K2 bytes per K2 rows
+                    const uint64_t gd = gd0 + (uint64_t)(2 * K2 * (T2 - 1 - S2 * c.b));
 #pragma unroll
-                    for (int s = 0; s < 4; ++s)
-                        mma_i8(tmem + c_col(cb), vd + (uint64_t)((s * 2 * 128 * 16) >> 4),
-                               hd + (uint64_t)((s * 32 * 16) >> 4), id2, (c.b > 0 || s > 0) ? 1u : 0u);
+                    for (int s = 0; s < S2; ++s) {
+                        const uint64_t ad = gd - (uint64_t)(2 * K2 * s);
+                        const uint64_t bd = hd + (uint64_t)((s * K2 * 16) >> 4);
+                        const uint32_t acc = (c.b > 0 || s > 0) ? 1u : 0u;
+                        if constexpr (MODE == kF16) {
+                            mma_f16(tmem + c_col(cb), ad, bd, id2, acc);
+                        } else {
+                            mma_i8(tmem + c_col(cb), ad, bd, id2, acc);
+                        }
+                    }
                     mma_commit(&bars[HS_EMPTY + hb]);
                     if (c.b == nb - 1) mma_commit(&bars[C_FULL + cb]);
                 }
@@ -504,18 +564,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                 // product 2 of unit u - 2 has read the buffer
                 if (c.u >= 2) ok = wait_all(&bars[HS_EMPTY + hb], (uint32_t)(((c.u >> 1) - 1) & 1));
                 if (!ok) break;
-                uint8_t* hsb = hs + hb * 128 * kTc + m * 16;
+                // 16 bytes of one row m per store; consecutive N groups of 16 bytes
+                // are 128 rows x 16 bytes apart
+                uint8_t* hsb = hs + hb * 128 * kTc * HB + m * 16;
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
                     const uint32_t* v = e ? vb : va;
+                    if constexpr (MODE == kF16) {
+                        // register r = columns 2r, 2r + 1 as 16-bit halves; + 0x6400 in
+                        // each half gives the f16 of H + 1024 (H <= 1024: no carry out)
 #pragma unroll
-                    for (int hh = 0; hh < 2; ++hh) {
-                        uint4 wv;
-                        wv.x = prmt(v[8 * hh + 0], v[8 * hh + 1], 0x6420u);
-                        wv.y = prmt(v[8 * hh + 2], v[8 * hh + 3], 0x6420u);
-                        wv.z = prmt(v[8 * hh + 4], v[8 * hh + 5], 0x6420u);
-                        wv.w = prmt(v[8 * hh + 6], v[8 * hh + 7], 0x6420u);
-                        *(uint4*)(hsb + (4 * h + 2 * e + hh) * 128 * 16) = wv;
+                        for (int j = 0; j < 4; ++j) {
+                            uint4 wv;
+                            wv.x = v[4 * j + 0] + 0x64006400u;
+                            wv.y = v[4 * j + 1] + 0x64006400u;
+                            wv.z = v[4 * j + 2] + 0x64006400u;
+                            wv.w = v[4 * j + 3] + 0x64006400u;
+                            *(uint4*)(hsb + (4 * (2 * h + e) + j) * 128 * 16) = wv;
+                        }
+                    } else {
+#pragma unroll
+                        for (int hh = 0; hh < 2; ++hh) {
+                            uint4 wv;
+                            wv.x = prmt(v[8 * hh + 0], v[8 * hh + 1], 0x6420u);
+                            wv.y = prmt(v[8 * hh + 2], v[8 * hh + 3], 0x6420u);
+                            wv.z = prmt(v[8 * hh + 4], v[8 * hh + 5], 0x6420u);
+                            wv.w = prmt(v[8 * hh + 6], v[8 * hh + 7], 0x6420u);
+                            *(uint4*)(hsb + (4 * h + 2 * e + hh) * 128 * 16) = wv;
+                        }
                     }
                 }
                 fence_proxy_async();
@@ -543,33 +619,54 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                 ok = wait_all(&bars[C_FULL + cb], (uint32_t)((j >> 1) & 1));
                 if (!ok) break;
                 fence_after();
-                uint32_t v[16];
-                tmem_ld32p(tmem + lane_off + c_col(cb), v);
-                tmem_wait16(v);
-                fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&bars[C_EMPTY + cb]);
                 uint32_t acc = 0u;
-                if (!LANES16) {
-                    // accumulator column 4k+j = output cell 8j+k: four box counts per
-                    // register, bit 7 of each byte lane = the rule's result
+                if constexpr (MODE >= kLanes32) {
+                    // accumulator column n = output cell n, one box count (s32, or
+                    // the f32 bits of the count plus a constant) per register, bit
+                    // 31 = the rule's result
+                    uint32_t v0[16], v1[16];
+                    tmem_ld16(tmem + lane_off + c_col(cb), v0);
+                    tmem_ld16(tmem + lane_off + c_col(cb) + 16, v1);
+                    tmem_wait_2x16(v0, v1);
+                    fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&bars[C_EMPTY + cb]);
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const uint32_t B4 = prmt(v[2 * k], v[2 * k + 1], 0x6420u);
-                        const uint32_t s4 = (cw >> k) & 0x01010101u;
-                        const uint32_t ge = (B4 + nlo0) + s4 * dlo;  // bit 7: B >= lo(s)
-                        const uint32_t le = (hiH0 + s4 * dhi) - B4;  // bit 7: B <= hi(s)
-                        acc |= (ge & le & 0x80808080u) >> (7 - k);
+                    for (int k = 0; k < 32; ++k) {
+                        const uint32_t B = k < 16 ? v0[k] : v1[k - 16];
+                        const uint32_t s1 = (cw >> k) & 1u;
+                        const uint32_t ge = (B + nlo0) + s1 * dlo;
+                        const uint32_t le = (hiH0 + s1 * dhi) - B;
+                        acc |= ((ge & le) >> 31) << k;
                     }
                 } else {
-                    // accumulator column 2r+e = output cell 16e+r: two box counts per
-                    // register, bit 15 of each 16-bit lane = the rule's result
+                    uint32_t v[16];
+                    tmem_ld32p(tmem + lane_off + c_col(cb), v);
+                    tmem_wait16(v);
+                    fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&bars[C_EMPTY + cb]);
+                    if constexpr (MODE == kLanes8) {
+                        // accumulator column 4k+j = output cell 8j+k: four box counts per
+                        // register, bit 7 of each byte lane = the rule's result
 #pragma unroll
-                    for (int k = 0; k < 16; ++k) {
-                        const uint32_t s2 = (cw >> k) & 0x00010001u;
-                        const uint32_t ge = (v[k] + nlo0) + s2 * dlo;
-                        const uint32_t le = (hiH0 + s2 * dhi) - v[k];
-                        acc |= (ge & le & 0x80008000u) >> (15 - k);
+                        for (int k = 0; k < 8; ++k) {
+                            const uint32_t B4 = prmt(v[2 * k], v[2 * k + 1], 0x6420u);
+                            const uint32_t s4 = (cw >> k) & 0x01010101u;
+                            const uint32_t ge = (B4 + nlo0) + s4 * dlo;  // bit 7: B >= lo(s)
+                            const uint32_t le = (hiH0 + s4 * dhi) - B4;  // bit 7: B <= hi(s)
+                            acc |= (ge & le & 0x80808080u) >> (7 - k);
+                        }
+                    } else {
+                        // accumulator column 2r+e = output cell 16e+r: two box counts per
+                        // register, bit 15 of each 16-bit lane = the rule's result
+#pragma unroll
+                        for (int k = 0; k < 16; ++k) {
+                            const uint32_t s2 = (cw >> k) & 0x00010001u;
+                            const uint32_t ge = (v[k] + nlo0) + s2 * dlo;
+                            const uint32_t le = (hiH0 + s2 * dhi) - v[k];
+                            acc |= (ge & le & 0x80008000u) >> (15 - k);
+                        }
                     }
                 }
                 if (at >= 0) p.dst[at] = acc;
@@ -599,6 +696,7 @@ struct TensorPlan {
     TcKernel kernel;
     int smem_bytes;
     int grid;
+    int operand_bits;  // product-2 operand: 8 (u8) or 16 (f16)
     unsigned int* err;
 };
 
@@ -608,24 +706,39 @@ struct TensorPlan {
 //   R 17..48     16-bit lanes, 7 K steps (row blocks from R = 33)
 //   R 49..80     16-bit lanes, 9 K steps
 //   R 81..90     16-bit lanes, 11 K steps
-template <bool L16, int NG>
+//   R 91..112    32-bit lanes, 11 K steps
+//   R 113..127   32-bit lanes, 13 K steps
+//   R 128        32-bit lanes on f32 counts, f16 product 2, 13 K steps
+template <int MODE, int NG>
 static TcKernel pick_fast(bool fast) {
-    return fast ? k_tensor_step<L16, true, NG> : k_tensor_step<L16, false, NG>;
+    return fast ? k_tensor_step<MODE, true, NG> : k_tensor_step<MODE, false, NG>;
 }
-static TcKernel pick_kernel(bool lanes16, bool fast, int ng) {
-    if (!lanes16) return ng == 5 ? pick_fast<false, 5>(fast) : nullptr;
-    switch (ng) {
-        case 5: return pick_fast<true, 5>(fast);
-        case 7: return pick_fast<true, 7>(fast);
-        case 9: return pick_fast<true, 9>(fast);
-        case 11: return pick_fast<true, 11>(fast);
+static TcKernel pick_kernel(int mode, bool fast, int ng) {
+    switch (mode) {
+        case kLanes8: return ng == 5 ? pick_fast<kLanes8, 5>(fast) : nullptr;
+        case kLanes16:
+            switch (ng) {
+                case 5: return pick_fast<kLanes16, 5>(fast);
+                case 7: return pick_fast<kLanes16, 7>(fast);
+                case 9: return pick_fast<kLanes16, 9>(fast);
+                case 11: return pick_fast<kLanes16, 11>(fast);
+                default: return nullptr;
+            }
+        case kLanes32:
+            switch (ng) {
+                case 11: return pick_fast<kLanes32, 11>(fast);
+                case 13: return pick_fast<kLanes32, 13>(fast);
+                default: return nullptr;
+            }
+        case kF16: return ng == 13 ? pick_fast<kF16, 13>(fast) : nullptr;
         default: return nullptr;
     }
 }
 
-// Largest radius of the tensor step: box counts (2R+1)^2 must fit the 16-bit
-// rule lanes (< 2^15) and row sums 2R+1 the u8 operand of product 2.
-constexpr int kTensorMaxRadius = 90;
+// Largest radius of the tensor step.  Row sums 2R+1 <= 255 travel as u8; R = 128
+// (row sums up to 257) as f16.  Above it the X tiles of three or more row blocks
+// and the f16 operands no longer fit one SM's shared memory twice over.
+constexpr int kTensorMaxRadius = 128;
 
 bool tensor_supported(int n, int radius, char* why, size_t why_len) {
     if (radius < 1 || radius > kTensorMaxRadius) {
@@ -656,6 +769,29 @@ static void lane_consts(int lo, int hi, int bits, int& nlo, int& hiH) {
     hiH = top + hi;
 }
 
+// The same for one 32-bit lane (marker bit 31).  The lane holds either the
+// box count B itself (s32) or, with `fbits`, the bit pattern of the f32 value
+// B + off; both are below 2^31 and ordered like B, so the thresholds are
+// transformed the same way.  An empty interval gives nlo = 0 (B + 0 never has
+// bit 31 set).
+static void lane_consts32(int lo, int hi, int maxB, bool fbits, int off, uint32_t& nlo, uint32_t& hiH) {
+    if (lo < 0) lo = 0;
+    if (hi > maxB) hi = maxB;
+    if (hi < lo) {
+        nlo = 0u;
+        hiH = 0x80000000u;
+        return;
+    }
+    uint32_t l = (uint32_t)lo, h = (uint32_t)hi;
+    if (fbits) {
+        const float fl = (float)(lo + off), fh = (float)(hi + off);
+        memcpy(&l, &fl, 4);
+        memcpy(&h, &fh, 4);
+    }
+    nlo = 0x80000000u - l;
+    hiH = 0x80000000u + h;
+}
+
 // Tile geometry for radius R (also restated in tests/test_tensor_tiles.py):
 //   Tc = 128 output columns per tile (H and C, two buffers each, fill the 512
 //          TMEM columns);
@@ -664,23 +800,36 @@ static void lane_consts(int lo, int hi, int bits, int& nlo, int& hiH) {
 //   nb = 1 row block for R <= 32 (Tr = 128 - 2R output rows per tile), else
 //          enough 128-row blocks for Tr = 128 rows plus 2R halo rows;
 //   ng = ceil((PADC + Tc + R) / 32) product-1 K steps reach every X column
-//          that any output column of the tile needs.
+//          that any output column of the tile needs;
+//   mode = the rule lanes and product-2 operand (TcMode);
+//   fast = the packed words of the next units staged through shared memory,
+//          where n allows it and the ring fits beside the deepest X ring.
 struct TensorGeometry {
-    int PADC, Tr, nb, ng, lanes16, stages;
+    int PADC, Tr, nb, ng, mode, stages;
+    bool fast;
 };
 
-static bool tensor_geometry(int R, bool fast, TensorGeometry& G) {
+static int tensor_mode(int R) {
+    if ((2 * R + 1) * (2 * R + 1) <= 127) return kLanes8;
+    if ((2 * R + 1) * (2 * R + 1) < (1 << 15)) return kLanes16;
+    return 2 * R + 1 <= 255 ? kLanes32 : kF16;
+}
+
+static bool tensor_geometry(int R, bool fast_ok, TensorGeometry& G) {
     G.PADC = R <= 16 ? 16 : 16 + 32 * ((R - 16 + 31) / 32);
     G.nb = R <= 32 ? 1 : (128 + 2 * R + 127) / 128;
     G.Tr = G.nb == 1 ? 128 - 2 * R : std::min(128, 128 * G.nb - 2 * R);
     G.ng = (G.PADC + kTc + R + 31) / 32;
-    G.lanes16 = (2 * R + 1) * (2 * R + 1) > 127 ? 1 : 0;
-    if (G.Tr < 1 || (2 * R + 1) * (2 * R + 1) >= (1 << 15) || 2 * R + 1 > 255) return false;
-    // the deepest X ring that fits
-    for (int st = kMaxStages; st >= 2; --st) {
-        if (smem_layout(st, G.ng, G.nb, fast).total + 1024 <= kSmemLimit) {
-            G.stages = st;
-            return true;
+    G.mode = tensor_mode(R);
+    if (G.Tr < 1 || R > kTensorMaxRadius || 2 * R + 1 + kF16Offset > 2048) return false;
+    // the deepest X ring that fits, with the word ring where possible
+    for (int f = fast_ok ? 1 : 0; f >= 0; --f) {
+        for (int st = kMaxStages; st >= 2; --st) {
+            if (smem_layout(st, G.ng, G.nb, f != 0, G.mode).total + 1024 <= kSmemLimit) {
+                G.stages = st;
+                G.fast = f != 0;
+                return true;
+            }
         }
     }
     return false;
@@ -704,18 +853,33 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
     // one correction wraps a row (rows span [-R, n + 128 nb)) and a word index
     // (words span [-4, nw + ng)); groups are word halves
     const int nb_of_r = R <= 32 ? 1 : (128 + 2 * R + 127) / 128;
-    const bool fast = a.n % 32 == 0 && nw >= 4 && a.n >= 128 * nb_of_r + R;
+    const bool fast_ok = a.n % 32 == 0 && nw >= 4 && a.n >= 128 * nb_of_r + R;
     TensorGeometry G{};
-    if (!tensor_geometry(R, fast, G)) {
+    if (!tensor_geometry(R, fast_ok, G)) {
         snprintf(why, why_len, "no tile shape for R=%d", R);
         return nullptr;
     }
+    const bool fast = G.fast;
     TensorPlan* P = new TensorPlan();
-    const int bits = G.lanes16 ? 16 : 8;
-    const uint32_t bcast = G.lanes16 ? 0x00010001u : 0x01010101u;
-    int nlo_d, hiH_d, nlo_s, hiH_s;
-    lane_consts(rule.bmin, rule.bmax, bits, nlo_d, hiH_d);
-    lane_consts(rule.smin + 1, rule.smax + 1, bits, nlo_s, hiH_s);
+    P->operand_bits = G.mode == kF16 ? 16 : 8;
+    uint32_t nlo_d, hiH_d, nlo_s, hiH_s, bcast = 1u;
+    if (G.mode >= kLanes32) {
+        const int maxB = (2 * R + 1) * (2 * R + 1);
+        const bool fb = G.mode == kF16;
+        const int off = fb ? kF16Offset * (2 * R + 1) : 0;
+        lane_consts32(rule.bmin, rule.bmax, maxB, fb, off, nlo_d, hiH_d);
+        lane_consts32(rule.smin + 1, rule.smax + 1, maxB, fb, off, nlo_s, hiH_s);
+    } else {
+        const int bits = G.mode == kLanes16 ? 16 : 8;
+        bcast = G.mode == kLanes16 ? 0x00010001u : 0x01010101u;
+        int a0, b0, a1, b1;
+        lane_consts(rule.bmin, rule.bmax, bits, a0, b0);
+        lane_consts(rule.smin + 1, rule.smax + 1, bits, a1, b1);
+        nlo_d = (uint32_t)a0;
+        hiH_d = (uint32_t)b0;
+        nlo_s = (uint32_t)a1;
+        hiH_s = (uint32_t)b1;
+    }
     const PackedFrame* src[2] = {&a, &b};
     const PackedFrame* dst[2] = {&b, &a};
     for (int i = 0; i < 2; ++i) {
@@ -732,10 +896,10 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
         q.stages = G.stages;
         q.tiles_x = (a.n + kTc - 1) / kTc;
         q.tiles_y = (a.n + G.Tr - 1) / G.Tr;
-        q.nlo0 = (uint32_t)nlo_d * bcast;
-        q.dlo = (uint32_t)(nlo_s - nlo_d);
-        q.hiH0 = (uint32_t)hiH_d * bcast;
-        q.dhi = (uint32_t)(hiH_s - hiH_d);
+        q.nlo0 = nlo_d * bcast;
+        q.dlo = nlo_s - nlo_d;
+        q.hiH0 = hiH_d * bcast;
+        q.dhi = hiH_s - hiH_d;
     }
     if (cudaMalloc(&P->err, sizeof(unsigned int)) != cudaSuccess) {
         snprintf(why, why_len, "error-flag allocation failed");
@@ -748,14 +912,14 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
         q.wait_ns = kWaitLimitNs;
         q.inject_missing_commit = 0;
     }
-    P->kernel = pick_kernel(G.lanes16 != 0, fast, G.ng);
+    P->kernel = pick_kernel(G.mode, fast, G.ng);
     if (!P->kernel) {
         snprintf(why, why_len, "no kernel instantiation for R=%d", R);
         cudaFree(P->err);
         delete P;
         return nullptr;
     }
-    P->smem_bytes = smem_layout(G.stages, G.ng, G.nb, fast).total + 1024;
+    P->smem_bytes = smem_layout(G.stages, G.ng, G.nb, fast, G.mode).total + 1024;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     P->grid = std::min(P->prm[0].tiles_x * P->prm[0].tiles_y, sms);
@@ -783,7 +947,7 @@ void tensor_plan_set_wait(TensorPlan* p, unsigned long long ns, int inject_missi
         q.inject_missing_commit = inject_missing_commit;
     }
 }
-int tensor_plan_operand_bits(const TensorPlan*) { return 8; }
+int tensor_plan_operand_bits(const TensorPlan* p) { return p ? p->operand_bits : 0; }
 unsigned int* tensor_plan_error_flag(TensorPlan* p) { return p ? p->err : nullptr; }
 
 cudaError_t launch_tensor_pass(TensorPlan* p, bool src_is_a, cudaStream_t s) {

@@ -191,5 +191,14 @@ __host__ __device__ constexpr uint32_t idesc_u8(int N, bool b_mn_major) {
            | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
+// Instruction descriptor: kind::f16, f16 x f16 -> f32, M = 128.
+__host__ __device__ constexpr uint32_t idesc_f16(int N, bool b_mn_major) {
+    return (1u << 4)                       // D format f32
+           | (0u << 7) | (0u << 10)        // A, B f16
+           | (0u << 15)                    // A K-major
+           | ((b_mn_major ? 1u : 0u) << 16)
+           | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
 }  // namespace tc
 }  // namespace ltl

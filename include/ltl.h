@@ -60,7 +60,7 @@ typedef struct {
  * GPU codes; radius and rule are run-time values instead of the RADIUS/SMIN/
  * SMAX/BMIN/BMAX macros (Makefile:10-14).  n >= radius is required (the
  * reference's torus halo is only defined there, HostSolver.tpp:93-140).
- * Radius ranges: plain 1..2038, packed 1..32, tensor 1..90; outside them
+ * Radius ranges: plain 1..2038, packed 1..32, tensor 1..128; outside them
  * LTL_EUNSUPPORTED. */
 int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin, int smax, int bmin, int bmax,
                int variant);

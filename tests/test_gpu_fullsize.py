@@ -68,7 +68,7 @@ def test_large_radius_32768(radius):
     checked against the oracle."""
     import cat_cpu_b200 as C
     rule = O.scaled_rule(radius)
-    variants = [C.VARIANT_PLAIN] + ([C.VARIANT_TENSOR] if radius <= 90 else [])
+    variants = [C.VARIANT_PLAIN] + ([C.VARIANT_TENSOR] if radius <= 128 else [])
     for seed, d, steps in ((3, 0.3, 2), (3, 0.448, 2)):
         start = C.start_grid(N, seed, d, 1)
         wants = []
