@@ -80,9 +80,10 @@ constexpr int kN1 = 32;      // one chunk = one output word
 constexpr int kUnpackWarps = 4;       // one X row per unpack thread
 constexpr int kRqWarps = 2 * 4;       // re-quantisation: two chunks per warp, four lane quarters
 constexpr int kRuleWarps = kChunks * 4;  // rule: one chunk per warp
-// warp 0: product-1 MMAs, warp 1: product-2 MMAs, 2..5: unpack,
-// 6..13: re-quantisation, 14..29: rule
-constexpr int kUnpackWarp0 = 2;
+// warp 0: product-1 MMAs, warp 1: product-2 MMAs, 2: packed-word loads,
+// 3..6: unpack, 7..14: re-quantisation, 15..30: rule
+constexpr int kLoadWarp = 2;
+constexpr int kUnpackWarp0 = 3;
 constexpr int kRqWarp0 = kUnpackWarp0 + kUnpackWarps;
 constexpr int kRuleWarp0 = kRqWarp0 + kRqWarps;
 constexpr int kThreads = 32 * (kRuleWarp0 + kRuleWarps);
@@ -127,7 +128,9 @@ enum Bar {
     C_FULL = HS_EMPTY + 2,    // [2] per C buffer
     C_EMPTY = C_FULL + 2,     // [2]
     DRAIN = C_EMPTY + 2,      // [2] per MMA-issuing warp
-    NBARS = DRAIN + 2
+    W_FULL = DRAIN + 2,       // [kWordDepth] packed-word ring slots
+    W_EMPTY = W_FULL + kWordDepth,
+    NBARS = W_EMPTY + kWordDepth
 };
 
 // Rule lanes and product-2 operand type (the template parameter MODE):
@@ -301,6 +304,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             mbar_init(&bars[C_EMPTY + i], kRuleWarps);
             mbar_init(&bars[DRAIN + i], 1);
         }
+        for (int i = 0; i < kWordDepth; ++i) {
+            mbar_init(&bars[W_FULL + i], 32);  // one cp.async-tracking arrival per loader lane
+            mbar_init(&bars[W_EMPTY + i], kUnpackWarps);
+        }
         fence_mbar_init();
     }
     if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
@@ -353,7 +360,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
     fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp < kUnpackWarp0) {
+    if (warp < kLoadWarp) {
         // --------------------------- MMA issuers ----------------------------
         // Warp 0 issues product 1 of every unit, warp 1 product 2, so that the
         // tensor core queue gets the next unit's product 1 while product 2 waits
@@ -434,6 +441,53 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         if (leader) mma_commit(&bars[DRAIN + warp]);
         __syncwarp();
         if (!__all_sync(0xffffffffu, mbar_wait(&bars[DRAIN + warp], 0u, p.wait_ns)) && leader) atomicOr(p.err, 32u);
+    } else if (warp == kLoadWarp) {
+        // --------------------------- packed words ---------------------------
+        // FAST tiles: the NG + 1 packed words of every X row of a unit (group g =
+        // upper half of word g, lower half of word g + 1) go by cp.async into a
+        // ring of kWordDepth units, lane l loading rows l, l + 32, l + 64, l + 96.
+        // The ring slot's barrier tracks the copies themselves
+        // (cp.async.mbarrier.arrive), so the unpack warps, whose proxy fences wait
+        // for every memory access of their own still in flight, never have a
+        // global load outstanding.
+        if (FAST) {
+            constexpr int NW1 = NG + 1;
+            uint32_t* ring = (uint32_t*)(smem + L.wr_off);  // [kWordDepth][NW1][128]
+            const Walk wk(p);
+            Cursor c;
+            c.init(wk);
+            bool ok = true;
+            for (; c.u < units; c.next(wk)) {
+                const int slot = c.u & (kWordDepth - 1);
+                if (c.u >= kWordDepth) {
+                    ok = __all_sync(0xffffffffu, mbar_wait(&bars[W_EMPTY + slot],
+                                                           (uint32_t)(((c.u / kWordDepth) - 1) & 1), p.wait_ns,
+                                                           kSleepNs));
+                    if (!ok) break;
+                }
+                uint32_t* d = ring + slot * NW1 * 128;
+                int wi0 = (c.tx * kTc - p.PADC - 16) >> 5;  // word holding X column 0
+                if (wi0 < 0) wi0 += p.nw;
+                const int gr0 = c.ty * p.Tr - R + 128 * c.b;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int row = lane + 32 * i;
+                    int gr = gr0 + row;
+                    if (gr < 0) gr += p.n;
+                    else if (gr >= p.n) gr -= p.n;
+                    const uint32_t* rp = p.src + (size_t)gr * (size_t)p.wpitch;
+                    int wi = wi0;
+#pragma unroll
+                    for (int k = 0; k < NW1; ++k) {
+                        cp_async4(d + k * 128 + row, rp + wi);
+                        if (++wi == p.nw) wi = 0;
+                    }
+                }
+                cp_async_mbar_arrive(&bars[W_FULL + slot]);
+            }
+            cp_async_wait<0>();
+            if (!ok && lane == 0) atomicOr(p.err, 64u);
+        }
     } else if (warp < kRqWarp0) {
         // ------------------------------ unpack ------------------------------
         // Thread `row` (0..127) fills X row `row` of every stage: NG groups of 32
@@ -441,9 +495,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         const int row = tid - 32 * kUnpackWarp0;
         const int sw = row & 7;
         const Walk wk(p);
-        Cursor c, cn;  // the unit being stored and the one being fetched
+        Cursor c;  // the unit being stored
         c.init(wk);
-        cn.init(wk);
         bool ok = true;
         // spreads X row `row` of unit c to the stage: group g from x_of(g)
         auto store = [&](const Cursor& cc, auto x_of) -> bool {
@@ -470,45 +523,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             return true;
         };
         if (FAST) {
-            // The NG + 1 packed words that hold X row `row` of a unit (group g =
-            // upper half of word g, lower half of word g + 1) travel by cp.async
-            // into a ring of kWordDepth units, so that several units' loads are in
-            // flight while this thread unpacks.
+            // words from the loader warp's ring (see above)
             constexpr int NW1 = NG + 1;
-            uint32_t* ring = (uint32_t*)(smem + L.wr_off) + row;  // [kWordDepth][NW1][128]
-            auto fetch = [&](const Cursor& cc) {
-                int gr = cc.ty * p.Tr - R + 128 * cc.b + row;
-                if (gr < 0) gr += p.n;
-                else if (gr >= p.n) gr -= p.n;
-                const uint32_t* rp = p.src + (size_t)gr * (size_t)p.wpitch;
-                int wi = (cc.tx * kTc - p.PADC - 16) >> 5;  // word holding X column 0
-                if (wi < 0) wi += p.nw;
-                uint32_t* d = ring + (cc.u & (kWordDepth - 1)) * NW1 * 128;
-#pragma unroll
-                for (int k = 0; k < NW1; ++k) {
-                    cp_async4(d + k * 128, rp + wi);
-                    if (++wi == p.nw) wi = 0;
-                }
-            };
-#pragma unroll
-            for (int d = 0; d < kWordDepth - 1; ++d) {
-                if (cn.u < units) fetch(cn);
-                cp_async_commit();
-                cn.next(wk);
-            }
+            const uint32_t* ring = (const uint32_t*)(smem + L.wr_off) + row;  // [kWordDepth][NW1][128]
             for (; c.u < units; c.next(wk)) {
-                if (cn.u < units) fetch(cn);
-                cp_async_commit();
-                cn.next(wk);
-                cp_async_wait<kWordDepth - 1>();  // unit c's words have landed
-                const uint32_t* d = ring + (c.u & (kWordDepth - 1)) * NW1 * 128;
+                const int slot = c.u & (kWordDepth - 1);
+                ok = __all_sync(0xffffffffu, mbar_wait(&bars[W_FULL + slot], (uint32_t)((c.u / kWordDepth) & 1),
+                                                       p.wait_ns, kSleepNs));
+                if (!ok) break;
+                const uint32_t* d = ring + slot * NW1 * 128;
                 uint32_t w[NW1];
 #pragma unroll
                 for (int k = 0; k < NW1; ++k) w[k] = d[k * 128];
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bars[W_EMPTY + slot]);
                 ok = store(c, [&](int g) { return prmt(w[g], w[g + 1], 0x5432u); });
                 if (!ok) break;
             }
-            cp_async_wait<0>();
         } else {
             uint32_t w[NG];
             // the NG groups of X row `row` of unit cc, rows and columns taken modulo n
