@@ -92,38 +92,40 @@ __device__ __forceinline__ uint32_t halo_word(const uint32_t* row, int fw, int n
     return packed_halo_word(row, fw, n, nw, [&] { return halo_word_bits(row, fw, n, nw); });
 }
 
-// One thread per inner row writes the row's three column-halo words: frame word
-// 0 (cells n-32 .. n-1), the last inner word's bits past n, and frame word nw + 1
-// (the cells that follow).  For n >= 64 it reads the four inner words they come
+// The three column-halo words of one inner frame row: frame word 0 (cells
+// n-32 .. n-1), the last inner word's bits past n, and frame word nw + 1 (the
+// cells that follow).  For n >= 64 it reads the four inner words they come
 // from once (first two, last two); smaller grids take the bit-by-bit path.
+__device__ __forceinline__ void halo_cols_row(uint32_t* row, int n, int nw) {
+    if (n >= 64) {
+        const uint32_t w1 = row[1], w2 = row[2];  // inner words 0 and 1
+        const uint32_t wl = row[nw], wp = row[nw - 1];  // inner words nw - 1 and nw - 2
+        const int ib = n - 32 * (nw - 1);  // inner bits of the last word, 1..32
+        // the last inner word with its bits past n filled from the row's start
+        const uint32_t last = ib >= 32 ? wl : ((wl & ((1u << ib) - 1u)) | (w1 << ib));
+        // frame word 0: cells n-32 .. n-1 = the 32 bits that end at inner bit ib of the last word
+        const uint32_t left = ib >= 32 ? wl : __funnelshift_r(wp, wl, ib);
+        // frame word nw + 1: cells 32 nw - n .. (the row's start shifted by the bits past n)
+        const int c = 32 * nw - n;
+        const uint32_t right = c ? __funnelshift_r(w1, w2, c) : w1;
+        row[0] = left;
+        row[nw] = last;
+        row[nw + 1] = right;
+    } else {
+        for (int k = 0; k < 3; ++k) {
+            const int fw = k == 0 ? 0 : nw + (k - 1);
+            row[fw] = halo_word(row, fw, n, nw);
+        }
+    }
+}
+
+// One thread per inner row writes the row's three column-halo words.
 __global__ void k_batch_halo_cols(uint32_t* __restrict__ arena, const BatchGrid* __restrict__ grids,
                                   const int* __restrict__ list) {
     const BatchGrid g = grids[list[blockIdx.y]];
     uint32_t* f = arena + g.off;
-    const int n = g.n, nw = g.nw;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t* row = f + (size_t)(g.HR + i) * g.wp;
-        if (n >= 64) {
-            const uint32_t w1 = row[1], w2 = row[2];  // inner words 0 and 1
-            const uint32_t wl = row[nw], wp = row[nw - 1];  // inner words nw - 1 and nw - 2
-            const int ib = n - 32 * (nw - 1);  // inner bits of the last word, 1..32
-            // the last inner word with its bits past n filled from the row's start
-            const uint32_t last = ib >= 32 ? wl : ((wl & ((1u << ib) - 1u)) | (w1 << ib));
-            // frame word 0: cells n-32 .. n-1 = the 32 bits that end at inner bit ib of the last word
-            const uint32_t left = ib >= 32 ? wl : __funnelshift_r(wp, wl, ib);
-            // frame word nw + 1: cells 32 nw - n .. (the row's start shifted by the bits past n)
-            const int c = 32 * nw - n;
-            const uint32_t right = c ? __funnelshift_r(w1, w2, c) : w1;
-            row[0] = left;
-            row[nw] = last;
-            row[nw + 1] = right;
-        } else {
-            for (int k = 0; k < 3; ++k) {
-                const int fw = k == 0 ? 0 : nw + (k - 1);
-                row[fw] = halo_word(row, fw, n, nw);
-            }
-        }
-    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x)
+        halo_cols_row(f + (size_t)(g.HR + i) * g.wp, g.n, g.nw);
 }
 
 __global__ void k_batch_halo_rows(uint32_t* __restrict__ arena, const BatchGrid* __restrict__ grids,
@@ -234,6 +236,84 @@ k_batch_resident(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, c
 }
 
 // ---------------------------------------------------------------------------
+// Persistent kernel: one launch per rule class advances every grid of the
+// class through all the generations of one ltl_batch_step.  A CTA takes whole
+// grids from a device counter, largest first, and runs a grid's generations
+// back to back with CTA barriers between them, so the grid stays in this SM's
+// L1 and the L2 for the whole run (temporal blocking of the run) and no
+// per-generation launch or halo launch is made.  Rows of fewer than 32 words
+// are handled by segments of a warp working on different row bands.
+// ---------------------------------------------------------------------------
+constexpr int kPersistWarps = 8;
+
+// Halo of one frame in global memory, by the whole CTA: the column words of
+// every inner row, then the top and bottom halo rows (copies of whole frame
+// rows, their column words included).  Plain loads: the CTA reads what it
+// wrote before the barrier.
+__device__ void frame_halo_cta(uint32_t* f, const BatchGrid& g) {
+    for (int i = threadIdx.x; i < g.n; i += blockDim.x) halo_cols_row(f + (size_t)(g.HR + i) * g.wp, g.n, g.nw);
+    __syncthreads();
+    const int total = 2 * g.HR * g.wp;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        const int band = t / g.wp, w = t % g.wp;
+        const int r = band < g.HR ? band : g.n + band;
+        const int src = g.HR + (((r - g.HR) % g.n) + g.n) % g.n;
+        f[(size_t)r * g.wp + w] = f[(size_t)src * g.wp + w];
+    }
+    __syncthreads();
+}
+
+template <int R>
+__global__ void __launch_bounds__(kPersistWarps * 32)
+k_batch_persist(uint32_t* a0, uint32_t* a1, const BatchGrid* __restrict__ grids, const int* __restrict__ order,
+                int n_order, int* next, int steps, const __grid_constant__ PackedRule pr) {
+    using Ring = PackedRing<R, kPersistWarps>;
+    extern __shared__ uint32_t ring_all[];
+    __shared__ int s_item;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t* ring_lane = ring_all + (size_t)wid * Ring::WARP_WORDS + lane;
+    while (true) {
+        if (threadIdx.x == 0) s_item = atomicAdd(next, 1);
+        __syncthreads();
+        const int li = s_item;
+        __syncthreads();  // every thread has read s_item before it is overwritten
+        if (li >= n_order) break;
+        const BatchGrid g = grids[order[li]];
+        uint32_t* f0 = a0 + g.off;
+        uint32_t* f1 = a1 + g.off;
+        frame_halo_cta(f0, g);
+        // lanes per segment: the row's words rounded up to a power of two, at most 32
+        const int seg = g.nw >= 32 ? 32 : (g.nw <= 1 ? 1 : 1 << (32 - __clz(g.nw - 1)));
+        const int ns = 32 / seg;  // segments per warp
+        const int strips = (g.nw + seg - 1) / seg;
+        // enough bands for every segment of the CTA, none shorter than 2 (2R + 1)
+        // rows (a band first counts 2R + 1 rows to start its window)
+        const int want = max(1, kPersistWarps * ns / strips);
+        const int band_rows = min(g.n, max((g.n + want - 1) / want, 4 * R + 2));
+        const int bands = (g.n + band_rows - 1) / band_rows;
+        const int items = strips * bands;
+        const int wl = lane & (seg - 1), sidx = lane / seg;
+        for (int s = 0; s < steps; ++s) {
+            const uint32_t* src = (s & 1) ? f1 : f0;
+            uint32_t* dst = (s & 1) ? f0 : f1;
+            for (int base = wid * ns; base < items; base += kPersistWarps * ns) {  // warp-uniform
+                const int item = base + sidx;
+                const bool valid = item < items;
+                const int strip = valid ? item % strips : 0;
+                const int band = valid ? item / strips : 0;
+                const int r0 = band * band_rows, r1 = min(r0 + band_rows, g.n);
+                const int w = strip * seg + wl;
+                const bool active = valid && w < g.nw;
+                packed_band_seg<R, Ring::fits>(src, dst, (size_t)g.wp, g.HR, r0, r1, band_rows, 1 + w, active,
+                                               wl == 0, wl == seg - 1 || w == g.nw - 1, ring_lane, pr);
+            }
+            __syncthreads();
+            frame_halo_cta(dst, g);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Dense staging <-> arena (all grids of a list, or one grid)
 // ---------------------------------------------------------------------------
 __global__ void k_batch_pack(const uint8_t* __restrict__ cells, uint32_t* __restrict__ arena,
@@ -300,6 +380,29 @@ static cudaError_t launch_batch_resident_r(const uint32_t* src, uint32_t* dst, c
     return cudaGetLastError();
 }
 
+template <int R>
+static cudaError_t launch_batch_persist_r(uint32_t* a0, uint32_t* a1, const BatchGrid* grids, const int* order,
+                                          int n_order, int* next, int steps, const PackedRule& pr, int ctas,
+                                          cudaStream_t s) {
+    using Ring = PackedRing<R, kPersistWarps>;
+    const int smem = Ring::fits ? Ring::BYTES : 0;
+    k_batch_persist<R><<<ctas, kPersistWarps * 32, smem, s>>>(a0, a1, grids, order, n_order, next, steps, pr);
+    return cudaGetLastError();
+}
+
+// Shared-memory limit of the persistent kernel (its h rings), set outside any
+// stream capture; returns the CTAs one SM holds.
+template <int R>
+static cudaError_t prepare_persist_r(int* per_sm) {
+    using Ring = PackedRing<R, kPersistWarps>;
+    const int smem = Ring::fits ? Ring::BYTES : 0;
+    // always raised: the kernel's own static shared memory counts against the
+    // default 48 KiB too
+    cudaError_t e = cudaFuncSetAttribute(k_batch_persist<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_persist<R>, kPersistWarps * 32, smem);
+}
+
 #define LTL_BATCH_RADII(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
 
 static cudaError_t batch_step_dispatch(int R, const uint32_t* cur, uint32_t* nxt, const BatchGrid* grids,
@@ -350,6 +453,28 @@ static cudaError_t batch_prepare_dispatch(int R, size_t smem) {
     }
 }
 
+static cudaError_t batch_persist_dispatch(int R, uint32_t* a0, uint32_t* a1, const BatchGrid* grids,
+                                          const int* order, int n_order, int* next, int steps, const PackedRule& pr,
+                                          int ctas, cudaStream_t s) {
+    switch (R) {
+#define LTL_C(r) \
+    case r: return launch_batch_persist_r<r>(a0, a1, grids, order, n_order, next, steps, pr, ctas, s);
+        LTL_BATCH_RADII(LTL_C)
+#undef LTL_C
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+static cudaError_t batch_persist_prepare_dispatch(int R, int* per_sm) {
+    switch (R) {
+#define LTL_C(r) \
+    case r: return prepare_persist_r<r>(per_sm);
+        LTL_BATCH_RADII(LTL_C)
+#undef LTL_C
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 static size_t res_smem_dispatch(int R, int n) {
     switch (R) {
 #define LTL_C(r) \
@@ -369,6 +494,9 @@ struct BatchClass {
     PackedRule pr;
     std::vector<int> resident;   // grid ids kept in shared memory
     std::vector<int> streamed;   // grid ids streamed per step
+    std::vector<int> order;      // persistent mode: every grid id of the class, largest first
+    int* d_order = nullptr;
+    int persist_ctas = 0;
     int* d_resident = nullptr;
     int4* d_items = nullptr;
     int n_items = 0;
@@ -393,8 +521,14 @@ struct ltl_batch {
     long long total_cells = 0;
     bool cur_is_a = true;
     bool no_graph = false;
+    bool persistent = true;
+    int* d_next = nullptr;  // persistent mode: one grid counter per class
     cudaStream_t own = nullptr, stream = nullptr, aux = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
+    // persistent mode: the class launches run concurrently on these streams
+    static constexpr int kLanes = 4;
+    cudaStream_t lanes[kLanes] = {};
+    cudaEvent_t lane_join[kLanes] = {};
     // graph cache: (steps, parity) -> exec
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
 };
@@ -406,6 +540,12 @@ static void batch_release(ltl_batch* b) {
     for (auto& c : b->classes) {
         if (c.d_resident) cudaFree(c.d_resident);
         if (c.d_items) cudaFree(c.d_items);
+        if (c.d_order) cudaFree(c.d_order);
+    }
+    if (b->d_next) cudaFree(b->d_next);
+    for (int i = 0; i < ltl_batch::kLanes; ++i) {
+        if (b->lane_join[i]) cudaEventDestroy(b->lane_join[i]);
+        if (b->lanes[i]) cudaStreamDestroy(b->lanes[i]);
     }
     if (b->d_grids) cudaFree(b->d_grids);
     if (b->d_streamed_all) cudaFree(b->d_streamed_all);
@@ -428,6 +568,9 @@ static void batch_release(ltl_batch* b) {
         }                                                                                          \
     } while (0)
 
+static uint32_t* cur_arena(ltl_batch* b);
+static cudaError_t refresh_streamed_halo(ltl_batch* b, uint32_t* arena, cudaStream_t s);
+
 // Work plan: which grids are resident, and the streamed work lists.  Rebuilt
 // when a shape parameter changes (the arenas' layout does not depend on it).
 static int batch_plan(ltl_batch* b) {
@@ -436,16 +579,39 @@ static int batch_plan(ltl_batch* b) {
     for (auto& c : b->classes) {
         if (c.d_resident) cudaFree(c.d_resident);
         if (c.d_items) cudaFree(c.d_items);
+        if (c.d_order) cudaFree(c.d_order);
         c.d_resident = nullptr;
         c.d_items = nullptr;
+        c.d_order = nullptr;
         c.resident.clear();
         c.streamed.clear();
+        c.order.clear();
         c.n_items = 0;
         c.res_smem = 0;
+        c.persist_ctas = 0;
     }
     if (b->d_streamed_all) cudaFree(b->d_streamed_all);
     b->d_streamed_all = nullptr;
+    b->n_streamed_all = 0;
     const int count = (int)b->grids.size();
+    if (b->persistent) {
+        // every grid of a class in one list, largest first (the CTAs take them in order)
+        for (int i = 0; i < count; ++i) b->classes[b->cls_id[i]].order.push_back(i);
+        std::map<int, int> per_sm_by_radius;
+        for (auto& c : b->classes) {
+            std::stable_sort(c.order.begin(), c.order.end(),
+                             [&](int x, int y) { return b->grids[x].n > b->grids[y].n; });
+            if (!per_sm_by_radius.count(c.rule.radius)) {
+                int per_sm = 0;
+                BATCH_CUDA(batch_persist_prepare_dispatch(c.rule.radius, &per_sm));
+                per_sm_by_radius[c.rule.radius] = std::max(per_sm, 1);
+            }
+            c.persist_ctas = std::max(1, std::min((int)c.order.size(), b->sms * per_sm_by_radius[c.rule.radius]));
+            BATCH_CUDA(cudaMalloc(&c.d_order, sizeof(int) * c.order.size()));
+            BATCH_CUDA(cudaMemcpy(c.d_order, c.order.data(), sizeof(int) * c.order.size(), cudaMemcpyHostToDevice));
+        }
+        return LTL_OK;
+    }
     std::vector<int> streamed_all;
     for (int i = 0; i < count; ++i) {
         BatchClass& c = b->classes[b->cls_id[i]];
@@ -491,6 +657,11 @@ static int batch_plan(ltl_batch* b) {
             BATCH_CUDA(cudaMemcpy(c.d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
         }
     }
+    // the streamed kernels read halos that an upload made in persistent mode left unset
+    if (b->stream && b->arena[0]) {
+        BATCH_CUDA(refresh_streamed_halo(b, cur_arena(b), b->stream));
+        BATCH_CUDA(cudaStreamSynchronize(b->stream));
+    }
     return LTL_OK;
 }
 
@@ -534,6 +705,8 @@ static int batch_build(ltl_batch* b, int flags) {
     b->stream_band_rows = (int)tuning_lookup("batch", -1, 0, "stream_band_rows", 64);
     b->resident_max = (flags & LTL_BATCH_STREAM_ALL) ? 0
                                                      : tuning_lookup("batch", -1, 0, "resident_max_bytes", kResSmemLimit);
+    b->persistent = !(flags & LTL_BATCH_STREAM_ALL) && tuning_lookup("batch", -1, 0, "persistent", 1) != 0;
+    BATCH_CUDA(cudaMalloc(&b->d_next, sizeof(int) * std::max<size_t>(b->classes.size(), 1)));
     BATCH_CUDA(cudaMalloc(&b->d_grids, sizeof(BatchGrid) * count));
     BATCH_CUDA(cudaMemcpy(b->d_grids, b->grids.data(), sizeof(BatchGrid) * count, cudaMemcpyHostToDevice));
     for (auto& a : b->arena) {
@@ -557,6 +730,12 @@ extern "C" int ltl_batch_set_param(ltl_batch* b, const char* name, long long val
             return LTL_EINVAL;
         }
         b->stream_band_rows = (int)value;
+    } else if (std::strcmp(name, "persistent") == 0) {
+        if (value != 0 && value != 1) {
+            ltl_set_error("ltl_batch_set_param: persistent must be 0 or 1");
+            return LTL_EINVAL;
+        }
+        b->persistent = value != 0;
     } else if (std::strcmp(name, "resident_max_bytes") == 0) {
         if (value < 0 || value > kResSmemLimit) {
             ltl_set_error("ltl_batch_set_param: resident_max_bytes must be in [0, %d]", kResSmemLimit);
@@ -602,6 +781,10 @@ extern "C" int ltl_batch_create(ltl_batch** out, int device, const ltl_grid_desc
     if (se == cudaSuccess) se = cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking);
     if (se == cudaSuccess) se = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (se == cudaSuccess) se = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
+    for (int i = 0; i < ltl_batch::kLanes && se == cudaSuccess; ++i) {
+        se = cudaStreamCreateWithFlags(&b->lanes[i], cudaStreamNonBlocking);
+        if (se == cudaSuccess) se = cudaEventCreateWithFlags(&b->lane_join[i], cudaEventDisableTiming);
+    }
     if (se != cudaSuccess) {
         ltl_set_error("ltl_batch_create: stream/event creation failed: %s", cudaGetErrorString(se));
         batch_release(b);
@@ -726,6 +909,36 @@ static cudaError_t enqueue_steps(ltl_batch* b, int steps, const char** what) {
     cudaError_t e = cudaSuccess;
     uint32_t* a0 = cur_arena(b);
     uint32_t* a1 = nxt_arena(b);
+    if (b->persistent) {
+        // one launch per rule class, the classes spread over kLanes forked streams
+        const int nc = (int)b->classes.size();
+        *what = "grid counter reset";
+        e = cudaMemsetAsync(b->d_next, 0, sizeof(int) * nc, b->stream);
+        if (e == cudaSuccess) {
+            *what = "fork event record";
+            e = cudaEventRecord(b->fork, b->stream);
+        }
+        const int used = std::min(nc, (int)ltl_batch::kLanes);
+        for (int i = 0; i < used && e == cudaSuccess; ++i) {
+            *what = "fork stream wait";
+            e = cudaStreamWaitEvent(b->lanes[i], b->fork, 0);
+        }
+        for (int ci = 0; ci < nc && e == cudaSuccess; ++ci) {
+            BatchClass& c = b->classes[ci];
+            *what = "persistent kernel launch";
+            e = batch_persist_dispatch(c.rule.radius, a0, a1, b->d_grids, c.d_order, (int)c.order.size(),
+                                       b->d_next + ci, steps, c.pr, c.persist_ctas, b->lanes[ci % used]);
+        }
+        for (int i = 0; i < used && e == cudaSuccess; ++i) {
+            *what = "join event record";
+            e = cudaEventRecord(b->lane_join[i], b->lanes[i]);
+            if (e == cudaSuccess) {
+                *what = "join stream wait";
+                e = cudaStreamWaitEvent(b->stream, b->lane_join[i], 0);
+            }
+        }
+        return e;
+    }
     bool any_res = false;
     for (auto& c : b->classes) any_res |= !c.resident.empty();
     if (any_res) {
@@ -831,9 +1044,10 @@ extern "C" int ltl_batch_info(const ltl_batch* b, long long* cells, long long* d
     if (cells) *cells = b->total_cells;
     if (device_bytes) *device_bytes = (long long)(2 * b->arena_words * 4 + b->total_cells);
     if (temporal_depth) {
+        // grids that run every generation of an ltl_batch_step inside one launch
         int res = 0;
-        for (auto& c : b->classes) res += (int)c.resident.size();
-        *temporal_depth = res;  // number of grids advanced in shared memory for a whole ltl_batch_step
+        for (auto& c : b->classes) res += (int)(b->persistent ? c.order.size() : c.resident.size());
+        *temporal_depth = res;
     }
     return LTL_OK;
 }

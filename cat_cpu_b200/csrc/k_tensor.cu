@@ -79,9 +79,11 @@ constexpr int kChunks = kTc / 32;
 constexpr int kN1 = 32;      // one chunk = one output word
 constexpr int kUnpackWarps = 4;       // one X row per unpack thread
 constexpr int kRqWarps = 2 * 4;       // re-quantisation: two chunks per warp, four lane quarters
-constexpr int kRuleWarps = kChunks * 4;  // rule: one chunk per warp
+constexpr int kRuleChunks = 2;        // rule: two chunks per warp, four lane quarters
+constexpr int kRuleWarps = kChunks / kRuleChunks * 4;
+static_assert(kRuleChunks == 2, "the rule role handles two chunks per warp");
 // warp 0: product-1 MMAs, warp 1: product-2 MMAs, 2: packed-word loads,
-// 3..6: unpack, 7..14: re-quantisation, 15..30: rule
+// 3..6: unpack, 7..14: re-quantisation, 15..22: rule
 constexpr int kLoadWarp = 2;
 constexpr int kUnpackWarp0 = 3;
 constexpr int kRqWarp0 = kUnpackWarp0 + kUnpackWarps;
@@ -90,9 +92,8 @@ constexpr int kThreads = 32 * (kRuleWarp0 + kRuleWarps);
 constexpr int kWordDepth = 4;  // packed-word ring of the unpack warps: units in flight
 constexpr int kSmemLimit = 227 * 1024;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any legitimate wait
-// Back-off between barrier tries of the unpack and epilogue warps: they share
-// every scheduler with the single MMA-issuing warp, whose waits are the
-// critical ones and do not sleep.
+// Back-off between barrier tries: every waiting warp shares its scheduler
+// with working ones, so none of them polls without a pause.
 constexpr uint32_t kSleepNs = 32;
 // TMEM columns: H in two buffers (units alternate), C in two buffers (tiles alternate)
 __host__ __device__ constexpr uint32_t h_col(int buf) { return 128u * (uint32_t)buf; }
@@ -371,7 +372,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         // start-address offsets in 16-byte units (within the 14-bit field).
         const bool leader = lane == 0;
         auto wait = [&](uint64_t* bar, uint32_t ph) -> bool {
-            return __all_sync(0xffffffffu, mbar_wait(bar, ph, p.wait_ns));
+            return __all_sync(0xffffffffu, mbar_wait(bar, ph, p.wait_ns, kSleepNs));
         };
         const Walk wk(p);
         Cursor c;
@@ -630,80 +631,103 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                 if (lane == 0) mbar_arrive(&bars[HS_FULL + hb]);
             }
         } else {
-            // rule: chunk grp of C(j % 2) for every tile j, bits straight into the output word
-            const int grp = (warp - kRuleWarp0) >> 2;
-            const uint32_t lane_off = ((uint32_t)(q * 32) << 16) + (uint32_t)(kN1 * grp);
+            // rule: chunks grp0 and grp0 + 1 of C(j % 2) for every tile j, bits
+            // straight into the output words
+            const int grp0 = ((warp - kRuleWarp0) >> 2) * kRuleChunks;
+            const uint32_t lane_off = ((uint32_t)(q * 32) << 16) + (uint32_t)(kN1 * grp0);
             const uint32_t nlo0 = p.nlo0, dlo = p.dlo, hiH0 = p.hiH0, dhi = p.dhi;
-            // output word of this thread in the tile of cursor c (offset, or -1)
-            auto out_at = [&](const Cursor& cc) -> long long {
+            // output word e of this thread in the tile of cursor c (offset, or -1)
+            auto out_at = [&](const Cursor& cc, int e) -> long long {
                 const int gi = cc.ty * p.Tr + m;
-                const int wi = cc.tx * kChunks + grp;
+                const int wi = cc.tx * kChunks + grp0 + e;
                 if (m >= p.Tr || gi >= p.n || wi >= p.nw) return -1;
                 return (long long)gi * p.wpitch + wi;
             };
-            // the centre word (the output word's own cells in the current grid) of
-            // the next tile is loaded while this one is processed
-            long long at = mine > 0 ? out_at(c) : -1;
-            uint32_t cw = at >= 0 ? __ldg(p.src + at) : 0u;
+            // one output word from a chunk loaded with .pack::16b (8- and 16-bit lanes)
+            auto rule16 = [&](const uint32_t (&v)[16], uint32_t cw) -> uint32_t {
+                uint32_t acc = 0u;
+                if constexpr (MODE == kLanes8) {
+                    // accumulator column 4k+j = output cell 8j+k: four box counts per
+                    // register, bit 7 of each byte lane = the rule's result
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const uint32_t B4 = prmt(v[2 * k], v[2 * k + 1], 0x6420u);
+                        const uint32_t s4 = (cw >> k) & 0x01010101u;
+                        const uint32_t ge = (B4 + nlo0) + s4 * dlo;  // bit 7: B >= lo(s)
+                        const uint32_t le = (hiH0 + s4 * dhi) - B4;  // bit 7: B <= hi(s)
+                        acc |= (ge & le & 0x80808080u) >> (7 - k);
+                    }
+                } else {
+                    // accumulator column 2r+e = output cell 16e+r: two box counts per
+                    // register, bit 15 of each 16-bit lane = the rule's result
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const uint32_t s2 = (cw >> k) & 0x00010001u;
+                        const uint32_t ge = (v[k] + nlo0) + s2 * dlo;
+                        const uint32_t le = (hiH0 + s2 * dhi) - v[k];
+                        acc |= (ge & le & 0x80008000u) >> (15 - k);
+                    }
+                }
+                return acc;
+            };
+            // one output word from a chunk of 32-bit counts: accumulator column n =
+            // output cell n, bit 31 = the rule's result (s32 counts, or the f32 bits
+            // of the count plus a constant)
+            auto rule32 = [&](const uint32_t (&v0)[16], const uint32_t (&v1)[16], uint32_t cw) -> uint32_t {
+                uint32_t acc = 0u;
+#pragma unroll
+                for (int k = 0; k < 32; ++k) {
+                    const uint32_t B = k < 16 ? v0[k] : v1[k - 16];
+                    const uint32_t s1 = (cw >> k) & 1u;
+                    const uint32_t ge = (B + nlo0) + s1 * dlo;
+                    const uint32_t le = (hiH0 + s1 * dhi) - B;
+                    acc |= ((ge & le) >> 31) << k;
+                }
+                return acc;
+            };
+            // the centre words (the output words' own cells in the current grid) of
+            // the next tile are loaded while this one is processed
+            long long at0 = mine > 0 ? out_at(c, 0) : -1, at1 = mine > 0 ? out_at(c, 1) : -1;
+            uint32_t cw0 = at0 >= 0 ? __ldg(p.src + at0) : 0u, cw1 = at1 >= 0 ? __ldg(p.src + at1) : 0u;
             for (int j = 0; j < mine && ok; ++j) {
                 const int cb = j & 1;
                 ok = wait_all(&bars[C_FULL + cb], (uint32_t)((j >> 1) & 1));
                 if (!ok) break;
                 fence_after();
-                uint32_t acc = 0u;
+                uint32_t acc0, acc1;
                 if constexpr (MODE >= kLanes32) {
-                    // accumulator column n = output cell n, one box count (s32, or
-                    // the f32 bits of the count plus a constant) per register, bit
-                    // 31 = the rule's result
+                    // 64 values do not fit the registers at once: one chunk after the
+                    // other, the C buffer released after the second chunk's loads
                     uint32_t v0[16], v1[16];
                     tmem_ld16(tmem + lane_off + c_col(cb), v0);
                     tmem_ld16(tmem + lane_off + c_col(cb) + 16, v1);
                     tmem_wait_2x16(v0, v1);
+                    acc0 = rule32(v0, v1, cw0);
+                    tmem_ld16(tmem + lane_off + c_col(cb) + kN1, v0);
+                    tmem_ld16(tmem + lane_off + c_col(cb) + kN1 + 16, v1);
+                    tmem_wait_2x16(v0, v1);
                     fence_before();
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&bars[C_EMPTY + cb]);
-#pragma unroll
-                    for (int k = 0; k < 32; ++k) {
-                        const uint32_t B = k < 16 ? v0[k] : v1[k - 16];
-                        const uint32_t s1 = (cw >> k) & 1u;
-                        const uint32_t ge = (B + nlo0) + s1 * dlo;
-                        const uint32_t le = (hiH0 + s1 * dhi) - B;
-                        acc |= ((ge & le) >> 31) << k;
-                    }
+                    acc1 = rule32(v0, v1, cw1);
                 } else {
-                    uint32_t v[16];
-                    tmem_ld32p(tmem + lane_off + c_col(cb), v);
-                    tmem_wait16(v);
+                    uint32_t va[16], vb[16];
+                    tmem_ld32p(tmem + lane_off + c_col(cb), va);
+                    tmem_ld32p(tmem + lane_off + c_col(cb) + kN1, vb);
+                    tmem_wait_2x16(va, vb);
                     fence_before();
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&bars[C_EMPTY + cb]);
-                    if constexpr (MODE == kLanes8) {
-                        // accumulator column 4k+j = output cell 8j+k: four box counts per
-                        // register, bit 7 of each byte lane = the rule's result
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) {
-                            const uint32_t B4 = prmt(v[2 * k], v[2 * k + 1], 0x6420u);
-                            const uint32_t s4 = (cw >> k) & 0x01010101u;
-                            const uint32_t ge = (B4 + nlo0) + s4 * dlo;  // bit 7: B >= lo(s)
-                            const uint32_t le = (hiH0 + s4 * dhi) - B4;  // bit 7: B <= hi(s)
-                            acc |= (ge & le & 0x80808080u) >> (7 - k);
-                        }
-                    } else {
-                        // accumulator column 2r+e = output cell 16e+r: two box counts per
-                        // register, bit 15 of each 16-bit lane = the rule's result
-#pragma unroll
-                        for (int k = 0; k < 16; ++k) {
-                            const uint32_t s2 = (cw >> k) & 0x00010001u;
-                            const uint32_t ge = (v[k] + nlo0) + s2 * dlo;
-                            const uint32_t le = (hiH0 + s2 * dhi) - v[k];
-                            acc |= (ge & le & 0x80008000u) >> (15 - k);
-                        }
-                    }
+                    acc0 = rule16(va, cw0);
+                    acc1 = rule16(vb, cw1);
                 }
-                if (at >= 0) p.dst[at] = acc;
+                if (at0 >= 0) p.dst[at0] = acc0;
+                if (at1 >= 0) p.dst[at1] = acc1;
                 for (int b = 0; b < nb; ++b) c.next(wk);
-                at = j + 1 < mine ? out_at(c) : -1;
-                cw = at >= 0 ? __ldg(p.src + at) : 0u;
+                at0 = j + 1 < mine ? out_at(c, 0) : -1;
+                at1 = j + 1 < mine ? out_at(c, 1) : -1;
+                cw0 = at0 >= 0 ? __ldg(p.src + at0) : 0u;
+                cw1 = at1 >= 0 ? __ldg(p.src + at1) : 0u;
             }
         }
         if (!ok && lane == 0) atomicOr(p.err, 8u);

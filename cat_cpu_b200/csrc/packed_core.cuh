@@ -272,6 +272,98 @@ __device__ __forceinline__ void packed_band(const uint32_t* __restrict__ cur, ui
     }
 }
 
+// Horizontal window count for the segmented band walk below: lanes work in
+// segments, and a lane at a segment's edge (edge_l / edge_r) loads its
+// neighbouring word itself instead of taking it from the next lane.  Loads go
+// through L1 without the read-only path (ld.global.ca), so words this CTA wrote
+// before a __syncthreads are seen.
+template <int R, int PH>
+__device__ __forceinline__ void hcount_seg(const uint32_t* row, int fw, bool active, bool edge_l, bool edge_r,
+                                           uint32_t (&h)[PH]) {
+    const uint32_t own = active ? __ldca(row + fw) : 0u;
+    uint32_t left = __shfl_up_sync(0xffffffffu, own, 1);
+    uint32_t right = __shfl_down_sync(0xffffffffu, own, 1);
+    if (edge_l && active) left = __ldca(row + fw - 1);
+    if (edge_r && active) right = __ldca(row + fw + 1);
+    uint32_t x[2 * R + 1];
+#pragma unroll
+    for (int d = -R; d <= R; ++d) {
+        uint32_t v;
+        if (d == 0)
+            v = own;
+        else if (d > 0)
+            v = __funnelshift_rc(own, right, d);
+        else
+            v = __funnelshift_lc(left, own, -d);
+        x[d + R] = v;
+    }
+    wallace<2 * R + 1, 0, PH>(x, h);
+}
+
+// packed_band for warps whose lanes work on different row bands: every lane
+// has its own band [r0, r1) (the same for the lanes of one segment), and the
+// whole warp runs `len` >= r1 - r0 iterations so that its shuffles stay
+// converged; a lane stops loading and writing once its band has ended.  The
+// h ring (kRing) is per lane, as in packed_band.  All lanes call it together.
+template <int R, bool kRing>
+__device__ __forceinline__ void packed_band_seg(const uint32_t* cur, uint32_t* nxt, size_t wp, int HR, int r0, int r1,
+                                                int len, int fw, bool active, bool edge_l, bool edge_r,
+                                                uint32_t* ring_lane, const PackedRule& pr) {
+    constexpr int PH = bits_for(2 * R + 1);
+    constexpr int PB = bits_for((2 * R + 1) * (2 * R + 1));
+    constexpr int RING = 2 * R + 2;
+    const uint32_t* rin = cur + (size_t)(HR + r0 - R) * wp;  // next row to count
+    const uint32_t* rs = cur + (size_t)(HR + r0) * wp + fw;  // centre row
+    uint32_t* ro = nxt + (size_t)(HR + r0) * wp + fw;        // output row
+    uint32_t B[PB];
+#pragma unroll
+    for (int i = 0; i < PB; ++i) B[i] = 0u;
+    const bool live0 = active && r0 < r1;
+#pragma unroll 1
+    for (int k = 0; k < 2 * R + 1; ++k, rin += wp) {
+        uint32_t h[PH];
+        hcount_seg<R, PH>(rin, fw, live0, edge_l, edge_r, h);
+        planes_add<PB, PH>(B, h);
+        if constexpr (kRing) {
+            uint32_t* sl = ring_lane + k * PH * 32;
+#pragma unroll
+            for (int i = 0; i < PH; ++i) sl[32 * i] = h[i];
+        }
+    }
+    int out_slot = 0;  // ring slot of row r - R; row r + R + 1 goes to the slot before it
+#pragma unroll 1
+    for (int k = 0; k < len; ++k, rs += wp, ro += wp, rin += wp) {
+        const int r = r0 + k;
+        if (active && r < r1) {
+            const uint32_t sv = __ldca(rs);
+            const uint32_t in1 = planes_in<PB>(B, pr.lo[1], pr.hi[1]) & pr.keep[1];
+            const uint32_t in0 = planes_in<PB>(B, pr.lo[0], pr.hi[0]) & pr.keep[0];
+            *ro = (sv & in1) | (~sv & in0);
+        }
+        if (k + 1 < len) {
+            const bool live = active && r + 1 < r1;
+            uint32_t h[PH];
+            const int in_slot = out_slot == 0 ? RING - 1 : out_slot - 1;
+            if constexpr (kRing) {
+                const uint32_t* sl = ring_lane + out_slot * PH * 32;
+#pragma unroll
+                for (int i = 0; i < PH; ++i) h[i] = sl[32 * i];
+            } else {
+                hcount_seg<R, PH>(rin - (size_t)(2 * R + 1) * wp, fw, live, edge_l, edge_r, h);
+            }
+            planes_sub<PB, PH>(B, h);
+            hcount_seg<R, PH>(rin, fw, live, edge_l, edge_r, h);
+            planes_add<PB, PH>(B, h);
+            if constexpr (kRing) {
+                uint32_t* sl = ring_lane + in_slot * PH * 32;
+#pragma unroll
+                for (int i = 0; i < PH; ++i) sl[32 * i] = h[i];
+            }
+            out_slot = out_slot + 1 == RING ? 0 : out_slot + 1;
+        }
+    }
+}
+
 // Halo word fw of a packed frame row with one halo word per side (inner word w
 // at frame word 1 + w): fw = 0 is the left halo (cells n-32 .. n-1), fw = nw
 // the last inner word with its bits past n rewritten (cells 0 ..), fw = nw + 1

@@ -41,8 +41,7 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
 // Bounded wait for `phase` of `bar`: false once `limit_ns` of wall time has
 // passed without the phase completing.  The clock is read once per 16 tries.
 // sleep_ns > 0 suspends the warp that long between tries, leaving the issue
-// slots of its scheduler to the warps that share it (for waiters off the
-// critical path; the MMA-issuing warp spins).
+// slots of its scheduler to the warps that share it.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint64_t limit_ns, uint32_t sleep_ns = 0) {
     if (mbar_try(bar, phase)) return true;
     const uint64_t t0 = globaltimer();

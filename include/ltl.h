@@ -151,7 +151,7 @@ typedef struct {
 typedef struct ltl_batch ltl_batch;
 
 /* ltl_batch_create flags */
-#define LTL_BATCH_STREAM_ALL 1  /* no shared-memory-resident grids: stream every grid every step */
+#define LTL_BATCH_STREAM_ALL 1  /* per-generation launches only: no persistent or shared-memory-resident grids */
 #define LTL_BATCH_NO_GRAPH 2    /* launch the step loop directly instead of replaying a CUDA graph */
 
 int ltl_batch_create(ltl_batch** out, int device, const ltl_grid_desc* descs, int count, int flags);
@@ -165,12 +165,19 @@ int ltl_batch_upload_all(ltl_batch* b, const uint8_t* cells);
 int ltl_batch_download_all(ltl_batch* b, uint8_t* cells);
 int ltl_batch_step(ltl_batch* b, int steps);
 /* Batch shape parameters (autotuned; also read from the tuning table):
+ *   "persistent"          1 (default): one persistent launch per rule class runs
+ *                         every generation of an ltl_batch_step, each CTA taking
+ *                         whole grids, largest first; 0: per-generation launches
+ *                         (the two parameters below apply)
  *   "stream_band_rows"    rows per work item of the streamed per-step kernels
  *   "resident_max_bytes"  shared-memory budget deciding which grids stay resident
  * Setting one rebuilds the work lists before the next step. */
 int ltl_batch_set_param(ltl_batch* b, const char* name, long long value);
 int ltl_batch_synchronize(ltl_batch* b);
-/* Total cells of the batch (sum of n^2) and its device bytes. */
+/* Total cells of the batch (sum of n^2) and its device bytes; temporal_depth =
+ * the number of grids that run all generations of an ltl_batch_step inside
+ * one launch (every grid in persistent mode, the shared-memory-resident ones
+ * otherwise). */
 int ltl_batch_info(const ltl_batch* b, long long* cells, long long* device_bytes, int* temporal_depth);
 
 /* Shape parameters (what cat_cpu_b200/autotune.py sweeps; the autotuned table

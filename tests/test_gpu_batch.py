@@ -66,6 +66,32 @@ def test_small_batch_every_step_vs_oracle(flags):
         done = target
 
 
+def test_batch_modes_and_switches_vs_oracle():
+    """The persistent launch (default), per-generation launches with grids kept in
+    shared memory, and per-generation launches only, each against the oracle;
+    the mode changes between calls on the same batch (the halos a mode leaves
+    must serve the next).  Includes narrow grids (one to a few words per row, so
+    that warps split into segments) and radii up to 16."""
+    import cat_cpu_b200 as C
+    cfg = [(40, 2, O.scaled_rule(2), 0.45, 21), (64, 8, O.scaled_rule(8), 0.45, 22), (100, 3, O.sweep_rule(3), 0.5, 23),
+           (33, 1, O.CONWAY, 0.35, 24), (257, 5, O.BOSCO_R5, 0.5, 25), (700, 16, O.scaled_rule(16), 0.45, 26),
+           (1100, 4, O.scaled_rule(4), 0.45, 27), (16, 12, O.scaled_rule(12), 0.45, 28), (130, 7, O.scaled_rule(7), 0.45, 29)]
+    b = C.Batch([(n, r, rule) for (n, r, rule, d, s) in cfg])
+    assert b.info()[2] == len(cfg)  # persistent: every grid runs each call in one launch
+    grids = start_grids(C, cfg)
+    b.upload_all(flat(grids))
+    plan = [({}, 3), ({"persistent": 0}, 2), ({"resident_max_bytes": 0}, 3), ({"persistent": 1}, 4),
+            ({"persistent": 0, "resident_max_bytes": 225280}, 1), ({"persistent": 1}, 5)]
+    for params, steps in plan:
+        for k, v in params.items():
+            b.set_param(k, v)
+        b.step(steps)
+        got = split(b, b.download_all())
+        for k, (n, r, rule, d, s) in enumerate(cfg):
+            grids[k] = O.run(grids[k], r, rule, steps)
+            assert np.array_equal(got[k], grids[k]), f"grid {k} n={n} r={r} after {params} + {steps} steps"
+
+
 def test_single_grid_upload_download():
     import cat_cpu_b200 as C
     cfg = [(300, 5, O.BOSCO_R5, 0.5, 1), (1200, 3, O.scaled_rule(3), 0.4, 2), (64, 8, O.scaled_rule(8), 0.45, 3)]
