@@ -526,7 +526,7 @@ struct ltl_batch {
     cudaStream_t own = nullptr, stream = nullptr, aux = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
     // persistent mode: the class launches run concurrently on these streams
-    static constexpr int kLanes = 4;
+    static constexpr int kLanes = 16;
     cudaStream_t lanes[kLanes] = {};
     cudaEvent_t lane_join[kLanes] = {};
     // graph cache: (steps, parity) -> exec
@@ -597,8 +597,15 @@ static int batch_plan(ltl_batch* b) {
     if (b->persistent) {
         // every grid of a class in one list, largest first (the CTAs take them in order)
         for (int i = 0; i < count; ++i) b->classes[b->cls_id[i]].order.push_back(i);
+        // The class launches run side by side from the start, each with a share
+        // of the GPU's CTA slots in proportion to its work (cells x a cost that
+        // grows with R), so that every class starts its largest grids at once
+        // instead of waiting for the classes launched before it.
         std::map<int, int> per_sm_by_radius;
-        for (auto& c : b->classes) {
+        std::vector<double> work(b->classes.size(), 0.0);
+        double total = 0.0;
+        for (size_t ci = 0; ci < b->classes.size(); ++ci) {
+            BatchClass& c = b->classes[ci];
             std::stable_sort(c.order.begin(), c.order.end(),
                              [&](int x, int y) { return b->grids[x].n > b->grids[y].n; });
             if (!per_sm_by_radius.count(c.rule.radius)) {
@@ -606,7 +613,14 @@ static int batch_plan(ltl_batch* b) {
                 BATCH_CUDA(batch_persist_prepare_dispatch(c.rule.radius, &per_sm));
                 per_sm_by_radius[c.rule.radius] = std::max(per_sm, 1);
             }
-            c.persist_ctas = std::max(1, std::min((int)c.order.size(), b->sms * per_sm_by_radius[c.rule.radius]));
+            for (int gi : c.order) work[ci] += (double)b->grids[gi].n * b->grids[gi].n * (4.0 + c.rule.radius);
+            total += work[ci];
+        }
+        for (size_t ci = 0; ci < b->classes.size(); ++ci) {
+            BatchClass& c = b->classes[ci];
+            const double slots = (double)b->sms * per_sm_by_radius[c.rule.radius];
+            const int share = (int)(slots * work[ci] / std::max(total, 1.0) + 0.5);
+            c.persist_ctas = std::max(1, std::min((int)c.order.size(), share));
             BATCH_CUDA(cudaMalloc(&c.d_order, sizeof(int) * c.order.size()));
             BATCH_CUDA(cudaMemcpy(c.d_order, c.order.data(), sizeof(int) * c.order.size(), cudaMemcpyHostToDevice));
         }
