@@ -337,22 +337,22 @@ def radius_sweep(C, torch, args, passes_per_variant, emit=None):
 
 
 def strips_run(C, torch, args, world, rank, local):
-    """The 16384^2 R=5 grid split into `world` row strips (one per rank, plain
-    variant), halos exchanged every args.strips generations (NCCL between ranks;
-    with one rank the strip exchanges with itself).  Strong scaling: the total
+    """The 16384^2 R=5 grid split into `world` row strips (one per rank,
+    bit-packed variant), halos exchanged every args.strips generations behind the
+    strips' own steps (NCCL between ranks; with one rank the strip exchanges with
+    itself).  Strong scaling: the total
     work is fixed.  Times `steps` generations after `warmup` with CUDA events on
     the rank's stream, max over ranks; checks the gathered grid at generation
     100 against the reference's grid."""
     from cat_cpu_b200 import strips as S
     k = args.strips
     dev = torch.device("cuda", local)
-    make = lambda rows, n: S.GpuStepper(rows, n, RADIUS, RULE, device=local)  # noqa: E731
+    make = lambda rows, n: S.GpuStepper(rows, n, RADIUS, RULE, device=local,  # noqa: E731
+                                        variant=C.VARIANT_PACKED)
     if world > 1:
         st = S.DistStrips(N, RADIUS, k, make, dev)
-        mine = [st.s]
     else:
         st = S.LocalStrips(N, RADIUS, 1, k, make, device=dev)
-        mine = st.strips
     start = C.start_grid(N, SEED, DENSITY, 1)
     try:
         st.set_state(start)
@@ -372,8 +372,7 @@ def strips_run(C, torch, args, world, rank, local):
         torch.cuda.synchronize()
         ms = max_over_ranks(a.elapsed_time(b), world)
     finally:
-        for s in mine:
-            s.st.close()
+        st.close()
     return dict(ms=ms, generations=gens, bit_exact=bit_exact, halo_rows=st.h)
 
 

@@ -31,9 +31,9 @@ static int packed_band_rows(int n, int n_wstrips, int resident_warps) {
     return std::max(16, (n + bands - 1) / bands);
 }
 
-template <int R>
+template <int R, bool FUSE>
 __global__ void __launch_bounds__(kPackedWarps * 32)
-k_packed_step(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int n, int nw, int HR, int HW,
+k_packed_step(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int rows, int nw, int HR, int HW,
               size_t wp, int n_wstrips, int n_items, int band_rows, const __grid_constant__ PackedRule pr) {
     using Ring = PackedRing<R, kPackedWarps>;
     extern __shared__ uint32_t ring_all[];
@@ -47,16 +47,23 @@ k_packed_step(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, int 
         const int ws = item % n_wstrips;
         const int band = item / n_wstrips;
         const int r0 = band * band_rows;
-        const int r1 = min(r0 + band_rows, n);
+        const int r1 = min(r0 + band_rows, rows);
         const int w = ws * 32 + lane;     // inner word
         const bool active = w <= nw;      // w == nw is the right halo word (neighbour of the last word)
         const bool outputs = w < nw;
-        packed_band<R, Ring::fits>(cur, nxt, wp, HR, r0, r1, HW + w, active, outputs, lane, ring_lane, pr);
+        packed_band<R, Ring::fits, FUSE>(cur, nxt, wp, HR, r0, r1, HW + w, active, outputs, lane, ring_lane, pr,
+                                         rows, nw);
         __syncwarp();
     }
 }
 
 bool packed_supported(int n, int radius) { return radius >= 1 && radius <= 32 && n >= radius; }
+
+// The step writes the output frame's halo itself (packed_band's kFuse) where
+// every halo word is a whole inner word: n a multiple of 32, one halo word.
+bool packed_fused_halo(const PackedFrame& f, int radius) {
+    return f.HW == 1 && f.n % 32 == 0 && f.n >= 64 && f.nrows() >= 2 * radius + 2;
+}
 
 template <int R>
 static cudaError_t launch_packed_r(const PackedFrame& c, const PackedFrame& x, const PackedRule& pr,
@@ -69,14 +76,16 @@ static cudaError_t launch_packed_r(const PackedFrame& c, const PackedFrame& x, c
     // word past its own directly, so no strip is needed for the halo alone
     const int n_wstrips = (c.nw + 31) / 32;
     const int smem = PackedRing<R, kPackedWarps>::fits ? PackedRing<R, kPackedWarps>::BYTES : 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_packed_step<R>, kPackedWarps * 32, smem);
+    const bool fuse = packed_fused_halo(x, R);
+    auto kernel = fuse ? k_packed_step<R, true> : k_packed_step<R, false>;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPackedWarps * 32, smem);
     if (per_sm < 1) per_sm = 1;
     const int band_rows =
-        band_override > 0 ? band_override : packed_band_rows(c.n, n_wstrips, sms * per_sm * kPackedWarps);
-    const int bands = (c.n + band_rows - 1) / band_rows;
+        band_override > 0 ? band_override : packed_band_rows(c.nrows(), n_wstrips, sms * per_sm * kPackedWarps);
+    const int bands = (c.nrows() + band_rows - 1) / band_rows;
     const int items = n_wstrips * bands;
     int ctas = std::min((items + kPackedWarps - 1) / kPackedWarps, sms * per_sm);
-    k_packed_step<R><<<ctas, kPackedWarps * 32, smem, s>>>(c.words, x.words, c.n, c.nw, c.HR, c.HW, c.wpitch,
+    kernel<<<ctas, kPackedWarps * 32, smem, s>>>(c.words, x.words, c.nrows(), c.nw, c.HR, c.HW, c.wpitch,
                                                            n_wstrips, items, band_rows, pr);
     return cudaGetLastError();
 }
@@ -85,7 +94,9 @@ template <int R>
 static cudaError_t prepare_packed_r() {
     const int smem = PackedRing<R, kPackedWarps>::fits ? PackedRing<R, kPackedWarps>::BYTES : 0;
     if (smem <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(k_packed_step<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(k_packed_step<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_packed_step<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 cudaError_t packed_prepare(int radius) {
@@ -126,10 +137,10 @@ __device__ __forceinline__ uint32_t packed_bit(const uint32_t* row, int HW, int 
     return (row[p >> 5] >> (p & 31)) & 1u;
 }
 
-__global__ void k_packed_halo_cols(uint32_t* __restrict__ g, int n, int nw, int HR, int HW, size_t wp) {
+__global__ void k_packed_halo_cols(uint32_t* __restrict__ g, int n, int rows, int nw, int HR, int HW, size_t wp) {
     // per inner row: words [0, HW) and [HW + nw - 1, HW + nw + HW)
     const int per_row = 2 * HW + 1;
-    const long long total = (long long)n * per_row;
+    const long long total = (long long)rows * per_row;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(t / per_row);
@@ -161,23 +172,23 @@ __global__ void k_packed_halo_cols(uint32_t* __restrict__ g, int n, int nw, int 
     }
 }
 
-__global__ void k_packed_halo_rows(uint32_t* __restrict__ g, int n, int HR, size_t wp) {
+__global__ void k_packed_halo_rows(uint32_t* __restrict__ g, int rows, int HR, size_t wp) {
     const int band = blockIdx.y;  // 0 .. 2HR-1
-    const int r = band < HR ? band : n + band;
-    const int src = HR + (((r - HR) % n) + n) % n;
+    const int r = band < HR ? band : rows + band;
+    const int src = HR + (((r - HR) % rows) + rows) % rows;
     uint32_t* d = g + (size_t)r * wp;
     const uint32_t* sp = g + (size_t)src * wp;
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < (int)wp; w += gridDim.x * blockDim.x) d[w] = sp[w];
 }
 
 cudaError_t launch_packed_halo(const PackedFrame& f, cudaStream_t s) {
-    const long long total = (long long)f.n * (2 * f.HW + 1);
+    const long long total = (long long)f.nrows() * (2 * f.HW + 1);
     int blocks = (int)std::min<long long>((total + 127) / 128, 4096);
-    k_packed_halo_cols<<<blocks, 128, 0, s>>>(f.words, f.n, f.nw, f.HR, f.HW, f.wpitch);
+    k_packed_halo_cols<<<blocks, 128, 0, s>>>(f.words, f.n, f.nrows(), f.nw, f.HR, f.HW, f.wpitch);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dim3 g2((unsigned)std::max<size_t>(1, std::min<size_t>((f.wpitch + 127) / 128, 64)), (unsigned)(2 * f.HR));
-    k_packed_halo_rows<<<g2, 128, 0, s>>>(f.words, f.n, f.HR, f.wpitch);
+    k_packed_halo_rows<<<g2, 128, 0, s>>>(f.words, f.nrows(), f.HR, f.wpitch);
     return cudaGetLastError();
 }
 
@@ -190,60 +201,80 @@ cudaError_t launch_packed_halo(const PackedFrame& f, cudaStream_t s) {
 __device__ __forceinline__ uint32_t bytes4_to_bits(uint32_t w) { return ((w & 0x01010101u) * 0x01020408u) >> 24; }
 __device__ __forceinline__ uint32_t bits4_to_bytes(uint32_t nib) { return (nib * 0x00204081u) & 0x01010101u; }
 
-__global__ void k_pack_frame(const uint8_t* __restrict__ src, int n, int H, size_t pitch, uint32_t* __restrict__ dst,
-                             int nw, int HR, int HW, size_t wp) {
-    const long long total = (long long)n * nw;
+// Inner rows [row0, row0 + nrows) of a packed frame from / to a dense byte
+// buffer whose row i (`pitch` bytes apart, `src`/`dst` = its cell (0, 0)) is
+// frame row row0 + i.  `vec`: buffer and pitch 16-byte aligned, so whole
+// 32-cell words move as two 16-byte vectors.
+__global__ void k_pack_rows(const uint8_t* __restrict__ src, size_t pitch, bool vec, int n, int nw, int HR, int HW,
+                            size_t wp, int row0, int nrows, uint32_t* __restrict__ dst) {
+    const long long total = (long long)nrows * nw;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(t / nw), w = (int)(t % nw);
-        const uint8_t* p = src + (size_t)(H + i) * pitch + H + 32 * w;  // 16-byte aligned (H, pitch)
+        const uint8_t* p = src + (size_t)i * pitch + 32 * w;
         uint32_t v = 0u;
-        if (32 * w + 32 <= n) {
+        if (vec && 32 * w + 32 <= n) {
             const uint4 a = *(const uint4*)p, b = *(const uint4*)(p + 16);
             const uint32_t q[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
             for (int k = 0; k < 8; ++k) v |= bytes4_to_bits(q[k]) << (4 * k);
         } else {
-            for (int b = 0; 32 * w + b < n; ++b) v |= (uint32_t)(p[b] & 1u) << b;
+            for (int b = 0; b < 32 && 32 * w + b < n; ++b) v |= (uint32_t)(p[b] & 1u) << b;
         }
-        dst[(size_t)(HR + i) * wp + HW + w] = v;
+        dst[(size_t)(HR + row0 + i) * wp + HW + w] = v;
     }
 }
 
-__global__ void k_unpack_frame(const uint32_t* __restrict__ src, int n, int nw, int HR, int HW, size_t wp,
-                               uint8_t* __restrict__ dst, int H, size_t pitch) {
-    const long long total = (long long)n * nw;
+__global__ void k_unpack_rows(const uint32_t* __restrict__ src, int n, int nw, int HR, int HW, size_t wp, int row0,
+                              int nrows, uint8_t* __restrict__ dst, size_t pitch, bool vec) {
+    const long long total = (long long)nrows * nw;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(t / nw), w = (int)(t % nw);
-        const uint32_t v = src[(size_t)(HR + i) * wp + HW + w];
-        uint8_t* p = dst + (size_t)(H + i) * pitch + H + 32 * w;  // 16-byte aligned (H, pitch)
-        if (32 * w + 32 <= n) {
+        const uint32_t v = src[(size_t)(HR + row0 + i) * wp + HW + w];
+        uint8_t* p = dst + (size_t)i * pitch + 32 * w;
+        if (vec && 32 * w + 32 <= n) {
             uint32_t q[8];
 #pragma unroll
             for (int k = 0; k < 8; ++k) q[k] = bits4_to_bytes((v >> (4 * k)) & 0xFu);
             *(uint4*)p = make_uint4(q[0], q[1], q[2], q[3]);
             *(uint4*)(p + 16) = make_uint4(q[4], q[5], q[6], q[7]);
         } else {
-            for (int b = 0; 32 * w + b < n; ++b) p[b] = (uint8_t)((v >> b) & 1u);
+            for (int b = 0; b < 32 && 32 * w + b < n; ++b) p[b] = (uint8_t)((v >> b) & 1u);
         }
     }
 }
 
-cudaError_t launch_pack_frame(const Frame& src, const PackedFrame& dst, cudaStream_t s) {
-    long long total = (long long)src.n * dst.nw;
-    int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
-    k_pack_frame<<<blocks, 256, 0, s>>>(src.base, src.n, src.H, src.pitch, dst.words, dst.nw, dst.HR, dst.HW,
-                                        dst.wpitch);
+static bool vec16(const void* p, size_t pitch) { return ((uintptr_t)p % 16 == 0) && (pitch % 16 == 0); }
+
+cudaError_t launch_pack_rows(const uint8_t* src, size_t pitch, const PackedFrame& dst, int row0, int nrows,
+                             cudaStream_t s) {
+    if (nrows <= 0) return cudaSuccess;
+    const long long total = (long long)nrows * dst.nw;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+    k_pack_rows<<<blocks, 256, 0, s>>>(src, pitch, vec16(src, pitch), dst.n, dst.nw, dst.HR, dst.HW, dst.wpitch,
+                                       row0, nrows, dst.words);
     return cudaGetLastError();
 }
 
+cudaError_t launch_unpack_rows(const PackedFrame& src, int row0, int nrows, uint8_t* dst, size_t pitch,
+                               cudaStream_t s) {
+    if (nrows <= 0) return cudaSuccess;
+    const long long total = (long long)nrows * src.nw;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+    k_unpack_rows<<<blocks, 256, 0, s>>>(src.words, src.n, src.nw, src.HR, src.HW, src.wpitch, row0, nrows, dst,
+                                         pitch, vec16(dst, pitch));
+    return cudaGetLastError();
+}
+
+// byte frame -> packed frame, inner cells only (halos are refilled after)
+cudaError_t launch_pack_frame(const Frame& src, const PackedFrame& dst, cudaStream_t s) {
+    return launch_pack_rows(src.base + (size_t)src.H * src.pitch + src.H, src.pitch, dst, 0, dst.nrows(), s);
+}
+
 cudaError_t launch_unpack_frame(const PackedFrame& src, const Frame& dst, cudaStream_t s) {
-    long long total = (long long)src.n * src.nw;
-    int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
-    k_unpack_frame<<<blocks, 256, 0, s>>>(src.words, src.n, src.nw, src.HR, src.HW, src.wpitch, dst.base, dst.H,
-                                          dst.pitch);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e =
+        launch_unpack_rows(src, 0, src.nrows(), dst.base + (size_t)dst.H * dst.pitch + dst.H, dst.pitch, s);
     if (e != cudaSuccess) return e;
     return launch_halo_fill(dst, s);
 }

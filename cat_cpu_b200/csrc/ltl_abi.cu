@@ -117,7 +117,7 @@ static void drop_graphs(ltl_ctx* c) {
     }
 }
 
-// rows x n torus (rows == n unless the plain-only rectangular form is asked for)
+// rows x n torus (rows == n unless a rectangular form is asked for: plain and packed)
 static int create_impl(ltl_ctx** out, int device, int rows, int n, int radius, int smin, int smax, int bmin,
                        int bmax, int variant) {
     if (!out) {
@@ -130,8 +130,8 @@ static int create_impl(ltl_ctx** out, int device, int rows, int n, int radius, i
                       rows, radius);
         return LTL_EINVAL;
     }
-    if (rows != n && variant != LTL_VARIANT_PLAIN) {
-        ltl_set_error("ltl_create_rect: rectangular grids are served by the plain variant only");
+    if (rows != n && variant != LTL_VARIANT_PLAIN && variant != LTL_VARIANT_PACKED) {
+        ltl_set_error("ltl_create_rect: rectangular grids are served by the plain and packed variants");
         return LTL_EUNSUPPORTED;
     }
     if (radius > 2047) {
@@ -227,11 +227,12 @@ static int create_impl(ltl_ctx** out, int device, int rows, int n, int radius, i
         // words itself and only needs the right halo word to exist
         PackedFrame p{};
         p.n = n;
+        p.rows = rows;
         p.nw = (n + 31) / 32;
         p.HR = variant == LTL_VARIANT_PACKED ? radius + 1 : 1;
         p.HW = 1;
         p.wpitch = round_up((size_t)p.nw + 2 * p.HW + 1, 4);  // +1: edge lanes read one word past the halo
-        size_t prow = (size_t)n + 2 * p.HR;
+        size_t prow = (size_t)rows + 2 * p.HR;
         size_t pone = round_up(prow * p.wpitch * sizeof(uint32_t), 4096);
         c->pwords_bytes = 2 * pone;
         e = cudaMalloc(&c->pwords, c->pwords_bytes);
@@ -274,6 +275,12 @@ extern "C" int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin
 extern "C" int ltl_create_rect(ltl_ctx** out, int device, int rows, int cols, int radius, int smin, int smax,
                                int bmin, int bmax) {
     return create_impl(out, device, rows, cols, radius, smin, smax, bmin, bmax, LTL_VARIANT_PLAIN);
+}
+
+extern "C" int ltl_create_rect_variant(ltl_ctx** out, int device, int rows, int cols, int radius, int smin,
+                                       int smax, int bmin, int bmax, int variant) {
+    if (variant == LTL_VARIANT_AUTO) variant = LTL_VARIANT_PLAIN;
+    return create_impl(out, device, rows, cols, radius, smin, smax, bmin, bmax, variant);
 }
 
 extern "C" int ltl_destroy(ltl_ctx* c) {
@@ -424,7 +431,11 @@ extern "C" int ltl_download_rows_device(ltl_ctx* c, int row0, int nrows, uint8_t
     if (int r = check_rows(c, "ltl_download_rows_device", row0, nrows, dev, pitch)) return r;
     if (nrows == 0) return LTL_OK;
     LTL_CUDA(cudaSetDevice(c->device));
-    if (int r = sync_from_packed(c)) return r;
+    if (c->variant != LTL_VARIANT_PLAIN) {
+        // straight from the packed frame: only the asked rows are unpacked
+        LTL_CUDA(launch_unpack_rows(cur_packed(c), row0, nrows, dev, pitch, c->stream));
+        return LTL_OK;
+    }
     Frame& f = cur_frame(c);
     LTL_CUDA(cudaMemcpy2DAsync(dev, pitch, f.inner(row0, 0), f.pitch, c->n, nrows, cudaMemcpyDeviceToDevice,
                                c->stream));
@@ -436,7 +447,13 @@ extern "C" int ltl_upload_rows_device(ltl_ctx* c, int row0, int nrows, const uin
     if (int r = check_rows(c, "ltl_upload_rows_device", row0, nrows, dev, pitch)) return r;
     if (nrows == 0) return LTL_OK;
     LTL_CUDA(cudaSetDevice(c->device));
-    if (int r = sync_from_packed(c)) return r;  // the other rows of a packed grid must survive
+    if (c->variant != LTL_VARIANT_PLAIN) {
+        // straight into the packed frame (the byte frame is staging only: every
+        // read of a packed grid unpacks it again), then its halo
+        LTL_CUDA(launch_pack_rows(dev, pitch, cur_packed(c), row0, nrows, c->stream));
+        if (c->variant == LTL_VARIANT_PACKED) LTL_CUDA(launch_packed_halo(cur_packed(c), c->stream));
+        return LTL_OK;
+    }
     Frame& f = cur_frame(c);
     LTL_CUDA(cudaMemcpy2DAsync(f.inner(row0, 0), f.pitch, dev, pitch, c->n, nrows, cudaMemcpyDeviceToDevice,
                                c->stream));
@@ -481,7 +498,8 @@ static cudaError_t enqueue_pass(ltl_ctx* c, int gens) {
             e = launch_packed_step(cur_packed(c), nxt_packed(c), c->rule, c->packed_band_rows, c->stream);
             step_kernels = 1;
             if (c->timing && e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
-            if (e == cudaSuccess) e = launch_packed_halo(nxt_packed(c), c->stream);
+            if (packed_fused_halo(nxt_packed(c), c->rule.radius)) halo_kernels = 0;
+            else if (e == cudaSuccess) e = launch_packed_halo(nxt_packed(c), c->stream);
             break;
         }
         case LTL_VARIANT_TENSOR: {

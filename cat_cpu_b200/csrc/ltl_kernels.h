@@ -61,14 +61,24 @@ struct PackedFrame {
     int HR;         // halo rows (>= R + 1)
     int HW;         // halo words on each side (1: radius <= 32)
     size_t wpitch;  // words per frame row
+    int rows = 0;   // inner rows of a rectangular torus (0: square, n rows)
+    __host__ __device__ int nrows() const { return rows ? rows : n; }
 };
 bool packed_supported(int n, int radius);
 // band_rows <= 0: built-in heuristic; > 0: rows per work item (tuning table / ltl_set_param)
 cudaError_t launch_packed_step(const PackedFrame& cur, const PackedFrame& nxt, const Rule& rule, int band_rows,
                                cudaStream_t s);
 cudaError_t launch_packed_halo(const PackedFrame& f, cudaStream_t s);
+// true when launch_packed_step also refreshes the output frame's halo
+bool packed_fused_halo(const PackedFrame& f, int radius);
 cudaError_t launch_pack_frame(const Frame& src, const PackedFrame& dst, cudaStream_t s);
 cudaError_t launch_unpack_frame(const PackedFrame& src, const Frame& dst, cudaStream_t s);
+// Inner rows [row0, row0 + nrows) of a packed frame to / from a dense byte
+// buffer (buffer row i = frame row row0 + i, `pitch` bytes apart, 0/1 cells).
+// After packing rows in, the frame's halo is stale: refresh it.
+cudaError_t launch_unpack_rows(const PackedFrame& src, int row0, int nrows, uint8_t* dst, size_t pitch, cudaStream_t s);
+cudaError_t launch_pack_rows(const uint8_t* src, size_t pitch, const PackedFrame& dst, int row0, int nrows,
+                             cudaStream_t s);
 cudaError_t launch_pack(const uint8_t* cells, size_t cell_pitch, int rows, int cols, uint64_t* words,
                         size_t word_pitch_words, cudaStream_t s);
 cudaError_t launch_unpack(const uint64_t* words, size_t word_pitch_words, int rows, int cols, uint8_t* cells,

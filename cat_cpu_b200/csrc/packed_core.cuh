@@ -214,10 +214,16 @@ struct PackedRing {
 // band (B -= h(r - R), B += h(r + R + 1)).  `cur`/`nxt` point at frame row 0,
 // `HR` halo rows, `wp` words per frame row.  ring_lane = this warp's ring + lane
 // (unused when !kRing).  All lanes of the warp must call it together.
-template <int R, bool kRing>
+// kFuse: the output frame's halo is written here too (one halo word per side,
+// n a multiple of 32 and n >= 2R + 2): every halo word and halo row is a copy of
+// an inner word or row, so the lane that computes a word also stores it where
+// the torus repeats it -- inner word nw - 1 in the left halo word, word 0 in
+// the right one, rows n - R .. n - 1 above the grid, rows 0 .. R below -- and
+// no halo pass runs between generations.
+template <int R, bool kRing, bool kFuse = false>
 __device__ __forceinline__ void packed_band(const uint32_t* __restrict__ cur, uint32_t* __restrict__ nxt, size_t wp,
                                             int HR, int r0, int r1, int fw, bool active, bool outputs, int lane,
-                                            uint32_t* ring_lane, const PackedRule& pr) {
+                                            uint32_t* ring_lane, const PackedRule& pr, int n = 0, int nw = 0) {
     constexpr int PH = bits_for(2 * R + 1);
     constexpr int PB = bits_for((2 * R + 1) * (2 * R + 1));
     constexpr int RING = 2 * R + 2;
@@ -226,6 +232,10 @@ __device__ __forceinline__ void packed_band(const uint32_t* __restrict__ cur, ui
     const uint32_t* rin = cur + (size_t)(HR + r0 - R) * wp;   // next row to count
     const uint32_t* rs = cur + (size_t)(HR + r0) * wp + fw;   // centre row
     uint32_t* ro = nxt + (size_t)(HR + r0) * wp + fw;         // output row
+    // kFuse: where this lane's word repeats in the same row (the other halo
+    // word column, or 0), and the row distance of a repeated row
+    const ptrdiff_t fdc = !kFuse ? 0 : fw - 1 == nw - 1 ? -(ptrdiff_t)nw : (fw - 1 == 0 ? (ptrdiff_t)nw : 0);
+    const ptrdiff_t fnr = (ptrdiff_t)n * (ptrdiff_t)wp;
     uint32_t B[PB];
 #pragma unroll
     for (int i = 0; i < PB; ++i) B[i] = 0u;
@@ -247,7 +257,16 @@ __device__ __forceinline__ void packed_band(const uint32_t* __restrict__ cur, ui
             const uint32_t sv = __ldg(rs);
             const uint32_t in1 = planes_in<PB>(B, pr.lo[1], pr.hi[1]) & pr.keep[1];
             const uint32_t in0 = planes_in<PB>(B, pr.lo[0], pr.hi[0]) & pr.keep[0];
-            *ro = (sv & in1) | (~sv & in0);
+            const uint32_t val = (sv & in1) | (~sv & in0);
+            *ro = val;
+            if constexpr (kFuse) {
+                if (fdc) ro[fdc] = val;
+                if (r <= R || r >= n - R) {  // a row the torus repeats above or below the grid
+                    const ptrdiff_t dr = r <= R ? fnr : -fnr;
+                    ro[dr] = val;
+                    if (fdc) ro[dr + fdc] = val;
+                }
+            }
         }
         if (r + 1 < r1) {
             uint32_t h[PH];

@@ -32,7 +32,7 @@ ABI_SYMBOLS = [
     "ltl_compare_device", "ltl_benchmark_seed", "ltl_generate_state", "ltl_pack_device", "ltl_unpack_device",
     "ltl_batch_create", "ltl_batch_destroy", "ltl_batch_set_stream", "ltl_batch_upload", "ltl_batch_download",
     "ltl_batch_upload_all", "ltl_batch_download_all", "ltl_batch_step", "ltl_batch_synchronize",
-    "ltl_batch_info", "ltl_batch_set_param", "ltl_set_param", "ltl_set_timing", "ltl_get_timing", "ltl_step_noalloc", "ltl_create_rect", "ltl_download_rows_device", "ltl_upload_rows_device",
+    "ltl_batch_info", "ltl_batch_set_param", "ltl_set_param", "ltl_set_timing", "ltl_get_timing", "ltl_step_noalloc", "ltl_create_rect", "ltl_create_rect_variant", "ltl_download_rows_device", "ltl_upload_rows_device",
     "ltl_last_error", "ltl_version",
 ]
 
@@ -102,6 +102,7 @@ def lib():
                                  ctypes.POINTER(ctypes.c_longlong)]
     L.ltl_step_noalloc.argtypes = [vp, sz, vp, sz, i, i, i, i, i, i, i, vp]
     L.ltl_create_rect.argtypes = [ctypes.POINTER(vp), i, i, i, i, i, i, i, i]
+    L.ltl_create_rect_variant.argtypes = [ctypes.POINTER(vp), i, i, i, i, i, i, i, i, i]
     L.ltl_download_rows_device.argtypes = [vp, i, i, vp, sz]
     L.ltl_upload_rows_device.argtypes = [vp, i, i, vp, sz]
     L.ltl_last_error.restype = ctypes.c_char_p
@@ -140,7 +141,7 @@ def start_grid(n, user_seed, density, threads=1):
 class CUDASolver:
     """One n x n torus on a GPU.  Method names follow CASolver (CASolver.h:7-28);
     radius and rule (reference centre-excluded convention) are run-time values.
-    rows: a rows x n torus instead (plain variant only; ltl_create_rect)."""
+    rows: a rows x n torus instead (plain or packed variant; ltl_create_rect_variant)."""
 
     def __init__(self, n, radius, rule, variant=VARIANT_AUTO, device=0, threads=1, rows=None):
         smin, smax, bmin, bmax = rule
@@ -149,8 +150,8 @@ class CUDASolver:
             check(lib().ltl_create(ctypes.byref(h), int(device), int(n), int(radius), int(smin), int(smax),
                                    int(bmin), int(bmax), int(variant)))
         else:
-            check(lib().ltl_create_rect(ctypes.byref(h), int(device), int(rows), int(n), int(radius), int(smin),
-                                        int(smax), int(bmin), int(bmax)))
+            check(lib().ltl_create_rect_variant(ctypes.byref(h), int(device), int(rows), int(n), int(radius),
+                                                int(smin), int(smax), int(bmin), int(bmax), int(variant)))
         self._h = h
         self.n, self.radius, self.rule, self.device, self.threads = n, radius, tuple(rule), device, threads
         self.rows = n if rows is None else int(rows)

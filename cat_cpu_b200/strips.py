@@ -2,17 +2,27 @@
 
 The reference steps one grid in one process; this splits an n x n torus by
 rows.  Strip p owns inner rows [a_p, b_p) (m_p rows) and is held as a torus of
-its own with m_p + 2h rows, h = R * k: h halo rows above and below.  Every k
-generations the strips exchange halos (ring neighbours on the torus):
+its own with m_p + 2h rows, h = R * k: h halo rows above and below.  Each
+generation the rows a strip cannot know (its halo edges, where its own torus
+wraps falsely) spoil R more rows from each end, so after k generations exactly
+the h halo rows are stale and the m inner rows are exact.  h/m of the step work
+is redone in the halos.
 
-    my inner rows [h, 2h)       -> the strip above, into its bottom halo
-    my inner rows [m, m + h)    -> the strip below, into its top halo
+Every block of k generations (ring neighbours on the torus):
 
-and then step k generations on their own.  Each generation the rows a strip
-cannot know (its halo edges, where its own torus wraps falsely) spoil R more
-rows from each end, so after k generations exactly the h halo rows are stale
-and the m inner rows are exact.  Each exchange moves 2h rows of n bytes per
-strip; h/m of the step work is redone in the halos.
+  1. the strip's new boundary rows -- its first and last h inner rows after
+     the block, which the neighbours need as halos for the next block -- come
+     first, from two small edge tori of 3h rows each (copies of its top and
+     bottom 3h rows, stepped k generations: their middle h rows are exact);
+  2. they go out (first rows to the strip above, last rows to the strip
+     below), and the neighbours' boundary rows are received as the new halos;
+  3. meanwhile the strip itself steps the k generations;
+  4. the received rows replace its (now stale) halo rows.
+
+With NCCL the transfer of step 2 runs on NCCL's own stream while the kernels
+of step 3 run on the strip's: the exchange is hidden behind the block's
+compute, at the price of stepping 2 x 3h extra rows.  Each exchange moves 2h
+rows of n bytes per strip.
 
 Two transports:
   LocalStrips  all strips in one process (tests, or several strips on one
@@ -22,8 +32,8 @@ Two transports:
 
 A strip is stepped by a "stepper": an object with `rows`, `n`, `read_rows(row0,
 nrows, out)`, `write_rows(row0, src)` (torch tensors of shape (nrows, n)) and
-`step(g)`.  GpuStepper wraps a rectangular plain-variant context
-(ltl_create_rect, ltl_download_rows_device / ltl_upload_rows_device).
+`step(g)`.  GpuStepper wraps a rectangular plain or bit-packed context
+(ltl_create_rect_variant, ltl_download_rows_device / ltl_upload_rows_device).
 """
 import torch
 
@@ -38,18 +48,20 @@ def halo_rows(radius, k):
 
 
 class GpuStepper:
-    """A strip as a rows x n torus on one GPU (plain variant), ordered on the
-    current torch stream, which must not be the legacy default stream: its
-    handle (0) would select the context's own stream, unordered with torch's
-    work.  The drivers below build their steppers inside a stream of their own."""
+    """A strip as a rows x n torus on one GPU (plain or bit-packed variant),
+    ordered on the current torch stream, which must not be the legacy default
+    stream: its handle (0) would select the context's own stream, unordered with
+    torch's work.  The drivers below build their steppers inside a stream of
+    their own."""
 
-    def __init__(self, rows, n, radius, rule, device=0):
-        from .ltl import CUDASolver
+    def __init__(self, rows, n, radius, rule, device=0, variant=None):
+        from .ltl import CUDASolver, VARIANT_PLAIN
         stream = torch.cuda.current_stream(device)
         if stream.cuda_stream == 0:
             raise RuntimeError("GpuStepper needs a non-default current stream (use torch.cuda.stream(...))")
         self.rows, self.n = rows, n
-        self.solver = CUDASolver(n, radius, rule, device=device, rows=rows)
+        self.solver = CUDASolver(n, radius, rule, variant=VARIANT_PLAIN if variant is None else variant,
+                                 device=device, rows=rows)
         self.solver.set_stream(stream.cuda_stream)
 
     def read_rows(self, row0, nrows, out):
@@ -66,21 +78,25 @@ class GpuStepper:
 
 
 class _Strip:
-    def __init__(self, a, b, h, stepper):
+    def __init__(self, a, b, h, stepper, top=None, bottom=None):
         self.a, self.b, self.h, self.st = a, b, h, stepper
         self.m = b - a
+        self.top, self.bottom = top, bottom  # edge tori of 3h rows (overlapped exchange)
 
 
 class _Base:
-    """Shared logic: loading the global grid, stepping with exchanges, gathering.
-    On a CUDA device all work (the steppers', the copies, the exchanges) runs on
-    one stream of the driver's own, `self.stream`."""
+    """Shared logic: loading the global grid, the block schedule, gathering.
+    On a CUDA device all work (the steppers', the copies, the exchanges) is
+    ordered on one stream of the driver's own, `self.stream`.  overlap=False
+    steps the strip first and reads its boundary rows from it afterwards (no
+    edge tori, nothing to hide the exchange behind)."""
 
-    def __init__(self, n, radius, k, device):
+    def __init__(self, n, radius, k, device, overlap=True):
         if k < 1:
             raise ValueError("k (generations per exchange) must be >= 1")
         self.n, self.radius, self.k = n, radius, k
         self.h = halo_rows(radius, k)
+        self.overlap = overlap
         self.device = torch.device(device)
         self.stream = torch.cuda.Stream(self.device) if self.device.type == "cuda" else None
 
@@ -94,31 +110,68 @@ class _Base:
                 raise ValueError(f"strip of {b - a} rows is thinner than its halo ({self.h} = R * k rows): "
                                  f"use fewer strips or a smaller k")
 
+    def _strip(self, a, b, make_stepper):
+        h, n = self.h, self.n
+        st = make_stepper(b - a + 2 * h, n)
+        if not self.overlap:
+            return _Strip(a, b, h, st)
+        return _Strip(a, b, h, st, make_stepper(3 * h, n), make_stepper(3 * h, n))
+
+    def _rows(self, count):
+        return torch.empty((count, self.n), dtype=torch.uint8, device=self.device)
+
     def _load(self, s, grid):
         """Strip s's local rows (inner rows a-h .. b+h, modulo n) from a global grid tensor."""
         idx = torch.arange(s.a - s.h, s.b + s.h, device=grid.device) % self.n
         s.st.write_rows(0, grid.index_select(0, idx).contiguous())
+
+    def _boundary_ahead(self, s, g):
+        """Strip s's first and last h inner rows as they will be after g <= k
+        generations, from its edge tori (local rows [0, 3h) and [m - h, m + 2h))."""
+        h = self.h
+        buf, first, last = self._rows(3 * h), self._rows(h), self._rows(h)
+        s.st.read_rows(0, 3 * h, buf)
+        s.top.write_rows(0, buf)
+        s.top.step(g)
+        s.top.read_rows(h, h, first)
+        s.st.read_rows(s.m - h, 3 * h, buf)
+        s.bottom.write_rows(0, buf)
+        s.bottom.step(g)
+        s.bottom.read_rows(h, h, last)
+        return first, last
+
+    def _boundary_now(self, s):
+        """Strip s's first and last h inner rows, read from the strip itself."""
+        first, last = self._rows(self.h), self._rows(self.h)
+        s.st.read_rows(self.h, self.h, first)
+        s.st.read_rows(s.m, self.h, last)
+        return first, last
 
     def step(self, generations):
         with self._on_stream():
             left = generations
             while left > 0:
                 g = min(self.k, left)
-                self._exchange()
-                for s in self._local():
-                    s.st.step(g)
+                self._block(g)
                 left -= g
+
+    def close(self):
+        """Release every stepper that has a close() (the GPU contexts)."""
+        for s in self._local():
+            for st in (s.st, s.top, s.bottom):
+                if st is not None and hasattr(st, "close"):
+                    st.close()
 
 
 class LocalStrips(_Base):
     """All strips in this process: `make_stepper(rows, n)` builds each strip's stepper."""
 
-    def __init__(self, n, radius, parts, k, make_stepper, device="cpu"):
-        super().__init__(n, radius, k, device)
+    def __init__(self, n, radius, parts, k, make_stepper, device="cpu", overlap=True):
+        super().__init__(n, radius, k, device, overlap)
         bounds = partition(n, parts)
         self._check(bounds)
         with self._on_stream():
-            self.strips = [_Strip(a, b, self.h, make_stepper(b - a + 2 * self.h, n)) for a, b in bounds]
+            self.strips = [self._strip(a, b, make_stepper) for a, b in bounds]
 
     def _local(self):
         return self.strips
@@ -129,19 +182,19 @@ class LocalStrips(_Base):
             for s in self.strips:
                 self._load(s, g)
 
-    def _exchange(self):
-        P, h, n = len(self.strips), self.h, self.n
-        tops, bots = [], []
-        for s in self.strips:
-            t = torch.empty((h, n), dtype=torch.uint8, device=self.device)
-            b = torch.empty((h, n), dtype=torch.uint8, device=self.device)
-            s.st.read_rows(h, h, t)        # my first inner rows
-            s.st.read_rows(s.m, h, b)      # my last inner rows
-            tops.append(t)
-            bots.append(b)
+    def _block(self, g):
+        P, h = len(self.strips), self.h
+        if self.overlap:
+            bounds = [self._boundary_ahead(s, g) for s in self.strips]
+            for s in self.strips:
+                s.st.step(g)
+        else:
+            for s in self.strips:
+                s.st.step(g)
+            bounds = [self._boundary_now(s) for s in self.strips]
         for p, s in enumerate(self.strips):
-            s.st.write_rows(0, bots[(p - 1) % P])          # above me: the previous strip's last rows
-            s.st.write_rows(s.m + h, tops[(p + 1) % P])    # below me: the next strip's first rows
+            s.st.write_rows(0, bounds[(p - 1) % P][1])      # above me: the previous strip's last rows
+            s.st.write_rows(s.m + h, bounds[(p + 1) % P][0])  # below me: the next strip's first rows
 
     def get_state(self):
         with self._on_stream():
@@ -157,9 +210,9 @@ class DistStrips(_Base):
     """One strip per rank of the default (or given) torch.distributed group.
     Tensors live on `device` (a CUDA device for NCCL, "cpu" for gloo)."""
 
-    def __init__(self, n, radius, k, make_stepper, device, group=None):
+    def __init__(self, n, radius, k, make_stepper, device, group=None, overlap=True):
         import torch.distributed as dist
-        super().__init__(n, radius, k, device)
+        super().__init__(n, radius, k, device, overlap)
         self.dist, self.group = dist, group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
@@ -168,7 +221,7 @@ class DistStrips(_Base):
         self.bounds = bounds
         a, b = bounds[self.rank]
         with self._on_stream():
-            self.s = _Strip(a, b, self.h, make_stepper(b - a + 2 * self.h, n))
+            self.s = self._strip(a, b, make_stepper)
 
     def _local(self):
         return [self.s]
@@ -178,31 +231,37 @@ class DistStrips(_Base):
         with self._on_stream():
             self._load(self.s, torch.as_tensor(grid, dtype=torch.uint8).to(self.device))
 
-    def _exchange(self):
-        s, h, n = self.s, self.h, self.n
+    def _post(self, first, last):
+        """Send my first rows up and my last rows down; receive the halo rows.
+        Returns (requests, rows from the strip above, rows from the strip below)."""
+        if self.world == 1:
+            return [], last, first  # the torus wraps onto this strip itself
         up = (self.rank - 1) % self.world
         down = (self.rank + 1) % self.world
-        top = torch.empty((h, n), dtype=torch.uint8, device=self.device)
-        bot = torch.empty((h, n), dtype=torch.uint8, device=self.device)
-        s.st.read_rows(h, h, top)
-        s.st.read_rows(s.m, h, bot)
-        if self.world == 1:
-            s.st.write_rows(0, bot)
-            s.st.write_rows(s.m + h, top)
-            return
-        from_up = torch.empty((h, n), dtype=torch.uint8, device=self.device)
-        from_down = torch.empty((h, n), dtype=torch.uint8, device=self.device)
+        from_up, from_down = self._rows(self.h), self._rows(self.h)
         d = self.dist
         # Per peer the messages match in issue order: my first rows go up, my last
         # rows go down; I receive the strip below's first rows, then the strip
         # above's last rows.  With two ranks both neighbours are the same peer and
         # that order pairs each message with the right halo.
-        ops = [d.P2POp(d.isend, top, up, self.group), d.P2POp(d.isend, bot, down, self.group),
+        ops = [d.P2POp(d.isend, first, up, self.group), d.P2POp(d.isend, last, down, self.group),
                d.P2POp(d.irecv, from_down, down, self.group), d.P2POp(d.irecv, from_up, up, self.group)]
-        for req in d.batch_isend_irecv(ops):
+        return d.batch_isend_irecv(ops), from_up, from_down
+
+    def _block(self, g):
+        s = self.s
+        if self.overlap:
+            # the exchange is posted before the strip's own k generations are
+            # enqueued, so that it runs beside them
+            reqs, from_up, from_down = self._post(*self._boundary_ahead(s, g))
+            s.st.step(g)
+        else:
+            s.st.step(g)
+            reqs, from_up, from_down = self._post(*self._boundary_now(s))
+        for req in reqs:
             req.wait()
         s.st.write_rows(0, from_up)
-        s.st.write_rows(s.m + h, from_down)
+        s.st.write_rows(s.m + s.h, from_down)
 
     def get_state(self):
         """The full grid on every rank (all-gather of the inner rows)."""

@@ -74,6 +74,15 @@ int ltl_create(ltl_ctx** out, int device, int n, int radius, int smin, int smax,
 int ltl_create_rect(ltl_ctx** out, int device, int rows, int cols, int radius, int smin, int smax, int bmin,
                     int bmax);
 
+/* ltl_create_rect for a chosen variant: LTL_VARIANT_PLAIN or LTL_VARIANT_PACKED
+ * (the bit-packed step also takes rows != cols; LTL_VARIANT_AUTO means plain,
+ * any other variant LTL_EUNSUPPORTED when rows != cols).  Row strips of the
+ * packed variant move their halo rows through ltl_download_rows_device /
+ * ltl_upload_rows_device, which unpack or pack only the rows asked for.  No
+ * counterpart in the reference. */
+int ltl_create_rect_variant(ltl_ctx** out, int device, int rows, int cols, int radius, int smin, int smax, int bmin,
+                            int bmax, int variant);
+
 /* Release device memory and graphs.  (The reference never frees its domains.) */
 int ltl_destroy(ltl_ctx* ctx);
 
