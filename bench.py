@@ -328,8 +328,14 @@ def radius_sweep(C, torch, args, passes_per_variant, emit=None):
                                          "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                                                       "unit": "GB/s", "frac": round(achieved / peak, 4),
                                                       "bytes_per_update": BYTES_PER_UPDATE[name]}}
+                if name == "tensor":
+                    # product-2 operand chosen from the exactness bound of the row sums
+                    out["variants"][name]["operand"] = "f16" if s.info.operand_bits == 16 else "u8"
             finally:
                 s.close()
+        v = out["variants"]
+        if "gcups" in v.get("tensor", {}) and "gcups" in v.get("plain", {}):
+            out["tensor_vs_plain"] = round(v["tensor"]["gcups"] / v["plain"]["gcups"], 3)
         records.append(out)
         if emit:
             emit(out)
@@ -538,10 +544,11 @@ def main():
                 "metric": METRIC, "value": round(N * N * r["generations"] / (r["ms"] * 1e-3) / 1e9, 3),
                 "unit": "GCUPS", "n_gpus": world, "steps": r["generations"], "warmup": args.warmup,
                 "ms_per_step": round(r["ms"] / r["generations"], 5), "higher_is_better": True, "scaling": "strong",
-                "vs_baseline": None, "dtype": "u8", "data": "synthetic: reference generator start grid (seed 1)",
-                "config": {"workload": WORKLOAD, "variant": "plain, row strips", "n": N, "radius": RADIUS,
+                "vs_baseline": None, "dtype": DTYPE["packed"],
+                "data": "synthetic: reference generator start grid (seed 1)",
+                "config": {"workload": WORKLOAD, "variant": "packed, row strips", "n": N, "radius": RADIUS,
                            "parallelism": f"row strips x{world}, {r['halo_rows']}-row halo exchange every "
-                                          f"{args.strips} generations",
+                                          f"{args.strips} generations, overlapped with the strips' steps",
                            "l2": "not flushed (continuous run)"},
                 "bit_exact_step100": r["bit_exact"]}))
         if world > 1:
@@ -582,7 +589,9 @@ def main():
             "kernel_ms_per_launch": round(kernel_ms_launch, 5), "temporal_depth": r["depth"],
             "bit_exact_step100": r["bit_exact_step100"], "dtype": DTYPE[name],
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": traffic.get(name)},
+                         "frac": round(achieved / peak, 4), "traffic": traffic.get(name),
+                         "traffic_source": "profiles/traffic_n16384_r5.txt: dram bytes of one ncu capture of "
+                                           "the step kernel (cache control on, the run's L2 flush not applied)"},
             "gpu_launches": r["all_launches"],
         }
         if r["bit_exact_step100"] and (best is None or gcups > variants[best]["gcups"]):
@@ -616,7 +625,9 @@ def main():
                     "U[0.2,0.6] (mt19937_64 seed 4), 256 steps per ltl_batch_step call, bit-packed",
         "grid_steps_per_s": round(world * br["grids"] * br["steps"] / (b_ms * 1e-3), 1),
         "gcups": round(b_gcups, 2), "ms": round(b_ms, 3), "cells": br["cells"],
-        "shared_memory_resident_grids": br["resident_grids"],
+        "mode": "persistent: one launch per rule class per ltl_batch_step call runs all 256 generations, "
+                "each CTA advancing whole grids (largest first) with the grid held in L1/L2",
+        "grids_all_steps_in_one_launch": br["resident_grids"],
         "roofline": {"bound": "hbm", "bytes_per_update": 0.25, "achieved": round(b_gcups * 0.25, 1),
                      "peak": peak, "unit": "GB/s", "frac": round(b_gcups * 0.25 / peak, 4),
                      "frac_u8_equivalent": round(b_gcups * 2.0 / peak, 4)},

@@ -431,7 +431,7 @@ extern "C" int ltl_download_rows_device(ltl_ctx* c, int row0, int nrows, uint8_t
     if (int r = check_rows(c, "ltl_download_rows_device", row0, nrows, dev, pitch)) return r;
     if (nrows == 0) return LTL_OK;
     LTL_CUDA(cudaSetDevice(c->device));
-    if (c->variant != LTL_VARIANT_PLAIN) {
+    if (keeps_packed(c) && c->packed_valid) {
         // straight from the packed frame: only the asked rows are unpacked
         LTL_CUDA(launch_unpack_rows(cur_packed(c), row0, nrows, dev, pitch, c->stream));
         return LTL_OK;
@@ -447,9 +447,13 @@ extern "C" int ltl_upload_rows_device(ltl_ctx* c, int row0, int nrows, const uin
     if (int r = check_rows(c, "ltl_upload_rows_device", row0, nrows, dev, pitch)) return r;
     if (nrows == 0) return LTL_OK;
     LTL_CUDA(cudaSetDevice(c->device));
-    if (c->variant != LTL_VARIANT_PLAIN) {
-        // straight into the packed frame (the byte frame is staging only: every
-        // read of a packed grid unpacks it again), then its halo
+    if (keeps_packed(c)) {
+        // straight into the packed frame once it holds the current state (the
+        // byte frame is staging only: every read of a packed grid unpacks it
+        // again), then its halo
+        if (!c->packed_valid) {
+            if (int r = sync_to_packed(c)) return r;
+        }
         LTL_CUDA(launch_pack_rows(dev, pitch, cur_packed(c), row0, nrows, c->stream));
         if (c->variant == LTL_VARIANT_PACKED) LTL_CUDA(launch_packed_halo(cur_packed(c), c->stream));
         return LTL_OK;
