@@ -32,7 +32,10 @@ struct BatchGrid {
     long long cell_off;  // byte offset of the grid in the dense staging buffer
     int n, nw, HR, wp;   // cells per side, inner words per row, halo rows, words per frame row
     int R;
+    int cls;             // rule class
 };
+
+#define LTL_BATCH_RADII(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
 
 constexpr int kBatchWarps = 4;
 constexpr int kResThreads = 1024;
@@ -236,13 +239,15 @@ k_batch_resident(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, c
 }
 
 // ---------------------------------------------------------------------------
-// Persistent kernel: one launch per rule class advances every grid of the
-// class through all the generations of one ltl_batch_step.  A CTA takes whole
-// grids from a device counter, largest first, and runs a grid's generations
-// back to back with CTA barriers between them, so the grid stays in this SM's
-// L1 and the L2 for the whole run (temporal blocking of the run) and no
-// per-generation launch or halo launch is made.  Rows of fewer than 32 words
-// are handled by segments of a warp working on different row bands.
+// Persistent kernel: one launch advances every grid of the batch through all
+// the generations of one ltl_batch_step.  A CTA takes whole grids from a device
+// counter, the most work first, and runs a grid's generations back to back with
+// CTA barriers between them, so the grid stays in this SM's L1 and the L2 for
+// the whole run (temporal blocking of the run) and no per-generation launch or
+// halo launch is made.  The grid's radius selects the band walk (a switch over
+// the compiled radii) and its rule class the comparator masks, which are loaded
+// once per grid.  Rows of fewer than 32 words are handled by segments of a warp
+// working on different row bands.
 // ---------------------------------------------------------------------------
 constexpr int kPersistWarps = 8;
 
@@ -263,15 +268,52 @@ __device__ void frame_halo_cta(uint32_t* f, const BatchGrid& g) {
     __syncthreads();
 }
 
+// All generations of one grid by the whole CTA (radius R).
 template <int R>
-__global__ void __launch_bounds__(kPersistWarps * 32)
-k_batch_persist(uint32_t* a0, uint32_t* a1, const BatchGrid* __restrict__ grids, const int* __restrict__ order,
-                int n_order, int* next, int steps, const __grid_constant__ PackedRule pr) {
+__device__ void persist_grid(const BatchGrid& g, uint32_t* a0, uint32_t* a1, int steps, const PackedRule& rule,
+                             uint32_t* ring_all) {
     using Ring = PackedRing<R, kPersistWarps>;
-    extern __shared__ uint32_t ring_all[];
-    __shared__ int s_item;
+    const PackedRule pr = rule;  // the masks the comparators use, kept in registers
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint32_t* ring_lane = ring_all + (size_t)wid * Ring::WARP_WORDS + lane;
+    uint32_t* f0 = a0 + g.off;
+    uint32_t* f1 = a1 + g.off;
+    frame_halo_cta(f0, g);
+    // lanes per segment: the row's words rounded up to a power of two, at most 32
+    const int seg = g.nw >= 32 ? 32 : (g.nw <= 1 ? 1 : 1 << (32 - __clz(g.nw - 1)));
+    const int ns = 32 / seg;  // segments per warp
+    const int strips = (g.nw + seg - 1) / seg;
+    // enough bands for every segment of the CTA, none shorter than 2 (2R + 1)
+    // rows (a band first counts 2R + 1 rows to start its window)
+    const int want = max(1, kPersistWarps * ns / strips);
+    const int band_rows = min(g.n, max((g.n + want - 1) / want, 4 * R + 2));
+    const int bands = (g.n + band_rows - 1) / band_rows;
+    const int items = strips * bands;
+    const int wl = lane & (seg - 1), sidx = lane / seg;
+    for (int s = 0; s < steps; ++s) {
+        const uint32_t* src = (s & 1) ? f1 : f0;
+        uint32_t* dst = (s & 1) ? f0 : f1;
+        for (int base = wid * ns; base < items; base += kPersistWarps * ns) {  // warp-uniform
+            const int item = base + sidx;
+            const bool valid = item < items;
+            const int strip = valid ? item % strips : 0;
+            const int band = valid ? item / strips : 0;
+            const int r0 = band * band_rows, r1 = min(r0 + band_rows, g.n);
+            const int w = strip * seg + wl;
+            const bool active = valid && w < g.nw;
+            packed_band_seg<R, Ring::fits>(src, dst, (size_t)g.wp, g.HR, r0, r1, band_rows, 1 + w, active, wl == 0,
+                                           wl == seg - 1 || w == g.nw - 1, ring_lane, pr);
+        }
+        __syncthreads();
+        frame_halo_cta(dst, g);
+    }
+}
+
+__global__ void __launch_bounds__(kPersistWarps * 32)
+k_batch_persist(uint32_t* a0, uint32_t* a1, const BatchGrid* __restrict__ grids, const PackedRule* __restrict__ rules,
+                const int* __restrict__ order, int n_order, int* next, int steps) {
+    extern __shared__ uint32_t ring_all[];
+    __shared__ int s_item;
     while (true) {
         if (threadIdx.x == 0) s_item = atomicAdd(next, 1);
         __syncthreads();
@@ -279,38 +321,22 @@ k_batch_persist(uint32_t* a0, uint32_t* a1, const BatchGrid* __restrict__ grids,
         __syncthreads();  // every thread has read s_item before it is overwritten
         if (li >= n_order) break;
         const BatchGrid g = grids[order[li]];
-        uint32_t* f0 = a0 + g.off;
-        uint32_t* f1 = a1 + g.off;
-        frame_halo_cta(f0, g);
-        // lanes per segment: the row's words rounded up to a power of two, at most 32
-        const int seg = g.nw >= 32 ? 32 : (g.nw <= 1 ? 1 : 1 << (32 - __clz(g.nw - 1)));
-        const int ns = 32 / seg;  // segments per warp
-        const int strips = (g.nw + seg - 1) / seg;
-        // enough bands for every segment of the CTA, none shorter than 2 (2R + 1)
-        // rows (a band first counts 2R + 1 rows to start its window)
-        const int want = max(1, kPersistWarps * ns / strips);
-        const int band_rows = min(g.n, max((g.n + want - 1) / want, 4 * R + 2));
-        const int bands = (g.n + band_rows - 1) / band_rows;
-        const int items = strips * bands;
-        const int wl = lane & (seg - 1), sidx = lane / seg;
-        for (int s = 0; s < steps; ++s) {
-            const uint32_t* src = (s & 1) ? f1 : f0;
-            uint32_t* dst = (s & 1) ? f0 : f1;
-            for (int base = wid * ns; base < items; base += kPersistWarps * ns) {  // warp-uniform
-                const int item = base + sidx;
-                const bool valid = item < items;
-                const int strip = valid ? item % strips : 0;
-                const int band = valid ? item / strips : 0;
-                const int r0 = band * band_rows, r1 = min(r0 + band_rows, g.n);
-                const int w = strip * seg + wl;
-                const bool active = valid && w < g.nw;
-                packed_band_seg<R, Ring::fits>(src, dst, (size_t)g.wp, g.HR, r0, r1, band_rows, 1 + w, active,
-                                               wl == 0, wl == seg - 1 || w == g.nw - 1, ring_lane, pr);
-            }
-            __syncthreads();
-            frame_halo_cta(dst, g);
+        switch (g.R) {
+#define LTL_C(r) \
+    case r: persist_grid<r>(g, a0, a1, steps, rules[g.cls], ring_all); break;
+            LTL_BATCH_RADII(LTL_C)
+#undef LTL_C
+            default: break;
         }
     }
+}
+
+// Shared memory of the persistent kernel for a batch whose largest radius is R:
+// 8 warps' h rings when they fit (else the walk counts leaving rows again).
+template <int R>
+static size_t persist_ring_bytes() {
+    using Ring = PackedRing<R, kPersistWarps>;
+    return Ring::fits ? (size_t)Ring::BYTES : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -380,31 +406,6 @@ static cudaError_t launch_batch_resident_r(const uint32_t* src, uint32_t* dst, c
     return cudaGetLastError();
 }
 
-template <int R>
-static cudaError_t launch_batch_persist_r(uint32_t* a0, uint32_t* a1, const BatchGrid* grids, const int* order,
-                                          int n_order, int* next, int steps, const PackedRule& pr, int ctas,
-                                          cudaStream_t s) {
-    using Ring = PackedRing<R, kPersistWarps>;
-    const int smem = Ring::fits ? Ring::BYTES : 0;
-    k_batch_persist<R><<<ctas, kPersistWarps * 32, smem, s>>>(a0, a1, grids, order, n_order, next, steps, pr);
-    return cudaGetLastError();
-}
-
-// Shared-memory limit of the persistent kernel (its h rings), set outside any
-// stream capture; returns the CTAs one SM holds.
-template <int R>
-static cudaError_t prepare_persist_r(int* per_sm) {
-    using Ring = PackedRing<R, kPersistWarps>;
-    const int smem = Ring::fits ? Ring::BYTES : 0;
-    // always raised: the kernel's own static shared memory counts against the
-    // default 48 KiB too
-    cudaError_t e = cudaFuncSetAttribute(k_batch_persist<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_batch_persist<R>, kPersistWarps * 32, smem);
-}
-
-#define LTL_BATCH_RADII(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
-
 static cudaError_t batch_step_dispatch(int R, const uint32_t* cur, uint32_t* nxt, const BatchGrid* grids,
                                        const int4* items, int n_items, const PackedRule& pr, int sms, cudaStream_t s) {
     switch (R) {
@@ -453,25 +454,13 @@ static cudaError_t batch_prepare_dispatch(int R, size_t smem) {
     }
 }
 
-static cudaError_t batch_persist_dispatch(int R, uint32_t* a0, uint32_t* a1, const BatchGrid* grids,
-                                          const int* order, int n_order, int* next, int steps, const PackedRule& pr,
-                                          int ctas, cudaStream_t s) {
+static size_t persist_ring_dispatch(int R) {
     switch (R) {
 #define LTL_C(r) \
-    case r: return launch_batch_persist_r<r>(a0, a1, grids, order, n_order, next, steps, pr, ctas, s);
+    case r: return persist_ring_bytes<r>();
         LTL_BATCH_RADII(LTL_C)
 #undef LTL_C
-        default: return cudaErrorInvalidValue;
-    }
-}
-
-static cudaError_t batch_persist_prepare_dispatch(int R, int* per_sm) {
-    switch (R) {
-#define LTL_C(r) \
-    case r: return prepare_persist_r<r>(per_sm);
-        LTL_BATCH_RADII(LTL_C)
-#undef LTL_C
-        default: return cudaErrorInvalidValue;
+        default: return 0;
     }
 }
 
@@ -494,9 +483,6 @@ struct BatchClass {
     PackedRule pr;
     std::vector<int> resident;   // grid ids kept in shared memory
     std::vector<int> streamed;   // grid ids streamed per step
-    std::vector<int> order;      // persistent mode: every grid id of the class, largest first
-    int* d_order = nullptr;
-    int persist_ctas = 0;
     int* d_resident = nullptr;
     int4* d_items = nullptr;
     int n_items = 0;
@@ -522,13 +508,16 @@ struct ltl_batch {
     bool cur_is_a = true;
     bool no_graph = false;
     bool persistent = true;
-    int* d_next = nullptr;  // persistent mode: one grid counter per class
+    // persistent mode: every grid, the most work first; the CTAs' grid counter;
+    // the rule classes' comparator masks
+    int* d_order = nullptr;
+    int n_order = 0;
+    int* d_next = nullptr;
+    PackedRule* d_rules = nullptr;
+    int persist_ctas = 0;
+    size_t persist_smem = 0;
     cudaStream_t own = nullptr, stream = nullptr, aux = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
-    // persistent mode: the class launches run concurrently on these streams
-    static constexpr int kLanes = 16;
-    cudaStream_t lanes[kLanes] = {};
-    cudaEvent_t lane_join[kLanes] = {};
     // graph cache: (steps, parity) -> exec
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;
 };
@@ -540,13 +529,10 @@ static void batch_release(ltl_batch* b) {
     for (auto& c : b->classes) {
         if (c.d_resident) cudaFree(c.d_resident);
         if (c.d_items) cudaFree(c.d_items);
-        if (c.d_order) cudaFree(c.d_order);
     }
     if (b->d_next) cudaFree(b->d_next);
-    for (int i = 0; i < ltl_batch::kLanes; ++i) {
-        if (b->lane_join[i]) cudaEventDestroy(b->lane_join[i]);
-        if (b->lanes[i]) cudaStreamDestroy(b->lanes[i]);
-    }
+    if (b->d_order) cudaFree(b->d_order);
+    if (b->d_rules) cudaFree(b->d_rules);
     if (b->d_grids) cudaFree(b->d_grids);
     if (b->d_streamed_all) cudaFree(b->d_streamed_all);
     for (auto& a : b->arena)
@@ -579,51 +565,40 @@ static int batch_plan(ltl_batch* b) {
     for (auto& c : b->classes) {
         if (c.d_resident) cudaFree(c.d_resident);
         if (c.d_items) cudaFree(c.d_items);
-        if (c.d_order) cudaFree(c.d_order);
         c.d_resident = nullptr;
         c.d_items = nullptr;
-        c.d_order = nullptr;
         c.resident.clear();
         c.streamed.clear();
-        c.order.clear();
         c.n_items = 0;
         c.res_smem = 0;
-        c.persist_ctas = 0;
     }
+    if (b->d_order) cudaFree(b->d_order);
+    b->d_order = nullptr;
+    b->n_order = 0;
     if (b->d_streamed_all) cudaFree(b->d_streamed_all);
     b->d_streamed_all = nullptr;
     b->n_streamed_all = 0;
     const int count = (int)b->grids.size();
     if (b->persistent) {
-        // every grid of a class in one list, largest first (the CTAs take them in order)
-        for (int i = 0; i < count; ++i) b->classes[b->cls_id[i]].order.push_back(i);
-        // The class launches run side by side from the start, each with a share
-        // of the GPU's CTA slots in proportion to its work (cells x a cost that
-        // grows with R), so that every class starts its largest grids at once
-        // instead of waiting for the classes launched before it.
-        std::map<int, int> per_sm_by_radius;
-        std::vector<double> work(b->classes.size(), 0.0);
-        double total = 0.0;
-        for (size_t ci = 0; ci < b->classes.size(); ++ci) {
-            BatchClass& c = b->classes[ci];
-            std::stable_sort(c.order.begin(), c.order.end(),
-                             [&](int x, int y) { return b->grids[x].n > b->grids[y].n; });
-            if (!per_sm_by_radius.count(c.rule.radius)) {
-                int per_sm = 0;
-                BATCH_CUDA(batch_persist_prepare_dispatch(c.rule.radius, &per_sm));
-                per_sm_by_radius[c.rule.radius] = std::max(per_sm, 1);
-            }
-            for (int gi : c.order) work[ci] += (double)b->grids[gi].n * b->grids[gi].n * (4.0 + c.rule.radius);
-            total += work[ci];
+        // one list of every grid, the most work first (cells x a cost that grows
+        // with R), which the CTAs of the one launch take in order
+        std::vector<int> order(count);
+        size_t smem = 0;
+        for (int i = 0; i < count; ++i) {
+            order[i] = i;
+            smem = std::max(smem, persist_ring_dispatch(b->grids[i].R));
         }
-        for (size_t ci = 0; ci < b->classes.size(); ++ci) {
-            BatchClass& c = b->classes[ci];
-            const double slots = (double)b->sms * per_sm_by_radius[c.rule.radius];
-            const int share = (int)(slots * work[ci] / std::max(total, 1.0) + 0.5);
-            c.persist_ctas = std::max(1, std::min((int)c.order.size(), share));
-            BATCH_CUDA(cudaMalloc(&c.d_order, sizeof(int) * c.order.size()));
-            BATCH_CUDA(cudaMemcpy(c.d_order, c.order.data(), sizeof(int) * c.order.size(), cudaMemcpyHostToDevice));
-        }
+        auto cost = [&](int i) { return (double)b->grids[i].n * b->grids[i].n * (4.0 + b->grids[i].R); };
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+        // always raised: the kernel's own static shared memory counts against the default 48 KiB too
+        BATCH_CUDA(cudaFuncSetAttribute(k_batch_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        BATCH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persist, kPersistWarps * 32, smem));
+        b->persist_smem = smem;
+        b->persist_ctas = std::max(1, std::min(count, b->sms * std::max(per_sm, 1)));
+        b->n_order = count;
+        BATCH_CUDA(cudaMalloc(&b->d_order, sizeof(int) * count));
+        BATCH_CUDA(cudaMemcpy(b->d_order, order.data(), sizeof(int) * count, cudaMemcpyHostToDevice));
         return LTL_OK;
     }
     std::vector<int> streamed_all;
@@ -711,6 +686,7 @@ static int batch_build(ltl_batch* b, int flags) {
         words += (size_t)(g.n + 2 * g.HR) * g.wp;
         words = (words + 31) / 32 * 32;
         cells += (long long)g.n * g.n;
+        g.cls = it->second;
         b->grids[i] = g;
         rmax = std::max(rmax, d.radius);
     }
@@ -720,7 +696,13 @@ static int batch_build(ltl_batch* b, int flags) {
     b->resident_max = (flags & LTL_BATCH_STREAM_ALL) ? 0
                                                      : tuning_lookup("batch", -1, 0, "resident_max_bytes", kResSmemLimit);
     b->persistent = !(flags & LTL_BATCH_STREAM_ALL) && tuning_lookup("batch", -1, 0, "persistent", 1) != 0;
-    BATCH_CUDA(cudaMalloc(&b->d_next, sizeof(int) * std::max<size_t>(b->classes.size(), 1)));
+    BATCH_CUDA(cudaMalloc(&b->d_next, sizeof(int)));
+    {
+        std::vector<PackedRule> rules;
+        for (auto& c : b->classes) rules.push_back(c.pr);
+        BATCH_CUDA(cudaMalloc(&b->d_rules, sizeof(PackedRule) * rules.size()));
+        BATCH_CUDA(cudaMemcpy(b->d_rules, rules.data(), sizeof(PackedRule) * rules.size(), cudaMemcpyHostToDevice));
+    }
     BATCH_CUDA(cudaMalloc(&b->d_grids, sizeof(BatchGrid) * count));
     BATCH_CUDA(cudaMemcpy(b->d_grids, b->grids.data(), sizeof(BatchGrid) * count, cudaMemcpyHostToDevice));
     for (auto& a : b->arena) {
@@ -795,10 +777,6 @@ extern "C" int ltl_batch_create(ltl_batch** out, int device, const ltl_grid_desc
     if (se == cudaSuccess) se = cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking);
     if (se == cudaSuccess) se = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (se == cudaSuccess) se = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
-    for (int i = 0; i < ltl_batch::kLanes && se == cudaSuccess; ++i) {
-        se = cudaStreamCreateWithFlags(&b->lanes[i], cudaStreamNonBlocking);
-        if (se == cudaSuccess) se = cudaEventCreateWithFlags(&b->lane_join[i], cudaEventDisableTiming);
-    }
     if (se != cudaSuccess) {
         ltl_set_error("ltl_batch_create: stream/event creation failed: %s", cudaGetErrorString(se));
         batch_release(b);
@@ -924,32 +902,13 @@ static cudaError_t enqueue_steps(ltl_batch* b, int steps, const char** what) {
     uint32_t* a0 = cur_arena(b);
     uint32_t* a1 = nxt_arena(b);
     if (b->persistent) {
-        // one launch per rule class, the classes spread over kLanes forked streams
-        const int nc = (int)b->classes.size();
         *what = "grid counter reset";
-        e = cudaMemsetAsync(b->d_next, 0, sizeof(int) * nc, b->stream);
+        e = cudaMemsetAsync(b->d_next, 0, sizeof(int), b->stream);
         if (e == cudaSuccess) {
-            *what = "fork event record";
-            e = cudaEventRecord(b->fork, b->stream);
-        }
-        const int used = std::min(nc, (int)ltl_batch::kLanes);
-        for (int i = 0; i < used && e == cudaSuccess; ++i) {
-            *what = "fork stream wait";
-            e = cudaStreamWaitEvent(b->lanes[i], b->fork, 0);
-        }
-        for (int ci = 0; ci < nc && e == cudaSuccess; ++ci) {
-            BatchClass& c = b->classes[ci];
             *what = "persistent kernel launch";
-            e = batch_persist_dispatch(c.rule.radius, a0, a1, b->d_grids, c.d_order, (int)c.order.size(),
-                                       b->d_next + ci, steps, c.pr, c.persist_ctas, b->lanes[ci % used]);
-        }
-        for (int i = 0; i < used && e == cudaSuccess; ++i) {
-            *what = "join event record";
-            e = cudaEventRecord(b->lane_join[i], b->lanes[i]);
-            if (e == cudaSuccess) {
-                *what = "join stream wait";
-                e = cudaStreamWaitEvent(b->stream, b->lane_join[i], 0);
-            }
+            k_batch_persist<<<b->persist_ctas, kPersistWarps * 32, b->persist_smem, b->stream>>>(
+                a0, a1, b->d_grids, b->d_rules, b->d_order, b->n_order, b->d_next, steps);
+            e = cudaGetLastError();
         }
         return e;
     }
@@ -1060,7 +1019,9 @@ extern "C" int ltl_batch_info(const ltl_batch* b, long long* cells, long long* d
     if (temporal_depth) {
         // grids that run every generation of an ltl_batch_step inside one launch
         int res = 0;
-        for (auto& c : b->classes) res += (int)(b->persistent ? c.order.size() : c.resident.size());
+        if (b->persistent) res = (int)b->grids.size();
+        else
+            for (auto& c : b->classes) res += (int)c.resident.size();
         *temporal_depth = res;
     }
     return LTL_OK;
