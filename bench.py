@@ -230,15 +230,30 @@ def run_variant(C, torch, name, start, args, flush, sampler=None):
         s.close()
 
 
-def e2e_run(C, torch, name, start, steps):
+def e2e_run(C, torch, name, start, steps, packed_io=None):
     """Through the public API with host buffers: upload the start grid from pinned
-    memory, advance `steps` generations, download the grid -- timed together."""
-    vcode = {"plain": C.VARIANT_PLAIN, "tensor": C.VARIANT_TENSOR, "packed": C.VARIANT_PACKED}[name]
-    stream = torch.cuda.Stream()
-    pinned_in = torch.from_numpy(start).pin_memory()
-    pinned_out = torch.empty_like(pinned_in).pin_memory()
+    memory, advance `steps` generations, download the grid -- timed together.
+    The bit-packed variants move the grid in the PACK coding (ltl_upload_packed /
+    ltl_download_packed: 1 bit per cell), the plain one as uint8 cells
+    (ltl_upload / ltl_download); packed_io=False forces uint8 for any variant.
+    The downloaded grid is checked against the context's own uint8 download."""
     import ctypes
+    import numpy as np
+    vcode = {"plain": C.VARIANT_PLAIN, "tensor": C.VARIANT_TENSOR, "packed": C.VARIANT_PACKED}[name]
+    if packed_io is None:
+        packed_io = name in ("packed", "tensor")
+    stream = torch.cuda.Stream()
+    if packed_io:
+        host = C.pack_grid(start)
+        pinned_in = torch.from_numpy(host.view(np.int64)).pin_memory()
+        pitch = host.shape[1] * 8
+    else:
+        pinned_in = torch.from_numpy(start).pin_memory()
+        pitch = N
+    pinned_out = torch.empty_like(pinned_in).pin_memory()
+    nbytes = pinned_in.numel() * pinned_in.element_size()
     L = C.lib()
+    up, down = (L.ltl_upload_packed, L.ltl_download_packed) if packed_io else (L.ltl_upload, L.ltl_download)
     s = C.CUDASolver(N, RADIUS, RULE, variant=vcode, device=torch.cuda.current_device())
     try:
         s.set_stream(stream.cuda_stream)
@@ -250,15 +265,20 @@ def e2e_run(C, torch, name, start, steps):
             b = torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
             a.record(stream)
-            C.ltl.check(L.ltl_upload(s._h, ctypes.c_void_p(pinned_in.data_ptr()), N))
+            C.ltl.check(up(s._h, ctypes.c_void_p(pinned_in.data_ptr()), pitch))
             s.doSteps(steps)
-            C.ltl.check(L.ltl_download(s._h, ctypes.c_void_p(pinned_out.data_ptr()), N))
+            C.ltl.check(down(s._h, ctypes.c_void_p(pinned_out.data_ptr()), pitch))
             b.record(stream)
             stream.synchronize()
             if it > 0:
                 times.append(a.elapsed_time(b))
         ms = sum(times) / len(times)
-        return dict(ms=ms, steps=steps, gcups=N * N * steps / (ms * 1e-3) / 1e9, h2d=N * N, d2h=N * N)
+        got = pinned_out.numpy()
+        got = C.unpack_grid(got.view(np.uint64), N) if packed_io else got
+        same = bool(np.array_equal(got, s.getCurrentState()))
+        return dict(ms=ms, steps=steps, gcups=N * N * steps / (ms * 1e-3) / 1e9, h2d=nbytes, d2h=nbytes,
+                    io="PACK-coded uint64 rows (1 bit per cell)" if packed_io else "uint8 cells",
+                    download_matches=same)
     finally:
         s.close()
 
@@ -638,8 +658,16 @@ def main():
     line["e2e"] = {"value": round(world * N * N * e2["steps"] / (e2_ms * 1e-3) / 1e9, 3), "unit": "GCUPS",
                    "h2d_bytes_per_step": int(e2["h2d"] / e2["steps"]), "d2h_bytes_per_step": int(e2["d2h"] /
                                                                                                 e2["steps"]),
+                   "io": e2["io"], "download_matches": e2["download_matches"],
                    "note": f"upload start grid from pinned host memory + {e2['steps']} steps + download, "
                            f"{best} variant"}
+    if best in ("packed", "tensor"):
+        # the same run with the grid moved as uint8 cells
+        e3 = e2e_run(C, torch, best, start, args.e2e_steps or args.steps, packed_io=False)
+        e3_ms = max_over_ranks(e3["ms"], world)
+        line["e2e"]["uint8_io"] = {"value": round(world * N * N * e3["steps"] / (e3_ms * 1e-3) / 1e9, 3),
+                                   "h2d_bytes_per_step": int(e3["h2d"] / e3["steps"]),
+                                   "d2h_bytes_per_step": int(e3["d2h"] / e3["steps"])}
     if rank == 0 and not args.no_sweep:
         # the radius-sweep workloads (32768^2, R in {1,2,4,8,16,32} and {64,128}) at
         # 4 timed generations per variant and radius; `bench.py --sweep` runs more
@@ -648,10 +676,13 @@ def main():
             "workload": "32768x32768 torus, scaled interval rule; seed 2 d=0.5 for R<=32, seed 3 d=0.3 for R=64,128; "
                         "4 generations per variant, L2 flushed before each, CUDA events",
             "unit": "GCUPS",
-            "by_radius": {str(r["radius"]): {v: ({"gcups": d["gcups"], "kernel_gcups": d["kernel_gcups"],
-                                                  "hbm_frac": d["roofline"]["frac"]} if "gcups" in d else
-                                                 {"unsupported": d["unsupported"]})
-                                             for v, d in r["variants"].items()} for r in recs}}
+            "by_radius": {str(r["radius"]): dict(
+                {v: ({"gcups": d["gcups"], "kernel_gcups": d["kernel_gcups"], "hbm_frac": d["roofline"]["frac"],
+                      **({"operand": d["operand"]} if "operand" in d else {})} if "gcups" in d else
+                     {"unsupported": d["unsupported"]})
+                 for v, d in r["variants"].items()},
+                **({"tensor_vs_plain": r["tensor_vs_plain"]} if "tensor_vs_plain" in r else {}))
+                for r in recs}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline_sample(os.cpu_count() or 1)
         if cb is not None:

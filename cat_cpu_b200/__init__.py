@@ -6,8 +6,8 @@ ctypes host mirror of the reference's solver interface (ltl.py).
 """
 from .ltl import (CASolverFactory, CUDASolver, Batch, LtlError, benchmark_seed, generate_state, start_grid,
                   compareCurrentStates, VARIANT_AUTO, VARIANT_PLAIN, VARIANT_TENSOR, VARIANT_PACKED,
-                  VARIANT_NAMES, lib)
+                  VARIANT_NAMES, lib, pack_grid, unpack_grid)
 
 __all__ = ["CASolverFactory", "CUDASolver", "Batch", "LtlError", "benchmark_seed", "generate_state", "start_grid",
            "compareCurrentStates", "VARIANT_AUTO", "VARIANT_PLAIN", "VARIANT_TENSOR", "VARIANT_PACKED",
-           "VARIANT_NAMES", "lib"]
+           "VARIANT_NAMES", "lib", "pack_grid", "unpack_grid"]

@@ -309,6 +309,34 @@ __global__ void k_unpack64(const uint64_t* __restrict__ words, size_t wp, int ro
     }
 }
 
+// Inner words of a packed frame -> PACK-coded rows (uint64 word k of a row =
+// frame words 2k and 2k + 1), bits past n cleared.
+__global__ void k_frame_to_pack64(const uint32_t* __restrict__ src, int n, int rows, int nw, int HR, int HW,
+                                  size_t wp, uint64_t* __restrict__ dst, size_t dst_wp) {
+    const int nw64 = (n + 63) / 64;
+    const long long total = (long long)rows * nw64;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / nw64), k = (int)(t % nw64);
+        const uint32_t* row = src + (size_t)(HR + i) * wp + HW;
+        uint32_t lo = row[2 * k];
+        uint32_t hi = 2 * k + 1 < nw ? row[2 * k + 1] : 0u;
+        uint64_t v = ((uint64_t)hi << 32) | lo;
+        const int valid = n - 64 * k;  // cells of this word inside the row
+        if (valid < 64) v &= (1ull << valid) - 1ull;
+        dst[(size_t)i * dst_wp + k] = v;
+    }
+}
+
+cudaError_t launch_frame_to_pack64(const PackedFrame& f, uint64_t* dst, size_t dst_pitch_words, cudaStream_t s) {
+    const long long total = (long long)f.nrows() * ((f.n + 63) / 64);
+    if (total == 0) return cudaSuccess;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 32);
+    k_frame_to_pack64<<<blocks, 256, 0, s>>>(f.words, f.n, f.nrows(), f.nw, f.HR, f.HW, f.wpitch, dst,
+                                             dst_pitch_words);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_pack(const uint8_t* cells, size_t cell_pitch, int rows, int cols, uint64_t* words,
                         size_t word_pitch_words, cudaStream_t s) {
     if (rows == 0 || cols == 0) return cudaSuccess;

@@ -58,6 +58,8 @@ struct ltl_ctx {
     PackedFrame pa{}, pb{};
     uint32_t* pwords = nullptr;
     size_t pwords_bytes = 0;
+    // PACK-coded staging rows of ltl_upload_packed / ltl_download_packed (made on first use)
+    uint64_t* pstage = nullptr;
     bool packed_valid = false;  // packed frames hold the current state
     // tensor variant
     TensorPlan* tplan = nullptr;
@@ -105,6 +107,7 @@ static void release(ltl_ctx* c) {
     if (c->tplan) tensor_plan_destroy(c->tplan);
     if (c->frames) cudaFree(c->frames);
     if (c->pwords) cudaFree(c->pwords);
+    if (c->pstage) cudaFree(c->pstage);
     if (c->scratch) cudaFree(c->scratch);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
@@ -400,6 +403,73 @@ extern "C" int ltl_download(ltl_ctx* c, uint8_t* inner, size_t pitch) {
     Frame& f = cur_frame(c);
     LTL_CUDA(cudaMemcpy2DAsync(inner, pitch, f.inner(0, 0), f.pitch, c->n, c->rows, cudaMemcpyDeviceToHost,
                                c->stream));
+    LTL_CUDA(cudaStreamSynchronize(c->stream));
+    return LTL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Host transfers in the PACK coding (ceil(n / 64) uint64 words per row).
+// ---------------------------------------------------------------------------
+static int pack_args(ltl_ctx* c, const char* who, const void* words, size_t word_pitch_bytes) {
+    if (!words || word_pitch_bytes < 8 * (size_t)((c->n + 63) / 64)) {
+        ltl_set_error("%s: bad buffer or word pitch %zu < %d", who, word_pitch_bytes, 8 * ((c->n + 63) / 64));
+        return LTL_EINVAL;
+    }
+    return LTL_OK;
+}
+
+static int pack_stage(ltl_ctx* c) {
+    if (c->pstage) return LTL_OK;
+    const size_t bytes = (size_t)c->rows * 8 * ((c->n + 63) / 64);
+    cudaError_t e = cudaMalloc(&c->pstage, std::max<size_t>(bytes, 8));
+    if (e != cudaSuccess) {
+        ltl_set_error("packed transfer staging allocation failed: %s", cudaGetErrorString(e));
+        return LTL_ENOMEM;
+    }
+    return LTL_OK;
+}
+
+extern "C" int ltl_upload_packed(ltl_ctx* c, const uint64_t* words, size_t word_pitch_bytes) {
+    if (int r = check_ctx(c)) return r;
+    if (int r = pack_args(c, "ltl_upload_packed", words, word_pitch_bytes)) return r;
+    LTL_CUDA(cudaSetDevice(c->device));
+    if (keeps_packed(c)) {
+        // straight into the packed frame: a little-endian uint64 row is its 32-bit
+        // word row; bits past n are rewritten by the halo pass (packed) or masked
+        // by the step (tensor)
+        PackedFrame& f = cur_packed(c);
+        LTL_CUDA(cudaMemcpy2DAsync(f.words + (size_t)f.HR * f.wpitch + f.HW, f.wpitch * sizeof(uint32_t), words,
+                                   word_pitch_bytes, (size_t)f.nw * sizeof(uint32_t), c->rows,
+                                   cudaMemcpyHostToDevice, c->stream));
+        if (c->variant == LTL_VARIANT_PACKED) LTL_CUDA(launch_packed_halo(f, c->stream));
+        c->packed_valid = true;
+    } else {
+        if (int r = pack_stage(c)) return r;
+        const size_t spitch = (size_t)(c->n + 63) / 64;  // words
+        LTL_CUDA(cudaMemcpy2DAsync(c->pstage, spitch * 8, words, word_pitch_bytes, spitch * 8, c->rows,
+                                   cudaMemcpyHostToDevice, c->stream));
+        Frame& f = cur_frame(c);
+        LTL_CUDA(launch_unpack(c->pstage, spitch, c->rows, c->n, f.inner(0, 0), f.pitch, c->stream));
+        if (int r = after_upload(c)) return r;
+    }
+    LTL_CUDA(cudaStreamSynchronize(c->stream));
+    return LTL_OK;
+}
+
+extern "C" int ltl_download_packed(ltl_ctx* c, uint64_t* words, size_t word_pitch_bytes) {
+    if (int r = check_ctx(c)) return r;
+    if (int r = pack_args(c, "ltl_download_packed", words, word_pitch_bytes)) return r;
+    LTL_CUDA(cudaSetDevice(c->device));
+    if (int r = pack_stage(c)) return r;
+    const size_t spitch = (size_t)(c->n + 63) / 64;  // words
+    if (keeps_packed(c) && c->packed_valid) {
+        LTL_CUDA(launch_frame_to_pack64(cur_packed(c), c->pstage, spitch, c->stream));
+    } else {
+        Frame& f = cur_frame(c);
+        LTL_CUDA(launch_pack(f.inner(0, 0), f.pitch, c->rows, c->n, c->pstage, spitch, c->stream));
+    }
+    LTL_CUDA(cudaMemcpy2DAsync(words, word_pitch_bytes, c->pstage, spitch * 8, spitch * 8, c->rows,
+                               cudaMemcpyDeviceToHost, c->stream));
     LTL_CUDA(cudaStreamSynchronize(c->stream));
     return LTL_OK;
 }

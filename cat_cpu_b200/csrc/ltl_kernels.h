@@ -79,6 +79,8 @@ cudaError_t launch_unpack_frame(const PackedFrame& src, const Frame& dst, cudaSt
 cudaError_t launch_unpack_rows(const PackedFrame& src, int row0, int nrows, uint8_t* dst, size_t pitch, cudaStream_t s);
 cudaError_t launch_pack_rows(const uint8_t* src, size_t pitch, const PackedFrame& dst, int row0, int nrows,
                              cudaStream_t s);
+// A packed frame's inner words as PACK-coded rows (bits past n cleared).
+cudaError_t launch_frame_to_pack64(const PackedFrame& f, uint64_t* dst, size_t dst_pitch_words, cudaStream_t s);
 cudaError_t launch_pack(const uint8_t* cells, size_t cell_pitch, int rows, int cols, uint64_t* words,
                         size_t word_pitch_words, cudaStream_t s);
 cudaError_t launch_unpack(const uint64_t* words, size_t word_pitch_words, int rows, int cols, uint8_t* cells,

@@ -28,6 +28,7 @@ SOLVER_CODE_TO_VARIANT = {7: VARIANT_PLAIN, 8: VARIANT_TENSOR, 9: VARIANT_PACKED
 # Every symbol include/ltl.h declares (tests check the library exports them all).
 ABI_SYMBOLS = [
     "ltl_create", "ltl_destroy", "ltl_set_stream", "ltl_get_info", "ltl_upload", "ltl_download",
+    "ltl_upload_packed", "ltl_download_packed",
     "ltl_upload_device", "ltl_download_device", "ltl_step", "ltl_synchronize", "ltl_population",
     "ltl_compare_device", "ltl_benchmark_seed", "ltl_generate_state", "ltl_pack_device", "ltl_unpack_device",
     "ltl_batch_create", "ltl_batch_destroy", "ltl_batch_set_stream", "ltl_batch_upload", "ltl_batch_download",
@@ -73,6 +74,8 @@ def lib():
     L.ltl_set_stream.argtypes = [vp, vp]
     L.ltl_get_info.argtypes = [vp, ctypes.POINTER(Info)]
     L.ltl_upload.argtypes = [vp, vp, sz]
+    L.ltl_upload_packed.argtypes = [vp, vp, sz]
+    L.ltl_download_packed.argtypes = [vp, vp, sz]
     L.ltl_download.argtypes = [vp, vp, sz]
     L.ltl_upload_device.argtypes = [vp, vp, sz]
     L.ltl_download_device.argtypes = [vp, vp, sz]
@@ -200,6 +203,19 @@ class CUDASolver:
 
     def synchronize(self):
         check(lib().ltl_synchronize(self._h))
+
+    def setStatePacked(self, words):
+        """Upload a grid in the PACK coding: uint64 array (rows, ceil(n / 64)),
+        cell (i, j) = bit j % 64 of word j / 64 (see pack_grid)."""
+        w = np.ascontiguousarray(words, dtype=np.uint64)
+        assert w.shape == (self.rows, (self.n + 63) // 64)
+        check(lib().ltl_upload_packed(self._h, _ptr(w), w.shape[1] * 8))
+
+    def getCurrentStatePacked(self):
+        """The current grid in the PACK coding (bits past n are 0)."""
+        out = np.empty((self.rows, (self.n + 63) // 64), dtype=np.uint64)
+        check(lib().ltl_download_packed(self._h, _ptr(out), out.shape[1] * 8))
+        return out
 
     def getCurrentState(self):
         """CASolver::getCurrentState (CASolver.cpp:9-13): inner n x n (rows x n) cells, uint8."""
@@ -335,3 +351,21 @@ class Batch:
 
     def set_stream(self, stream_ptr):
         check(lib().ltl_batch_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+
+def pack_grid(grid):
+    """A 0/1 uint8 grid (rows, n) in the PACK coding: uint64 (rows, ceil(n / 64)),
+    cell (i, j) = bit j % 64 of word j / 64."""
+    g = np.asarray(grid, dtype=np.uint8)
+    rows, n = g.shape
+    nw = (n + 63) // 64
+    padded = np.zeros((rows, nw * 64), dtype=np.uint8)
+    padded[:, :n] = g != 0
+    return np.packbits(padded, axis=1, bitorder="little").view("<u8").reshape(rows, nw)
+
+
+def unpack_grid(words, n):
+    """Inverse of pack_grid: uint8 (rows, n)."""
+    w = np.ascontiguousarray(words, dtype="<u8")
+    bits = np.unpackbits(w.view(np.uint8), axis=1, bitorder="little")
+    return bits[:, :n].copy()

@@ -102,6 +102,17 @@ int ltl_upload(ltl_ctx* ctx, const uint8_t* inner, size_t pitch);
  * (CASolver.cpp:9-13).  Synchronous. */
 int ltl_download(ltl_ctx* ctx, uint8_t* inner, size_t pitch);
 
+/* The same two transfers with the host grid in the PACK coding: row i holds
+ * ceil(cols / 64) uint64 words, cell (i, j) = bit j % 64 of word j / 64 (bits past
+ * cols are 0 on download and ignored on upload), rows `word_pitch_bytes` apart
+ * (at least 8 ceil(cols / 64)).  Eight times fewer bytes cross PCIe than with the
+ * uint8 forms; for the packed and tensor variants the words go straight into the
+ * device's packed frames (a little-endian uint64 row is the frames' 32-bit word
+ * row).  Synchronous.  The reference keeps uint8 grids only; this is the packed
+ * grid I/O of its GPU project's PACK solver, whose source it does not include. */
+int ltl_upload_packed(ltl_ctx* ctx, const uint64_t* words, size_t word_pitch_bytes);
+int ltl_download_packed(ltl_ctx* ctx, uint64_t* words, size_t word_pitch_bytes);
+
 /* Same as ltl_upload/ltl_download with device-resident inner grids (stream-ordered
  * on the context's stream, not synchronised). */
 int ltl_upload_device(ltl_ctx* ctx, const uint8_t* dev_inner, size_t pitch);

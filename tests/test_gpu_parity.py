@@ -278,6 +278,42 @@ def test_pack_codec_roundtrip():
         assert np.array_equal(back.cpu().numpy(), cells)
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_packed_host_io_vs_oracle(variant):
+    """ltl_upload_packed / ltl_download_packed (PACK-coded host grids) against the
+    uint8 transfers and the oracle: ragged and multiple-of-32/64 widths, uploads
+    in either form followed by downloads in either form, and steps in between."""
+    rng = np.random.default_rng(21 + VCODE[variant])
+    for n, r, rule in ((97, 3, O.sweep_rule(3)), (128, 5, O.BOSCO_R5), (200, 8, O.scaled_rule(8)),
+                       (64, 1, O.CONWAY), (300, 2, O.sweep_rule(2))):
+        g = (rng.random((n, n)) < 0.45).astype(np.uint8)
+        w = C.pack_grid(g)
+        s = make(variant, n, r, rule)
+        try:
+            s.setStatePacked(w)
+            assert np.array_equal(s.getCurrentState(), g)
+            assert np.array_equal(s.getCurrentStatePacked(), w)
+            s.doSteps(3)
+            g3 = O.run(g, r, rule, 3)
+            assert np.array_equal(s.getCurrentStatePacked(), C.pack_grid(g3)), (variant, n, r)
+            s.setState(g)                      # uint8 in, packed out
+            assert np.array_equal(s.getCurrentStatePacked(), w)
+            s.setStatePacked(C.pack_grid(g3))  # packed in, step, uint8 out
+            s.doStep()
+            assert np.array_equal(s.getCurrentState(), O.step(g3, r, rule))
+        finally:
+            s.close()
+    if variant == "packed":
+        rows, n = 77, 160
+        g = (rng.random((rows, n)) < 0.5).astype(np.uint8)
+        s = C.CUDASolver(n, 4, O.sweep_rule(4), variant=C.VARIANT_PACKED, rows=rows)
+        try:
+            s.setStatePacked(C.pack_grid(g))
+            assert np.array_equal(s.getCurrentState(), g)
+        finally:
+            s.close()
+
+
 def test_errors_on_device():
     with pytest.raises(C.LtlError) as e:
         C.CUDASolver(64, 40, (1, 2, 3, 4), variant=VCODE["packed"])
