@@ -82,10 +82,15 @@ constexpr int kRqWarps = 2 * 4;       // re-quantisation: two chunks per warp, f
 constexpr int kRuleChunks = 2;        // rule: two chunks per warp, four lane quarters
 constexpr int kRuleWarps = kChunks / kRuleChunks * 4;
 static_assert(kRuleChunks == 2, "the rule role handles two chunks per warp");
-// warp 0: product-1 MMAs, warp 1: product-2 MMAs, 2: packed-word loads,
-// 3..6: unpack, 7..14: re-quantisation, 15..22: rule
-constexpr int kLoadWarp = 2;
-constexpr int kUnpackWarp0 = 3;
+// warp 0: product-1 MMAs, warp 1: product-2 MMAs, 2..3: packed-word loads,
+// 4..7: unpack, 8..15: re-quantisation, 16..23: rule.  A warp runs on
+// scheduler warp % 4: each scheduler holds one unpack warp and one of the four
+// lighter single roles (the two MMA issuers, the two loaders), so that no
+// unpack warp -- all four gate every X stage -- shares its scheduler with more
+// work than the others.
+constexpr int kLoadWarp0 = 2;
+constexpr int kLoadWarps = 2;
+constexpr int kUnpackWarp0 = kLoadWarp0 + kLoadWarps;
 constexpr int kRqWarp0 = kUnpackWarp0 + kUnpackWarps;
 constexpr int kRuleWarp0 = kRqWarp0 + kRqWarps;
 constexpr int kThreads = 32 * (kRuleWarp0 + kRuleWarps);
@@ -147,6 +152,10 @@ __host__ __device__ constexpr int k2_rows(int mode) { return mode == kF16 ? 16 :
 // f16 row sums are stored as H + kF16Offset (see the header)
 constexpr int kF16Offset = 1024;
 
+// Words per X row in the packed-word ring: the NG + 1 words a row needs, rounded
+// up to whole 16-byte chunks (rows are 16-byte aligned in the ring).
+__host__ __device__ constexpr int ring_row_words(int ng) { return (ng + 1 + 3) / 4 * 4; }
+
 // W: (ng + kChunks - 1) * 32 rows (the N index) x 32 bytes (the K index of one step)
 __host__ __device__ constexpr int w_rows(int ng) { return 32 * (ng + kChunks - 1); }
 __host__ __device__ constexpr int atoms_for(int ng) { return (ng + 3) / 4; }
@@ -162,7 +171,7 @@ __host__ __device__ inline SmemLayout smem_layout(int stages, int ng, int nb, bo
     L.x_off = o;
     o += stages * atoms_for(ng) * kAtomBytes;  // 1024-aligned stages
     L.wr_off = o;
-    o += fast ? kWordDepth * (ng + 1) * 128 * 4 : 0;  // packed words of the next units
+    o += fast ? kWordDepth * 128 * ring_row_words(ng) * 4 : 0;  // packed words of the next units
     L.hs_off = o;
     o += 2 * 128 * kTc * h_bytes(mode);        // H (u8 or f16), MN-major, two buffers
     L.w_off = o;
@@ -306,7 +315,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             mbar_init(&bars[DRAIN + i], 1);
         }
         for (int i = 0; i < kWordDepth; ++i) {
-            mbar_init(&bars[W_FULL + i], 32);  // one cp.async-tracking arrival per loader lane
+            mbar_init(&bars[W_FULL + i], 32 * kLoadWarps);  // one cp.async-tracking arrival per loader thread
             mbar_init(&bars[W_EMPTY + i], kUnpackWarps);
         }
         fence_mbar_init();
@@ -361,7 +370,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
     fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp < kLoadWarp) {
+    if (warp < kLoadWarp0) {
         // --------------------------- MMA issuers ----------------------------
         // Warp 0 issues product 1 of every unit, warp 1 product 2, so that the
         // tensor core queue gets the next unit's product 1 while product 2 waits
@@ -442,18 +451,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
         if (leader) mma_commit(&bars[DRAIN + warp]);
         __syncwarp();
         if (!__all_sync(0xffffffffu, mbar_wait(&bars[DRAIN + warp], 0u, p.wait_ns)) && leader) atomicOr(p.err, 32u);
-    } else if (warp == kLoadWarp) {
+    } else if (warp < kUnpackWarp0) {
         // --------------------------- packed words ---------------------------
         // FAST tiles: the NG + 1 packed words of every X row of a unit (group g =
         // upper half of word g, lower half of word g + 1) go by cp.async into a
-        // ring of kWordDepth units, lane l loading rows l, l + 32, l + 64, l + 96.
+        // ring of kWordDepth units, row-major (ring_row_words per row); loader
+        // warp lw takes rows 64 lw .. 64 lw + 63.  Where the unit's words start on
+        // a 16-byte boundary and do not cross the torus seam (every interior tile
+        // when R <= 16) a row is whole 16-byte copies, else one copy per word.
         // The ring slot's barrier tracks the copies themselves
         // (cp.async.mbarrier.arrive), so the unpack warps, whose proxy fences wait
         // for every memory access of their own still in flight, never have a
         // global load outstanding.
         if (FAST) {
             constexpr int NW1 = NG + 1;
-            uint32_t* ring = (uint32_t*)(smem + L.wr_off);  // [kWordDepth][NW1][128]
+            constexpr int RW = ring_row_words(NG);
+            uint32_t* ring = (uint32_t*)(smem + L.wr_off);  // [kWordDepth][128][RW]
+            const int row_base = 64 * (warp - kLoadWarp0);
             const Walk wk(p);
             Cursor c;
             c.init(wk);
@@ -466,22 +480,33 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                                                            kSleepNs));
                     if (!ok) break;
                 }
-                uint32_t* d = ring + slot * NW1 * 128;
+                uint32_t* d = ring + slot * 128 * RW;
                 int wi0 = (c.tx * kTc - p.PADC - 16) >> 5;  // word holding X column 0
                 if (wi0 < 0) wi0 += p.nw;
+                // whole 16-byte chunks: aligned start (rows are 16-byte aligned:
+                // wpitch % 4 == 0), no seam inside the needed words, the chunks'
+                // extra words still inside the frame row
+                const bool vec = ((uintptr_t)(p.src + wi0) & 15) == 0 && (p.wpitch & 3) == 0 &&
+                                 wi0 + NW1 <= p.nw && wi0 + RW <= p.wpitch - 1;
                 const int gr0 = c.ty * p.Tr - R + 128 * c.b;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int row = lane + 32 * i;
+                for (int i = 0; i < 2; ++i) {
+                    const int row = row_base + lane + 32 * i;
                     int gr = gr0 + row;
                     if (gr < 0) gr += p.n;
                     else if (gr >= p.n) gr -= p.n;
                     const uint32_t* rp = p.src + (size_t)gr * (size_t)p.wpitch;
-                    int wi = wi0;
+                    uint32_t* dr = d + row * RW;
+                    if (vec) {
 #pragma unroll
-                    for (int k = 0; k < NW1; ++k) {
-                        cp_async4(d + k * 128 + row, rp + wi);
-                        if (++wi == p.nw) wi = 0;
+                        for (int k = 0; k < RW; k += 4) cp_async16(dr + k, rp + wi0 + k);
+                    } else {
+                        int wi = wi0;
+#pragma unroll
+                        for (int k = 0; k < NW1; ++k) {
+                            cp_async4(dr + k, rp + wi);
+                            if (++wi == p.nw) wi = 0;
+                        }
                     }
                 }
                 cp_async_mbar_arrive(&bars[W_FULL + slot]);
@@ -524,18 +549,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             return true;
         };
         if (FAST) {
-            // words from the loader warp's ring (see above)
+            // words from the loader warps' ring (see above): this row's, as 16-byte vectors
             constexpr int NW1 = NG + 1;
-            const uint32_t* ring = (const uint32_t*)(smem + L.wr_off) + row;  // [kWordDepth][NW1][128]
+            constexpr int RW = ring_row_words(NG);
+            const uint32_t* ring = (const uint32_t*)(smem + L.wr_off) + row * RW;  // [kWordDepth][128][RW]
             for (; c.u < units; c.next(wk)) {
                 const int slot = c.u & (kWordDepth - 1);
                 ok = __all_sync(0xffffffffu, mbar_wait(&bars[W_FULL + slot], (uint32_t)((c.u / kWordDepth) & 1),
                                                        p.wait_ns, kSleepNs));
                 if (!ok) break;
-                const uint32_t* d = ring + slot * NW1 * 128;
-                uint32_t w[NW1];
+                const uint4* d = (const uint4*)(ring + slot * 128 * RW);
+                uint32_t w[RW];
 #pragma unroll
-                for (int k = 0; k < NW1; ++k) w[k] = d[k * 128];
+                for (int k = 0; k < RW / 4; ++k) {
+                    const uint4 v = d[k];
+                    w[4 * k] = v.x;
+                    w[4 * k + 1] = v.y;
+                    w[4 * k + 2] = v.z;
+                    w[4 * k + 3] = v.w;
+                }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&bars[W_EMPTY + slot]);
                 ok = store(c, [&](int g) { return prmt(w[g], w[g + 1], 0x5432u); });
