@@ -51,6 +51,16 @@ class GpuSolver {
         check(ltl_download(ctx_, g.data(), (size_t)n_), "ltl_download");
         return g;
     }
+    // The grid in the PACK coding: n rows of ceil(n / 64) uint64 words, cell
+    // (i, j) = bit j % 64 of word j / 64 (ltl_upload_packed / ltl_download_packed).
+    void setStatePacked(const uint64_t* words) {
+        check(ltl_upload_packed(ctx_, words, 8 * (size_t)((n_ + 63) / 64)), "ltl_upload_packed");
+    }
+    std::vector<uint64_t> getCurrentStatePacked() {
+        std::vector<uint64_t> w((size_t)n_ * ((n_ + 63) / 64));
+        check(ltl_download_packed(ctx_, w.data(), 8 * (size_t)((n_ + 63) / 64)), "ltl_download_packed");
+        return w;
+    }
     void printCurrentState() {
         auto g = getCurrentState();
         for (int i = 0; i < n_; ++i) {

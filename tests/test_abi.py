@@ -88,3 +88,30 @@ def test_factory_unknown_code_returns_none():
     import cat_cpu_b200 as C
     assert C.CASolverFactory.createSolver(0, 0, 64, 5, 1, O.BOSCO_R5) is None
     assert C.CASolverFactory.createSolver(42, 0, 64, 5, 1, O.BOSCO_R5) is None
+
+
+def test_pack_coding_helpers():
+    """pack_grid / unpack_grid (the host side of ltl_upload_packed and
+    ltl_download_packed) against the PACK coding written out cell by cell:
+    cell (i, j) = bit j % 64 of uint64 word j / 64, bits past the row's end 0."""
+    import cat_cpu_b200 as C
+    rng = np.random.default_rng(8)
+    for rows, n in ((3, 1), (4, 63), (5, 64), (2, 65), (7, 200), (1, 128)):
+        g = (rng.random((rows, n)) < 0.5).astype(np.uint8)
+        w = C.pack_grid(g)
+        assert w.dtype == np.uint64 and w.shape == (rows, (n + 63) // 64)
+        want = np.zeros_like(w)
+        for i in range(rows):
+            for j in range(n):
+                if g[i, j]:
+                    want[i, j // 64] |= np.uint64(1) << np.uint64(j % 64)
+        assert np.array_equal(w, want)
+        assert np.array_equal(C.unpack_grid(w, n), g)
+
+
+def test_packed_io_argument_errors_without_device():
+    import cat_cpu_b200 as C
+    L = C.lib()
+    buf = (ctypes.c_uint64 * 4)()
+    assert L.ltl_upload_packed(None, buf, 32) == C.ltl.EINVAL
+    assert L.ltl_download_packed(None, buf, 32) == C.ltl.EINVAL
