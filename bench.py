@@ -47,6 +47,15 @@ BYTES_PER_UPDATE = {"plain": 2.0, "tensor": 0.25, "packed": 0.25}
 DTYPE = {"plain": "u8", "tensor": "b1 state, u8 x u8 -> s32 operands (tcgen05 kind::i8)",
          "packed": "b1 (32 cells per u32)"}
 REF_RULE_TAG = "R5_S32-56_B34-45"
+# What bounds each step kernel, from the committed ncu captures of the 16384^2 R=5
+# workload (the bit-packed kernels are bound by logic operations on the ALU pipe,
+# the tensor kernel by hand-offs between its warp roles, not by HBM).
+LIMITER = {
+    "plain": {"pipe": "alu", "ncu_pct_of_peak": 72.0, "source": "profiles/k_plain_swar8_tb_n16384_r5.md"},
+    "packed": {"pipe": "alu", "ncu_pct_of_peak": 70.7, "source": "profiles/k_packed_step_n16384_r5.md"},
+    "tensor": {"pipe": "tensor", "ncu_pct_of_peak": 29.5, "issue_active_pct": 56.5,
+               "source": "profiles/k_tensor_step_n16384_r5.md"},
+}
 
 
 def env_int(name, default):
@@ -612,6 +621,7 @@ def main():
                          "frac": round(achieved / peak, 4), "traffic": traffic.get(name),
                          "traffic_source": "profiles/traffic_n16384_r5.txt: dram bytes of one ncu capture of "
                                            "the step kernel (cache control on, the run's L2 flush not applied)"},
+            "limiter": LIMITER[name],
             "gpu_launches": r["all_launches"],
         }
         if r["bit_exact_step100"] and (best is None or gcups > variants[best]["gcups"]):
