@@ -12,7 +12,9 @@ scripts/extractBestRegionSize.py): here the swept shapes are
                    but leave fewer items to balance over 148 SMs);
   plain            depth: generations per pass of the temporally blocked kernel
                    (1, 2 or 3), swept jointly with band_rows;
-  batch            stream_band_rows of the streamed per-step kernels, and
+  batch            persistent: one launch per call that runs every generation of
+                   every grid (1), or per-generation launches (0), and for the
+                   latter stream_band_rows of the streamed per-step kernels and
                    resident_max_bytes: which grids are kept in shared memory for
                    a whole multi-step launch and which are streamed each step.
 The full landscape (every candidate's time) is written next to the table.
@@ -85,20 +87,24 @@ def tune_batch(torch, C, band_candidates, resident_candidates, steps):
     rows = []
     try:
         b.set_stream(stream.cuda_stream)
-        for rm in resident_candidates:
-            for br in band_candidates:
-                b.set_param("resident_max_bytes", rm)
-                b.set_param("stream_band_rows", br)
-                b.upload_all(flat)
-                b.step(steps)          # builds and warms the graph
-                b.synchronize()
-                a = torch.cuda.Event(enable_timing=True)
-                e = torch.cuda.Event(enable_timing=True)
-                a.record(stream)
-                b.step(steps)
-                e.record(stream)
-                stream.synchronize()
-                rows.append(((br, rm), a.elapsed_time(e)))
+        # (persistent, stream_band_rows, resident_max_bytes); the last two only
+        # matter for per-generation launches
+        cands = [(1, band_candidates[0], resident_candidates[0])] + \
+            [(0, br, rm) for rm in resident_candidates for br in band_candidates]
+        for pers, br, rm in cands:
+            b.set_param("persistent", pers)
+            b.set_param("resident_max_bytes", rm)
+            b.set_param("stream_band_rows", br)
+            b.upload_all(flat)
+            b.step(steps)          # builds and warms the graph
+            b.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            b.step(steps)
+            e.record(stream)
+            stream.synchronize()
+            rows.append(((pers, br, rm), a.elapsed_time(e)))
     finally:
         b.close()
     best = min(rows, key=lambda x: x[1])
@@ -136,10 +142,10 @@ def main():
         print(land[-1], flush=True)
     band_c = [32, 64, 128] if args.quick else [32, 48, 64, 96, 128]
     res_c = [0, 225280] if args.quick else [0, 65536, 131072, 225280]
-    ((br, rm), ms), rows = tune_batch(torch, C, band_c, res_c, 256)
-    table.append(f"variant=batch radius=* stream_band_rows={br} resident_max_bytes={rm}")
-    land.append("batch (stream_band_rows, resident_max_bytes): " +
-                ", ".join(f"{c}:{t:.2f}" for c, t in rows) + f"  -> {(br, rm)}")
+    ((pers, br, rm), ms), rows = tune_batch(torch, C, band_c, res_c, 256)
+    table.append(f"variant=batch radius=* persistent={pers} stream_band_rows={br} resident_max_bytes={rm}")
+    land.append("batch (persistent, stream_band_rows, resident_max_bytes): " +
+                ", ".join(f"{c}:{t:.2f}" for c, t in rows) + f"  -> {(pers, br, rm)}")
     print(land[-1], flush=True)
     with open(os.path.join(args.out, "ltl_tuning.txt"), "w") as f:
         f.write("\n".join(table) + "\n")
