@@ -103,6 +103,10 @@ constexpr uint32_t kSleepNs = 32;
 // TMEM columns: H in two buffers (units alternate), C in two buffers (tiles alternate)
 __host__ __device__ constexpr uint32_t h_col(int buf) { return 128u * (uint32_t)buf; }
 __host__ __device__ constexpr uint32_t c_col(int buf) { return 256u + 128u * (uint32_t)buf; }
+// X in tensor memory (the XT form, NG <= 5): one C buffer, and the X stages of
+// 8 NG columns each from column 384 (three stages of 40 columns at NG = 5)
+constexpr int kXtStages = 3;
+__host__ __device__ constexpr uint32_t x_col(int stage, int ng) { return 384u + 8u * (uint32_t)(ng * stage); }
 
 struct TcParams {
     const uint32_t* src;  // inner word (0, 0) of the current packed frame
@@ -165,11 +169,11 @@ __host__ __device__ constexpr int g_rows(int nb, int mode) {
     return 128 + k2_rows(mode) * (128 * nb / k2_rows(mode) - 1);
 }
 
-__host__ __device__ inline SmemLayout smem_layout(int stages, int ng, int nb, bool fast, int mode) {
+__host__ __device__ inline SmemLayout smem_layout(int stages, int ng, int nb, bool fast, int mode, bool xt = false) {
     SmemLayout L{};
     int o = 0;
     L.x_off = o;
-    o += stages * atoms_for(ng) * kAtomBytes;  // 1024-aligned stages
+    o += xt ? 0 : stages * atoms_for(ng) * kAtomBytes;  // 1024-aligned stages (none when X is in TMEM)
     L.wr_off = o;
     o += fast ? kWordDepth * 128 * ring_row_words(ng) * 4 : 0;  // packed words of the next units
     L.hs_off = o;
@@ -276,8 +280,10 @@ struct Cursor {
 // MODE: rule lanes and product-2 operand type (TcMode); FAST: n % 32 == 0 and
 // large enough that rows and words wrap with one correction; NG: product-1 K
 // steps = X groups of 32 columns per row.
-template <int MODE, bool FAST, int NG>
+template <int MODE, bool FAST, int NG, bool XT>
 __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_constant__ TcParams p) {
+    static_assert(!XT || (FAST && NG <= 5), "X in tensor memory: FAST tiles with at most 5 K steps");
+    constexpr int kCBufs = XT ? 1 : 2;  // C buffers in TMEM
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     constexpr int ATOMS = atoms_for(NG);
@@ -285,7 +291,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
     constexpr int K2 = k2_rows(MODE);   // K rows per product-2 MMA
     constexpr int S2 = 128 / K2;        // product-2 MMAs per row block
     const int nb = p.nb, S = p.stages, R = p.R;
-    const SmemLayout L = smem_layout(S, NG, nb, FAST, MODE);
+    const SmemLayout L = smem_layout(S, NG, nb, FAST, MODE, XT);
     uint8_t* xs = smem + L.x_off;
     uint8_t* hs = smem + L.hs_off;
     uint8_t* wm = smem + L.w_off;
@@ -405,7 +411,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                         // X group s: atom s / 4, byte 32 (s % 4) of its rows; W from row 32 (NG - 1 - s)
                         const uint64_t ad = xs0 + (uint64_t)((s >> 2) * (kAtomBytes >> 4) + (s & 3) * 2);
                         const uint64_t bd = wd0 + (uint64_t)((NG - 1 - s) * 4 * (256 >> 4));
-                        mma_i8(tmem + h_col(hb), ad, bd, id1, s > 0 ? 1u : 0u);
+                        if constexpr (XT) {
+                            mma_i8_ts(tmem + h_col(hb), tmem + x_col(c.st, NG) + 8u * (uint32_t)s, bd, id1,
+                                      s > 0 ? 1u : 0u);
+                        } else {
+                            mma_i8(tmem + h_col(hb), ad, bd, id1, s > 0 ? 1u : 0u);
+                        }
                     }
                     if (!(p.inject_missing_commit && c.u == 0)) mma_commit(&bars[H_FULL + hb]);
                     mma_commit(&bars[X_EMPTY + c.st]);  // the stage is free once product 1 has read it
@@ -420,9 +431,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             const uint64_t hsd0 = desc_noswz(smem_u32(hs), 128, 128 * 16);
             const int T2 = S2 * nb;
             for (; c.u < units && ok; c.next(wk)) {
-                const int hb = c.u & 1, cb = c.j & 1;
+                const int hb = c.u & 1, cb = c.j % kCBufs;
                 ok = wait(&bars[HS_FULL + hb], (uint32_t)((c.u >> 1) & 1));
-                if (ok && c.b == 0 && c.j >= 2) ok = wait(&bars[C_EMPTY + cb], (uint32_t)(((c.j >> 1) - 1) & 1));
+                if (ok && c.b == 0 && c.j >= kCBufs)
+                    ok = wait(&bars[C_EMPTY + cb], (uint32_t)(((c.j / kCBufs) - 1) & 1));
                 if (!ok) break;
                 fence_after();
                 if (leader) {
@@ -531,19 +543,36 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                 if (lane == 0) wt = mbar_wait(&bars[X_EMPTY + cc.st], (uint32_t)(cc.sph ^ 1), p.wait_ns, kSleepNs);
                 if (!__shfl_sync(0xffffffffu, wt, 0)) return false;
             }
-            uint8_t* xrow = xs + cc.st * kXB + row * 128;
+            if constexpr (XT) {
+                // X row `row` is TMEM lane `row` (this warp's lane quarter, warp % 4):
+                // group g is 8 columns, four K bytes per column
+                fence_after();
+                const uint32_t xa = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + x_col(cc.st, NG);
 #pragma unroll
-            for (int g = 0; g < NG; ++g) {
-                const uint32_t x = x_of(g);
-                uint32_t v[8];
+                for (int g = 0; g < NG; ++g) {
+                    const uint32_t x = x_of(g);
+                    uint32_t v[8];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) v[k] = (x >> k) & 0x01010101u;
-                uint8_t* ap = xrow + (g >> 2) * kAtomBytes;
-                const int ch = 2 * (g & 3);
-                *(uint4*)(ap + ((ch ^ sw) << 4)) = make_uint4(v[0], v[1], v[2], v[3]);
-                *(uint4*)(ap + (((ch + 1) ^ sw) << 4)) = make_uint4(v[4], v[5], v[6], v[7]);
+                    for (int k = 0; k < 8; ++k) v[k] = (x >> k) & 0x01010101u;
+                    tmem_st8(xa + 8u * (uint32_t)g, v);
+                }
+                tmem_wait_st();
+                fence_before();
+            } else {
+                uint8_t* xrow = xs + cc.st * kXB + row * 128;
+#pragma unroll
+                for (int g = 0; g < NG; ++g) {
+                    const uint32_t x = x_of(g);
+                    uint32_t v[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) v[k] = (x >> k) & 0x01010101u;
+                    uint8_t* ap = xrow + (g >> 2) * kAtomBytes;
+                    const int ch = 2 * (g & 3);
+                    *(uint4*)(ap + ((ch ^ sw) << 4)) = make_uint4(v[0], v[1], v[2], v[3]);
+                    *(uint4*)(ap + (((ch + 1) ^ sw) << 4)) = make_uint4(v[4], v[5], v[6], v[7]);
+                }
+                fence_proxy_async();
             }
-            fence_proxy_async();
             __syncwarp();
             if (lane == 0) mbar_arrive(&bars[X_FULL + cc.st]);
             return true;
@@ -722,8 +751,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             long long at0 = mine > 0 ? out_at(c, 0) : -1, at1 = mine > 0 ? out_at(c, 1) : -1;
             uint32_t cw0 = at0 >= 0 ? __ldg(p.src + at0) : 0u, cw1 = at1 >= 0 ? __ldg(p.src + at1) : 0u;
             for (int j = 0; j < mine && ok; ++j) {
-                const int cb = j & 1;
-                ok = wait_all(&bars[C_FULL + cb], (uint32_t)((j >> 1) & 1));
+                const int cb = j % kCBufs;
+                ok = wait_all(&bars[C_FULL + cb], (uint32_t)((j / kCBufs) & 1));
                 if (!ok) break;
                 fence_after();
                 uint32_t acc0, acc1;
@@ -798,9 +827,13 @@ struct TensorPlan {
 //   R 128        32-bit lanes on f32 counts, f16 product 2, 13 K steps
 template <int MODE, int NG>
 static TcKernel pick_fast(bool fast) {
-    return fast ? k_tensor_step<MODE, true, NG> : k_tensor_step<MODE, false, NG>;
+    return fast ? k_tensor_step<MODE, true, NG, false> : k_tensor_step<MODE, false, NG, false>;
 }
+// X in tensor memory: FAST tiles of 8- and 16-bit rule lanes with 5 K steps (R <= 16)
+static bool tensor_xt(int mode, bool fast, int ng) { return fast && ng == 5 && mode <= kLanes16; }
 static TcKernel pick_kernel(int mode, bool fast, int ng) {
+    if (tensor_xt(mode, fast, ng))
+        return mode == kLanes8 ? k_tensor_step<kLanes8, true, 5, true> : k_tensor_step<kLanes16, true, 5, true>;
     switch (mode) {
         case kLanes8: return ng == 5 ? pick_fast<kLanes8, 5>(fast) : nullptr;
         case kLanes16:
@@ -909,6 +942,12 @@ static bool tensor_geometry(int R, bool fast_ok, TensorGeometry& G) {
     G.ng = (G.PADC + kTc + R + 31) / 32;
     G.mode = tensor_mode(R);
     if (G.Tr < 1 || R > kTensorMaxRadius || 2 * R + 1 + kF16Offset > 2048) return false;
+    if (tensor_xt(G.mode, fast_ok, G.ng)) {
+        // X in tensor memory: kXtStages stages of TMEM columns, no X in shared memory
+        G.stages = kXtStages;
+        G.fast = true;
+        return smem_layout(G.stages, G.ng, G.nb, true, G.mode, true).total + 1024 <= kSmemLimit;
+    }
     // the deepest X ring that fits, with the word ring where possible
     for (int f = fast_ok ? 1 : 0; f >= 0; --f) {
         for (int st = kMaxStages; st >= 2; --st) {
@@ -1006,7 +1045,7 @@ TensorPlan* tensor_plan_create(const PackedFrame& a, const PackedFrame& b, const
         delete P;
         return nullptr;
     }
-    P->smem_bytes = smem_layout(G.stages, G.ng, G.nb, fast, G.mode).total + 1024;
+    P->smem_bytes = smem_layout(G.stages, G.ng, G.nb, fast, G.mode, tensor_xt(G.mode, fast, G.ng)).total + 1024;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     P->grid = std::min(P->prm[0].tiles_x * P->prm[0].tiles_y, sms);
