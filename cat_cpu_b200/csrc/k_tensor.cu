@@ -103,9 +103,12 @@ constexpr uint32_t kSleepNs = 32;
 // TMEM columns: H in two buffers (units alternate), C in two buffers (tiles alternate)
 __host__ __device__ constexpr uint32_t h_col(int buf) { return 128u * (uint32_t)buf; }
 __host__ __device__ constexpr uint32_t c_col(int buf) { return 256u + 128u * (uint32_t)buf; }
-// X in tensor memory (the XT form, NG <= 5): one C buffer, and the X stages of
-// 8 NG columns each from column 384 (three stages of 40 columns at NG = 5)
+// X in tensor memory (the XT form, NG <= 5): one H buffer (columns 0..127; the
+// re-quantisation warps release it as soon as they have loaded it), C at
+// columns 128..383, and the X stages of 8 NG columns each from column 384
+// (three stages of 40 columns at NG = 5)
 constexpr int kXtStages = 3;
+__host__ __device__ constexpr uint32_t c_col_xt(int buf) { return 128u + 128u * (uint32_t)buf; }
 __host__ __device__ constexpr uint32_t x_col(int stage, int ng) { return 384u + 8u * (uint32_t)(ng * stage); }
 
 struct TcParams {
@@ -283,7 +286,9 @@ struct Cursor {
 template <int MODE, bool FAST, int NG, bool XT>
 __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_constant__ TcParams p) {
     static_assert(!XT || (FAST && NG <= 5), "X in tensor memory: FAST tiles with at most 5 K steps");
-    constexpr int kCBufs = XT ? 1 : 2;  // C buffers in TMEM
+    constexpr int kHBufs = XT ? 1 : 2;  // H buffers in TMEM (C has two either way)
+    constexpr int kCBufs = 2;
+    auto ccol = [](int buf) -> uint32_t { return XT ? c_col_xt(buf) : c_col(buf); };
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     constexpr int ATOMS = atoms_for(NG);
@@ -399,9 +404,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             const uint64_t xd0 = desc_k_sw128(smem_u32(xs));
             const uint64_t wd0 = desc_noswz(smem_u32(wm), 128, 256);
             for (; c.u < units && ok; c.next(wk)) {
-                const int hb = c.u & 1;
+                const int hb = c.u % kHBufs;
                 ok = wait(&bars[X_FULL + c.st], (uint32_t)c.sph);
-                if (ok && c.u >= 2) ok = wait(&bars[H_EMPTY + hb], (uint32_t)(((c.u >> 1) - 1) & 1));
+                if (ok && c.u >= kHBufs) ok = wait(&bars[H_EMPTY + hb], (uint32_t)(((c.u / kHBufs) - 1) & 1));
                 if (!ok) break;
                 fence_after();
                 if (leader) {
@@ -447,9 +452,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                         const uint64_t bd = hd + (uint64_t)((s * K2 * 16) >> 4);
                         const uint32_t acc = (c.b > 0 || s > 0) ? 1u : 0u;
                         if constexpr (MODE == kF16) {
-                            mma_f16(tmem + c_col(cb), ad, bd, id2, acc);
+                            mma_f16(tmem + ccol(cb), ad, bd, id2, acc);
                         } else {
-                            mma_i8(tmem + c_col(cb), ad, bd, id2, acc);
+                            mma_i8(tmem + ccol(cb), ad, bd, id2, acc);
                         }
                     }
                     mma_commit(&bars[HS_EMPTY + hb]);
@@ -643,17 +648,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
             const int h = (warp - kRqWarp0) >> 2;
             const uint32_t lane_off = ((uint32_t)(q * 32) << 16) + (uint32_t)(2 * kN1 * h);
             for (; c.u < units && ok; c.next(wk)) {
-                const int hb = c.u & 1;
-                ok = wait_all(&bars[H_FULL + hb], (uint32_t)((c.u >> 1) & 1));
+                const int hb = c.u & 1;           // shared-memory H buffer (two)
+                const int tb = c.u % kHBufs;      // TMEM H buffer
+                ok = wait_all(&bars[H_FULL + tb], (uint32_t)((c.u / kHBufs) & 1));
                 if (!ok) break;
                 fence_after();
                 uint32_t va[16], vb[16];
-                tmem_ld32p(tmem + lane_off + h_col(hb), va);
-                tmem_ld32p(tmem + lane_off + h_col(hb) + kN1, vb);
+                tmem_ld32p(tmem + lane_off + h_col(tb), va);
+                tmem_ld32p(tmem + lane_off + h_col(tb) + kN1, vb);
                 tmem_wait_2x16(va, vb);
                 fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&bars[H_EMPTY + hb]);
+                if (lane == 0) mbar_arrive(&bars[H_EMPTY + tb]);
                 // product 2 of unit u - 2 has read the buffer
                 if (c.u >= 2) ok = wait_all(&bars[HS_EMPTY + hb], (uint32_t)(((c.u >> 1) - 1) & 1));
                 if (!ok) break;
@@ -760,12 +766,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                     // 64 values do not fit the registers at once: one chunk after the
                     // other, the C buffer released after the second chunk's loads
                     uint32_t v0[16], v1[16];
-                    tmem_ld16(tmem + lane_off + c_col(cb), v0);
-                    tmem_ld16(tmem + lane_off + c_col(cb) + 16, v1);
+                    tmem_ld16(tmem + lane_off + ccol(cb), v0);
+                    tmem_ld16(tmem + lane_off + ccol(cb) + 16, v1);
                     tmem_wait_2x16(v0, v1);
                     acc0 = rule32(v0, v1, cw0);
-                    tmem_ld16(tmem + lane_off + c_col(cb) + kN1, v0);
-                    tmem_ld16(tmem + lane_off + c_col(cb) + kN1 + 16, v1);
+                    tmem_ld16(tmem + lane_off + ccol(cb) + kN1, v0);
+                    tmem_ld16(tmem + lane_off + ccol(cb) + kN1 + 16, v1);
                     tmem_wait_2x16(v0, v1);
                     fence_before();
                     __syncwarp();
@@ -773,8 +779,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tensor_step(const __grid_consta
                     acc1 = rule32(v0, v1, cw1);
                 } else {
                     uint32_t va[16], vb[16];
-                    tmem_ld32p(tmem + lane_off + c_col(cb), va);
-                    tmem_ld32p(tmem + lane_off + c_col(cb) + kN1, vb);
+                    tmem_ld32p(tmem + lane_off + ccol(cb), va);
+                    tmem_ld32p(tmem + lane_off + ccol(cb) + kN1, vb);
                     tmem_wait_2x16(va, vb);
                     fence_before();
                     __syncwarp();
