@@ -53,7 +53,7 @@ REF_RULE_TAG = "R5_S32-56_B34-45"
 LIMITER = {
     "plain": {"pipe": "alu", "ncu_pct_of_peak": 72.0, "source": "profiles/k_plain_swar8_tb_n16384_r5.md"},
     "packed": {"pipe": "alu", "ncu_pct_of_peak": 70.7, "source": "profiles/k_packed_step_n16384_r5.md"},
-    "tensor": {"pipe": "tensor", "ncu_pct_of_peak": 29.5, "issue_active_pct": 56.5,
+    "tensor": {"pipe": "tensor", "ncu_pct_of_peak": 32.8, "issue_active_pct": 59.9,
                "source": "profiles/k_tensor_step_n16384_r5.md"},
 }
 
